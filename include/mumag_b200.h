@@ -1,0 +1,199 @@
+/*
+ * mumag_b200.h -- C ABI of libmumag_b200.so, the B200 (sm_100a) back end of the
+ * hysteresis-loop hot path of mammos-mumag.
+ *
+ * The reference runs its hot path as a subprocess, `run-escript scripts/loop.py <name>`
+ * (src/mammos_mumag/simulation.py:114-140, :285-332), whose solver core is a set of
+ * jitted JAX functions over escript-assembled sparse operators.  This library replaces
+ * that subprocess: the Python host (mammos_mumag.Simulation.run_loop) calls it in process.
+ * Plain C types only; host arrays are owned by the caller; device state lives behind an
+ * opaque mesh handle.  Every call returns an mm_status; on failure mm_last_error() holds
+ * a message.
+ *
+ * Layouts at this boundary are the reference's:
+ *   X    [N][3]  node coordinates in mesh-file order (nm), double
+ *   T    [E][4]  tetrahedra, 0-based node indices, int32
+ *   tag  [E]     element tags, int32; material row i belongs to the i-th tag in
+ *                ascending order (scripts/materials.py:22-25)
+ *   m    [3N]    interleaved magnetisation [mx0,my0,mz0,mx1,...] (scripts/converters.py:36-37)
+ *   u    [N]     magnetostatic scalar potential
+ * Energies are in the reference's internal units (J/m^3 times mu0); divide by
+ * scipy.constants.mu_0 for the .dat column (scripts/tools.py:20-24).
+ */
+#ifndef MUMAG_B200_H
+#define MUMAG_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef int mm_status;
+enum {
+  MM_OK = 0,
+  MM_BAD_INPUT = 1,    /* invalid sizes, indices, materials, or a missing mesh handle */
+  MM_CUDA_ERROR = 2,   /* a CUDA runtime call failed (message in mm_last_error) */
+  MM_NONFINITE = 3,    /* the energy became NaN/Inf during a solve */
+  MM_TIMEOUT = 4,      /* a device-side grid barrier gave up waiting (kernel returned early) */
+  MM_NO_DEVICE = 5     /* no usable sm_100 device */
+};
+
+/* One .krn row (src/mammos_mumag/templates/krn.jinja:1-3): theta phi K1 K2 Js A.
+ * Js in T, K1/K2 in J/m^3, A in J/m.  K2 is carried but, as in the reference
+ * (scripts/materials.py:28-34), not used. */
+typedef struct {
+  double theta, phi, K1, K2, Js, A;
+} mm_material;
+
+enum { MM_PREC_FP64 = 0, MM_PREC_MIXED = 1 };
+enum { MM_DIRICHLET_RHS_REFERENCE = 0, MM_DIRICHLET_RHS_ZERO = 1 };
+
+typedef struct {
+  double size;         /* length unit of X in m; the reference fixes 1e-9 (scripts/materials.py:13) */
+  int dirichlet_rhs;   /* MM_DIRICHLET_RHS_*: Poisson right-hand side on Dirichlet nodes */
+  int precision;       /* MM_PREC_*: arithmetic of the operator kernels */
+  int device;          /* CUDA device ordinal */
+  int grid_ctas;       /* persistent-kernel CTAs; 0 = autotuned */
+  int block_threads;   /* threads per CTA; 0 = autotuned */
+  int reorder;         /* 1 = reverse Cuthill-McKee node order on the device (default), 0 = file order */
+} mm_options;
+
+/* Solver settings of one field step (scripts/tools.py:64-120, scripts/minimizers.py:140-190). */
+typedef struct {
+  double hdir[3];      /* unit field direction (the .p2 [field] hx,hy,hz normalised) */
+  double tol_fun;      /* NCG tolerance (tol_fun) */
+  double tol_u;        /* Poisson PCG relative residual tolerance (tol_fun * tol_hmag_factor) */
+  int precond_iter;    /* truncated-CG iterations of the M_inv preconditioner */
+  int hmag_on;         /* 0 disables the magnetostatic term */
+  int mbar_mode;       /* 0: M_inv projects with the loop's initial m (the reference,
+                          scripts/loop.py:50-52); 1: with the current iterate */
+  int max_pcg_iter;    /* Poisson PCG cap (reference 10000, scripts/solvers.py:222) */
+  int max_ncg_iter;    /* NCG cap (reference 100000, scripts/minimizers.py:142) */
+} mm_solver_params;
+
+/* Result of one field step. */
+typedef struct {
+  double energy;       /* total energy at the minimiser (internal units) */
+  double mh;           /* magnetic polarisation along hdir, T (scripts/loop.py:25-38) */
+  int64_t ncg_iters;   /* NCG iterations k as returned by hestenes_stiefel_ncg */
+  int64_t evals;       /* energy+gradient evaluations */
+  int64_t pcg_iters;   /* Poisson PCG iterations summed over the evaluations */
+  int64_t ls_shrinks;  /* line-search step halvings */
+  int64_t minv_iters;  /* truncated-CG iterations inside M_inv */
+  int status;          /* MM_OK, MM_NONFINITE or MM_TIMEOUT */
+} mm_step_result;
+
+typedef struct {
+  int64_t nodes, elements;
+  int64_t sell_slices, sell_entries;   /* SELL-32 Poisson/operator pattern */
+  int64_t nnz;                         /* unpadded node-pair entries */
+  int32_t colours;                     /* element colours used by the assembly kernels */
+  int32_t airbox;                      /* 1: bare-box Dirichlet branch, 0: spherical shell */
+  int32_t grid_ctas, block_threads;    /* persistent-kernel launch shape in use */
+  int64_t dirichlet_nodes;
+  double volume;                       /* magnetic volume V, nm^3 */
+  double bandwidth_before, bandwidth_after;  /* max |i-j| over node pairs, file vs device order */
+} mm_mesh_info;
+
+/* Field-sweep parameters (the .p2 [field] section; scripts/loop.py:71-142). */
+typedef struct {
+  double hstart, hfinal, hstep, mstep, mfinal;
+  int32_t max_steps;   /* <= 0: int(|hfinal-hstart|/|hstep|)+1 as the reference */
+} mm_loop_params;
+
+/* One .dat row: vtk counter, mu0*Hext [T], polarisation [T], energy (internal units). */
+typedef struct {
+  double counter, hext, mh, energy;
+} mm_record;
+
+/* Called where the reference writes <name>_<counter:04d>.vtu (scripts/loop.py:103-116):
+ * m [3N] and u [N] in mesh-file order, valid for the duration of the call.
+ * A non-zero return aborts the loop with MM_BAD_INPUT. */
+typedef int (*mm_snapshot_cb)(int counter, const double* m, const double* u, int64_t n, void* user);
+
+typedef struct mm_mesh mm_mesh;
+
+/* Library version string. */
+const char* mm_version(void);
+
+/* Message of the last failed call on this thread ("" if none). */
+const char* mm_last_error(void);
+
+/* Default options / solver parameters (the reference's defaults). */
+void mm_default_options(mm_options* opt);
+void mm_default_solver_params(mm_solver_params* sp);
+
+/* Number of usable sm_100 devices (0 without a GPU; never fails). */
+int mm_device_count(void);
+
+/* ---- host-only mesh utilities (no GPU needed) ---------------------------------------- */
+
+/* Reverse Cuthill-McKee order of the node graph of T: perm[new] = old.
+ * Replaces nothing in the reference (escript keeps its own DOF order); used to make the
+ * device gathers local. */
+mm_status mm_rcm_permutation(int64_t N, const int32_t* T, int64_t E, int32_t* perm);
+
+/* Greedy element colouring: no two elements of one colour share a node.  colour[e] in
+ * [0, *ncolours).  Used so the assembly scatters are atomic-free. */
+mm_status mm_color_elements(int64_t N, const int32_t* T, int64_t E, int32_t* colour,
+                            int32_t* ncolours);
+
+/* ---- mesh handle ---------------------------------------------------------------------- */
+
+/* Build the device operators of one mesh: replaces escript2arrays
+ * (scripts/mapping.py:171-236) -- materials (scripts/materials.py:12-41), meas
+ * (scripts/escript_tools.py:13-17), exchange+anisotropy C and its exchange diagonal D
+ * (scripts/matrix.py:37-47, scripts/mapping.py:203-210), divergence dk and gradient gk
+ * (scripts/matrix.py:9-35), and the Poisson matrix with its boundary treatment
+ * (scripts/matrix.py:49-74, scripts/trafo.py:4-45). */
+mm_status mm_mesh_create(const double* X, int64_t N, const int32_t* T, const int32_t* tag,
+                         int64_t E, const mm_material* mats, int32_t nmats,
+                         const mm_options* opt, mm_mesh** out);
+mm_status mm_mesh_destroy(mm_mesh* mesh);
+mm_status mm_mesh_get_info(const mm_mesh* mesh, mm_mesh_info* info);
+
+/* Node measure meas [N] (mesh-file order) and the magnetic volume. */
+mm_status mm_get_meas(mm_mesh* mesh, double* meas, double* volume);
+
+/* Export the assembled operators as COO triplets in mesh-file order (parity checks).
+ * which: 0 S (Poisson, Dirichlet-modified), 1 exchange scalar (2A/V)K, 2..7 anisotropy
+ * blocks xx,xy,xz,yy,yz,zz, 8..10 dx,dy,dz, 11..13 gx,gy,gz.
+ * With rows == NULL only *nnz is returned. */
+mm_status mm_get_operator(mm_mesh* mesh, int32_t which, int64_t* nnz, int32_t* rows,
+                          int32_t* cols, double* vals);
+
+/* Set the solver state: m [3N] (required), u [N] (NULL: zeros), mbar [3N] the
+ * magnetisation M_inv projects with (NULL: m).  The full gradient carried between
+ * steps is reset to 0 as at scripts/loop.py:84. */
+mm_status mm_set_state(mm_mesh* mesh, const double* m, const double* u, const double* mbar);
+/* Read the state back; any pointer may be NULL. gfull [3N] is the last full gradient. */
+mm_status mm_get_state(mm_mesh* mesh, double* m, double* u, double* gfull);
+
+/* One energy + gradient evaluation, total_eg (scripts/energies.py:67-99), at the state's
+ * m with the state's u as PCG warm start; u and gfull in the state are updated.
+ * Outputs (NULL allowed): *energy, gproj [3N] = m x (g x m), *pcg_iters. */
+mm_status mm_energy_grad(mm_mesh* mesh, double h, const mm_solver_params* sp, double* energy,
+                         double* gproj, int64_t* pcg_iters);
+
+/* The M_inv preconditioner (scripts/loop.py:40-55) applied to g [3N]: z [3N]. Uses the
+ * state's mbar and gfull. */
+mm_status mm_apply_minv(mm_mesh* mesh, const mm_solver_params* sp, const double* g, double* z,
+                        int64_t* iters);
+
+/* One field step: hestenes_stiefel_ncg (scripts/minimizers.py:140-190) on the resident
+ * state at applied field h (T), then mh.  One persistent launch. */
+mm_status mm_minimize(mm_mesh* mesh, double h, const mm_solver_params* sp, mm_step_result* res);
+
+/* The field sweep, solve() + loop() (scripts/loop.py:71-142): starts from the state set by
+ * mm_set_state.  rec must hold max_steps rows; *nrec receives the rows written.  steps
+ * (NULL allowed) receives one mm_step_result per row.  cb may be NULL. */
+mm_status mm_loop(mm_mesh* mesh, const mm_loop_params* lp, const mm_solver_params* sp,
+                  mm_record* rec, int32_t* nrec, mm_step_result* steps, mm_snapshot_cb cb,
+                  void* user);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* MUMAG_B200_H */

@@ -1,0 +1,560 @@
+// C ABI of libmumag_b200.so (include/mumag_b200.h): mesh lifecycle, state transfer between
+// the reference's layout (interleaved m, mesh-file node order) and the device layout
+// (component planes, reverse Cuthill-McKee order), and the field-sweep driver that
+// replaces scripts/loop.py:71-142.
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstring>
+#include <memory>
+#include <new>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "device_mesh.h"
+
+struct mm_mesh {
+  mumag::DevMesh dm;
+};
+
+namespace mumag {
+
+namespace {
+thread_local std::string g_error;
+
+template <class T>
+void dalloc(T*& p, size_t n) {
+  MM_CK(cudaMalloc(reinterpret_cast<void**>(&p), sizeof(T) * (n ? n : 1)));
+}
+template <class T>
+void dfree(T*& p) {
+  if (p) cudaFree(p);
+  p = nullptr;
+}
+template <class T>
+void upload(T* d, const std::vector<T>& h, cudaStream_t st) {
+  if (!h.empty()) MM_CK(cudaMemcpyAsync(d, h.data(), sizeof(T) * h.size(), cudaMemcpyHostToDevice, st));
+}
+
+// file-order interleaved [3N] <-> device planes [3][Npad]
+void to_planes(const DevMesh& m, const double* in, std::vector<double>& out) {
+  const auto& h = m.h;
+  out.assign(3 * h.Npad, 0.0);
+  for (int64_t i = 0; i < h.N; ++i)
+    for (int q = 0; q < 3; ++q) out[q * h.Npad + h.iperm[i]] = in[3 * i + q];
+}
+void from_planes(const DevMesh& m, const std::vector<double>& in, double* out) {
+  const auto& h = m.h;
+  for (int64_t i = 0; i < h.N; ++i)
+    for (int q = 0; q < 3; ++q) out[3 * i + q] = in[q * h.Npad + h.iperm[i]];
+}
+void to_nodes(const DevMesh& m, const double* in, std::vector<double>& out) {
+  out.assign(m.h.Npad, 0.0);
+  for (int64_t i = 0; i < m.h.N; ++i) out[m.h.iperm[i]] = in[i];
+}
+void from_nodes(const DevMesh& m, const std::vector<double>& in, double* out) {
+  for (int64_t i = 0; i < m.h.N; ++i) out[i] = in[m.h.iperm[i]];
+}
+void d2h(std::vector<double>& h, const double* d, size_t n, cudaStream_t st) {
+  h.resize(n);
+  MM_CK(cudaMemcpyAsync(h.data(), d, sizeof(double) * n, cudaMemcpyDeviceToHost, st));
+  MM_CK(cudaStreamSynchronize(st));
+}
+
+void release(DevMesh& m) {
+  if (m.device >= 0) cudaSetDevice(m.device);
+  dfree(m.sl_off);
+  dfree(m.sl_w);
+  dfree(m.col);
+  dfree(m.rowlen);
+  dfree(m.vals);
+  dfree(m.diagS);
+  dfree(m.invdS);
+  dfree(m.Dex);
+  dfree(m.meas);
+  dfree(m.bnd);
+  dfree(m.Xd);
+  dfree(m.econn);
+  dfree(m.etag);
+  dfree(m.dmats);
+  dfree(m.ws);
+  dfree(m.bar);
+  dfree(m.red);
+  dfree(m.flags);
+  dfree(m.resd);
+  dfree(m.resi);
+  if (m.h_resd) cudaFreeHost(m.h_resd);
+  if (m.h_resi) cudaFreeHost(m.h_resi);
+  if (m.h_flags) cudaFreeHost(m.h_flags);
+  m.h_resd = nullptr;
+  m.h_resi = nullptr;
+  m.h_flags = nullptr;
+  if (m.stream) cudaStreamDestroy(m.stream);
+  m.stream = nullptr;
+}
+
+mm_status fail(mm_status st, const std::string& msg) {
+  g_error = msg;
+  return st;
+}
+
+#define API_BEGIN try {
+#define API_END                                                \
+  }                                                            \
+  catch (const mumag::CudaFailure& e) {                        \
+    return mumag::fail(MM_CUDA_ERROR, e.what());               \
+  }                                                            \
+  catch (const std::bad_alloc&) {                              \
+    return mumag::fail(MM_BAD_INPUT, "host allocation failed"); \
+  }                                                            \
+  catch (const std::exception& e) {                            \
+    return mumag::fail(MM_BAD_INPUT, e.what());                \
+  }
+
+void check_mesh(const mm_mesh* mesh) {
+  if (!mesh) throw std::runtime_error("mesh handle is NULL");
+}
+
+void check_params(const mm_solver_params* sp) {
+  if (!sp) throw std::runtime_error("solver parameters are NULL");
+  if (!(sp->tol_fun > 0) || !(sp->tol_u >= 0)) throw std::runtime_error("tolerances must be positive");
+  if (sp->max_pcg_iter < 0 || sp->max_ncg_iter < 1) throw std::runtime_error("iteration caps must be positive");
+}
+
+// Run one persistent launch and collect its status.
+mm_status run(DevMesh& m, const SolveArgs& a) {
+  MM_CK(cudaSetDevice(m.device));
+  MM_CK(solver_launch(m, a));
+  MM_CK(cudaMemcpyAsync(m.h_resd, m.resd, 2 * sizeof(double), cudaMemcpyDeviceToHost, m.stream));
+  MM_CK(cudaMemcpyAsync(m.h_resi, m.resi, 8 * sizeof(long long), cudaMemcpyDeviceToHost, m.stream));
+  MM_CK(cudaMemcpyAsync(m.h_flags, m.flags, 2 * sizeof(int), cudaMemcpyDeviceToHost, m.stream));
+  MM_CK(cudaStreamSynchronize(m.stream));
+  const int st = m.h_flags[FLAG_STATUS];
+  if (st == MM_TIMEOUT) return fail(MM_TIMEOUT, "a grid barrier of the persistent solver kernel timed out");
+  return st;
+}
+
+}  // namespace
+
+void set_error(const std::string& msg) { g_error = msg; }
+
+}  // namespace mumag
+
+using namespace mumag;
+
+extern "C" {
+
+const char* mm_version(void) { return "mumag_b200 0.1.0 (sm_100a)"; }
+
+const char* mm_last_error(void) { return g_error.c_str(); }
+
+void mm_default_options(mm_options* opt) {
+  if (!opt) return;
+  std::memset(opt, 0, sizeof(*opt));
+  opt->size = 1e-9;
+  opt->dirichlet_rhs = MM_DIRICHLET_RHS_REFERENCE;
+  opt->precision = MM_PREC_FP64;
+  opt->device = 0;
+  opt->grid_ctas = 0;
+  opt->block_threads = 0;
+  opt->reorder = 1;
+}
+
+void mm_default_solver_params(mm_solver_params* sp) {
+  if (!sp) return;
+  std::memset(sp, 0, sizeof(*sp));
+  sp->hdir[2] = 1.0;
+  sp->tol_fun = 1e-10;
+  sp->tol_u = 1e-10;
+  sp->precond_iter = 10;
+  sp->hmag_on = 1;
+  sp->mbar_mode = 0;
+  sp->max_pcg_iter = 10000;
+  sp->max_ncg_iter = 100000;
+}
+
+int mm_device_count(void) {
+  int n = 0;
+  if (cudaGetDeviceCount(&n) != cudaSuccess) {
+    cudaGetLastError();
+    return 0;
+  }
+  int ok = 0;
+  for (int d = 0; d < n; ++d) {
+    cudaDeviceProp p;
+    if (cudaGetDeviceProperties(&p, d) == cudaSuccess && p.major == 10) ++ok;
+  }
+  return ok;
+}
+
+mm_status mm_rcm_permutation(int64_t N, const int32_t* T, int64_t E, int32_t* perm) {
+  API_BEGIN
+  if (!T || !perm) throw std::runtime_error("NULL array");
+  auto p = rcm_order(N, T, E);
+  std::memcpy(perm, p.data(), sizeof(int32_t) * N);
+  return MM_OK;
+  API_END
+}
+
+mm_status mm_color_elements(int64_t N, const int32_t* T, int64_t E, int32_t* colour, int32_t* ncolours) {
+  API_BEGIN
+  if (!T || !colour || !ncolours) throw std::runtime_error("NULL array");
+  if (N <= 0 || E <= 0) throw std::runtime_error("mesh needs N > 0 nodes and E > 0 elements");
+  for (int64_t k = 0; k < 4 * E; ++k)
+    if (T[k] < 0 || T[k] >= N) throw std::runtime_error("element node index out of range");
+  *ncolours = greedy_colour(N, T, E, nullptr, colour);
+  return MM_OK;
+  API_END
+}
+
+mm_status mm_mesh_create(const double* X, int64_t N, const int32_t* T, const int32_t* tag, int64_t E,
+                         const mm_material* mats, int32_t nmats, const mm_options* opt, mm_mesh** out) {
+  API_BEGIN
+  if (!out) throw std::runtime_error("output handle pointer is NULL");
+  *out = nullptr;
+  if (!X || !T || !tag || !mats) throw std::runtime_error("NULL input array");
+  mm_options o;
+  mm_default_options(&o);
+  if (opt) o = *opt;
+  if (!(o.size > 0)) throw std::runtime_error("options.size must be positive");
+  for (int64_t i = 0; i < 3 * N; ++i)
+    if (!std::isfinite(X[i])) throw std::runtime_error("non-finite node coordinate");
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+    cudaGetLastError();
+    return fail(MM_NO_DEVICE, "no CUDA device");
+  }
+  if (o.device < 0 || o.device >= ndev) throw std::runtime_error("options.device out of range");
+  cudaDeviceProp prop;
+  MM_CK(cudaGetDeviceProperties(&prop, o.device));
+  if (prop.major != 10) return fail(MM_NO_DEVICE, "device is not sm_100 (B200): " + std::string(prop.name));
+  std::unique_ptr<mm_mesh> mesh(new mm_mesh());
+  DevMesh& m = mesh->dm;
+  m.device = o.device;
+  m.opt = o;
+  preprocess(X, N, T, tag, E, nmats, o.reorder != 0, m.h);
+  HostMesh& h = m.h;
+  m.ncolours = (int32_t)h.colour_off.size() - 1;
+  // materials, scripts/materials.py:17-35
+  const double mu0 = 4e-7 * M_PI;
+  m.mats.resize(h.tags.size());
+  for (size_t t = 0; t < h.tags.size(); ++t) {
+    const mm_material& r = mats[t];
+    MatRow mr{};
+    if (r.Js > 0) {
+      mr.u[0] = std::sin(r.theta) * std::cos(r.phi);
+      mr.u[1] = std::sin(r.theta) * std::sin(r.phi);
+      mr.u[2] = std::cos(r.theta);
+      mr.K = mu0 * r.K1;
+      mr.Js = r.Js;
+      mr.A = mu0 * r.A / (o.size * o.size);
+    }
+    m.mats[t] = mr;
+  }
+  try {
+    MM_CK(cudaSetDevice(m.device));
+    MM_CK(cudaStreamCreateWithFlags(&m.stream, cudaStreamNonBlocking));
+    dalloc(m.sl_off, h.sl_off.size());
+    dalloc(m.sl_w, h.sl_w.size());
+    dalloc(m.col, h.col.size());
+    dalloc(m.rowlen, h.rowlen.size());
+    dalloc(m.vals, (size_t)kNumPlanes * h.nent);
+    dalloc(m.diagS, h.Npad);
+    dalloc(m.invdS, h.Npad);
+    dalloc(m.Dex, h.Npad);
+    dalloc(m.meas, h.Npad);
+    dalloc(m.bnd, h.Npad);
+    dalloc(m.Xd, h.Xd.size());
+    dalloc(m.econn, h.econn.size());
+    dalloc(m.etag, h.etag.size());
+    dalloc(m.dmats, m.mats.size());
+    upload(m.sl_off, h.sl_off, m.stream);
+    upload(m.sl_w, h.sl_w, m.stream);
+    upload(m.col, h.col, m.stream);
+    upload(m.rowlen, h.rowlen, m.stream);
+    upload(m.bnd, h.bnd, m.stream);
+    upload(m.Xd, h.Xd, m.stream);
+    upload(m.econn, h.econn, m.stream);
+    upload(m.etag, h.etag, m.stream);
+    upload(m.dmats, m.mats, m.stream);
+    assemble_operators(m);
+    // solver state: 12 three-vectors and 5 node vectors
+    const size_t np = h.Npad;
+    dalloc(m.ws, 41 * np);
+    MM_CK(cudaMemsetAsync(m.ws, 0, sizeof(double) * 41 * np, m.stream));
+    double* p = m.ws;
+    double** v3[] = {&m.x, &m.x1, &m.g, &m.g1, &m.d, &m.gf, &m.mbar, &m.zp, &m.tr, &m.tz, &m.td, &m.tBd};
+    for (double** q : v3) {
+      *q = p;
+      p += 3 * np;
+    }
+    double** v1[] = {&m.u, &m.pr, &m.pz, &m.pp, &m.pq};
+    for (double** q : v1) {
+      *q = p;
+      p += np;
+    }
+    solver_configure(m);
+    dalloc(m.bar, 1);
+    dalloc(m.red, (size_t)2 * kMaxRed * m.grid);
+    dalloc(m.flags, 2);
+    dalloc(m.resd, 2);
+    dalloc(m.resi, 8);
+    MM_CK(cudaHostAlloc(reinterpret_cast<void**>(&m.h_resd), 2 * sizeof(double), cudaHostAllocDefault));
+    MM_CK(cudaHostAlloc(reinterpret_cast<void**>(&m.h_resi), 8 * sizeof(long long), cudaHostAllocDefault));
+    MM_CK(cudaHostAlloc(reinterpret_cast<void**>(&m.h_flags), 2 * sizeof(int), cudaHostAllocDefault));
+    MM_CK(cudaStreamSynchronize(m.stream));
+  } catch (...) {
+    release(m);
+    throw;
+  }
+  *out = mesh.release();
+  return MM_OK;
+  API_END
+}
+
+mm_status mm_mesh_destroy(mm_mesh* mesh) {
+  if (!mesh) return MM_OK;
+  release(mesh->dm);
+  delete mesh;
+  return MM_OK;
+}
+
+mm_status mm_mesh_get_info(const mm_mesh* mesh, mm_mesh_info* info) {
+  API_BEGIN
+  check_mesh(mesh);
+  if (!info) throw std::runtime_error("info is NULL");
+  const DevMesh& m = mesh->dm;
+  info->nodes = m.h.N;
+  info->elements = m.h.E;
+  info->sell_slices = m.h.nslices;
+  info->sell_entries = m.h.nent;
+  info->nnz = m.h.nnz;
+  info->colours = m.ncolours;
+  info->airbox = m.h.airbox;
+  info->grid_ctas = m.grid;
+  info->block_threads = m.block;
+  int64_t nb = 0;
+  for (auto b : m.h.bnd) nb += b;
+  info->dirichlet_nodes = nb;
+  info->volume = m.V;
+  info->bandwidth_before = (double)m.h.bandwidth_before;
+  info->bandwidth_after = (double)m.h.bandwidth_after;
+  return MM_OK;
+  API_END
+}
+
+mm_status mm_get_meas(mm_mesh* mesh, double* meas, double* volume) {
+  API_BEGIN
+  check_mesh(mesh);
+  DevMesh& m = mesh->dm;
+  MM_CK(cudaSetDevice(m.device));
+  if (meas) {
+    std::vector<double> t;
+    d2h(t, m.meas, m.h.Npad, m.stream);
+    from_nodes(m, t, meas);
+  }
+  if (volume) *volume = m.V;
+  return MM_OK;
+  API_END
+}
+
+mm_status mm_get_operator(mm_mesh* mesh, int32_t which, int64_t* nnz, int32_t* rows, int32_t* cols, double* vals) {
+  API_BEGIN
+  check_mesh(mesh);
+  if (which < 0 || which >= kNumPlanes) throw std::runtime_error("operator index out of range");
+  if (!nnz) throw std::runtime_error("nnz is NULL");
+  DevMesh& m = mesh->dm;
+  const HostMesh& h = m.h;
+  *nnz = h.nnz;
+  if (!rows) return MM_OK;
+  if (!cols || !vals) throw std::runtime_error("NULL output array");
+  MM_CK(cudaSetDevice(m.device));
+  std::vector<double> pv;
+  d2h(pv, m.vals + (size_t)which * h.nent, h.nent, m.stream);
+  int64_t q = 0;
+  for (int64_t s = 0; s < h.nslices; ++s)
+    for (int l = 0; l < kSlice; ++l) {
+      const int64_t i = s * kSlice + l;
+      if (i >= h.N) continue;
+      for (int32_t k = 0; k < h.rowlen[i]; ++k) {
+        const int64_t e = h.sl_off[s] + (int64_t)k * kSlice + l;
+        rows[q] = h.perm[i];
+        cols[q] = h.perm[h.col[e]];
+        vals[q] = pv[e];
+        ++q;
+      }
+    }
+  return MM_OK;
+  API_END
+}
+
+mm_status mm_set_state(mm_mesh* mesh, const double* mv, const double* uv, const double* mbar) {
+  API_BEGIN
+  check_mesh(mesh);
+  if (!mv) throw std::runtime_error("m is NULL");
+  DevMesh& m = mesh->dm;
+  const size_t np = m.h.Npad;
+  for (int64_t i = 0; i < 3 * m.h.N; ++i)
+    if (!std::isfinite(mv[i]) || (mbar && !std::isfinite(mbar[i]))) throw std::runtime_error("non-finite magnetisation");
+  MM_CK(cudaSetDevice(m.device));
+  std::vector<double> t;
+  to_planes(m, mv, t);
+  MM_CK(cudaMemcpyAsync(m.x, t.data(), sizeof(double) * 3 * np, cudaMemcpyHostToDevice, m.stream));
+  if (mbar) to_planes(m, mbar, t);
+  MM_CK(cudaMemcpyAsync(m.mbar, t.data(), sizeof(double) * 3 * np, cudaMemcpyHostToDevice, m.stream));
+  std::vector<double> tu(np, 0.0);
+  if (uv) {
+    for (int64_t i = 0; i < m.h.N; ++i)
+      if (!std::isfinite(uv[i])) throw std::runtime_error("non-finite potential");
+    to_nodes(m, uv, tu);
+  }
+  MM_CK(cudaMemcpyAsync(m.u, tu.data(), sizeof(double) * np, cudaMemcpyHostToDevice, m.stream));
+  MM_CK(cudaMemsetAsync(m.gf, 0, sizeof(double) * 3 * np, m.stream));
+  MM_CK(cudaStreamSynchronize(m.stream));
+  return MM_OK;
+  API_END
+}
+
+mm_status mm_get_state(mm_mesh* mesh, double* mv, double* uv, double* gfull) {
+  API_BEGIN
+  check_mesh(mesh);
+  DevMesh& m = mesh->dm;
+  const size_t np = m.h.Npad;
+  MM_CK(cudaSetDevice(m.device));
+  std::vector<double> t;
+  if (mv) {
+    d2h(t, m.x, 3 * np, m.stream);
+    from_planes(m, t, mv);
+  }
+  if (uv) {
+    d2h(t, m.u, np, m.stream);
+    from_nodes(m, t, uv);
+  }
+  if (gfull) {
+    d2h(t, m.gf, 3 * np, m.stream);
+    from_planes(m, t, gfull);
+  }
+  return MM_OK;
+  API_END
+}
+
+mm_status mm_energy_grad(mm_mesh* mesh, double h, const mm_solver_params* sp, double* energy, double* gproj,
+                         int64_t* pcg_iters) {
+  API_BEGIN
+  check_mesh(mesh);
+  check_params(sp);
+  DevMesh& m = mesh->dm;
+  mm_status st = run(m, solver_args(m, MODE_EVAL, h, *sp));
+  if (energy) *energy = m.h_resd[0];
+  if (pcg_iters) *pcg_iters = m.h_resi[2];
+  if (gproj) {
+    std::vector<double> t;
+    d2h(t, m.g, 3 * m.h.Npad, m.stream);
+    from_planes(m, t, gproj);
+  }
+  if (st == MM_NONFINITE) return fail(st, "energy is not finite");
+  return st;
+  API_END
+}
+
+mm_status mm_apply_minv(mm_mesh* mesh, const mm_solver_params* sp, const double* g, double* z, int64_t* iters) {
+  API_BEGIN
+  check_mesh(mesh);
+  check_params(sp);
+  if (!g || !z) throw std::runtime_error("NULL vector");
+  DevMesh& m = mesh->dm;
+  const size_t np = m.h.Npad;
+  MM_CK(cudaSetDevice(m.device));
+  std::vector<double> t;
+  to_planes(m, g, t);
+  MM_CK(cudaMemcpyAsync(m.g, t.data(), sizeof(double) * 3 * np, cudaMemcpyHostToDevice, m.stream));
+  mm_status st = run(m, solver_args(m, MODE_MINV, 0.0, *sp));
+  d2h(t, m.zp, 3 * np, m.stream);
+  from_planes(m, t, z);
+  if (iters) *iters = m.h_resi[4];
+  return st;
+  API_END
+}
+
+mm_status mm_minimize(mm_mesh* mesh, double h, const mm_solver_params* sp, mm_step_result* res) {
+  API_BEGIN
+  check_mesh(mesh);
+  check_params(sp);
+  DevMesh& m = mesh->dm;
+  mm_status st = run(m, solver_args(m, MODE_MINIMIZE, h, *sp));
+  if (res) {
+    res->energy = m.h_resd[0];
+    res->mh = m.h_resd[1];
+    res->ncg_iters = m.h_resi[0];
+    res->evals = m.h_resi[1];
+    res->pcg_iters = m.h_resi[2];
+    res->ls_shrinks = m.h_resi[3];
+    res->minv_iters = m.h_resi[4];
+    res->status = st;
+  }
+  if (st == MM_NONFINITE) return fail(st, "energy is not finite");
+  return st;
+  API_END
+}
+
+mm_status mm_loop(mm_mesh* mesh, const mm_loop_params* lp, const mm_solver_params* sp, mm_record* rec,
+                  int32_t* nrec, mm_step_result* steps, mm_snapshot_cb cb, void* user) {
+  API_BEGIN
+  check_mesh(mesh);
+  check_params(sp);
+  if (!lp || !rec || !nrec) throw std::runtime_error("NULL loop argument");
+  if (!(lp->hstep != 0.0) || !std::isfinite(lp->hstart) || !std::isfinite(lp->hfinal))
+    throw std::runtime_error("invalid field sweep");
+  DevMesh& m = mesh->dm;
+  // scripts/loop.py:126-131
+  int64_t nmax = (int64_t)(std::fabs(lp->hfinal - lp->hstart) / std::fabs(lp->hstep)) + 1;
+  if (lp->max_steps > 0) nmax = std::min<int64_t>(nmax, lp->max_steps);
+  *nrec = 0;
+  double mh = 1.7976931348623157e308, last_saved = mh;
+  int counter = 0;
+  double hext = lp->hstart;
+  std::vector<double> tm, tu, fm, fu;
+  for (int64_t idx = 0; idx < nmax && mh > lp->mfinal; ++idx) {
+    mm_step_result r{};
+    mm_status st = run(m, solver_args(m, MODE_MINIMIZE, hext, *sp));
+    r.energy = m.h_resd[0];
+    r.mh = m.h_resd[1];
+    r.ncg_iters = m.h_resi[0];
+    r.evals = m.h_resi[1];
+    r.pcg_iters = m.h_resi[2];
+    r.ls_shrinks = m.h_resi[3];
+    r.minv_iters = m.h_resi[4];
+    r.status = st;
+    if (st != MM_OK) {
+      if (steps) steps[idx] = r;
+      return st == MM_NONFINITE ? fail(st, "energy is not finite at field " + std::to_string(hext)) : st;
+    }
+    mh = r.mh;
+    if ((last_saved - mh) > lp->mstep) {  // scripts/loop.py:103-116
+      counter += 1;
+      last_saved = mh;
+      if (cb) {
+        d2h(tm, m.x, 3 * m.h.Npad, m.stream);
+        d2h(tu, m.u, m.h.Npad, m.stream);
+        fm.resize(3 * m.h.N);
+        fu.resize(m.h.N);
+        from_planes(m, tm, fm.data());
+        from_nodes(m, tu, fu.data());
+        if (cb(counter, fm.data(), fu.data(), m.h.N, user) != 0)
+          return fail(MM_BAD_INPUT, "snapshot callback aborted the loop");
+      }
+    }
+    rec[idx].counter = counter;
+    rec[idx].hext = hext;
+    rec[idx].mh = mh;
+    rec[idx].energy = r.energy;
+    if (steps) steps[idx] = r;
+    *nrec = (int32_t)(idx + 1);
+    hext = hext + lp->hstep;
+  }
+  return MM_OK;
+  API_END
+}
+
+}  // extern "C"

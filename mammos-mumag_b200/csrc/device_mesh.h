@@ -1,0 +1,110 @@
+// Device-resident mesh, operators and solver state, plus the launchers of the CUDA
+// kernels (assemble.cu, solver.cu).  Host code only; no device code here.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "mumag_internal.h"
+
+namespace mumag {
+
+// A failed CUDA runtime call (mapped to MM_CUDA_ERROR at the C ABI).
+struct CudaFailure : std::runtime_error {
+  using std::runtime_error::runtime_error;
+};
+
+#define MM_CK(call)                                                                          \
+  do {                                                                                       \
+    cudaError_t e_ = (call);                                                                 \
+    if (e_ != cudaSuccess)                                                                   \
+      throw ::mumag::CudaFailure(std::string(#call) + ": " + cudaGetErrorString(e_) + " (" + \
+                                 __FILE__ + ":" + std::to_string(__LINE__) + ")");           \
+  } while (0)
+
+// Materials per element tag, scripts/materials.py:17-35: Js [T], K = mu0*K1,
+// A = mu0*A/size^2, easy axis u.  All zero for Js <= 0.
+struct MatRow {
+  double Js, K, A, u[3];
+};
+
+// Arguments of the persistent solver kernel (passed by value, __grid_constant__).
+struct SolveArgs {
+  // SELL-32 pattern and operator planes (plane stride nent)
+  const int64_t* sl_off;
+  const int32_t* sl_w;
+  const int32_t* col;
+  const double* vals;  // [kNumPlanes][nent]
+  int64_t nent;
+  const double* invdS;
+  const double* Dex;
+  const double* meas;
+  int32_t nslices, Npad;
+  double V;
+  // vectors; 3-vectors are 3 planes of Npad
+  double *x, *x1, *g, *g1, *d, *gf, *mbar, *zp, *tr, *tz, *td, *tBd;
+  double *u, *pr, *pz, *pp, *pq;
+  // grid synchronisation
+  unsigned long long* bar;  // arrival counter, zeroed before each launch
+  double* red;              // [2][kMaxRed][gridDim.x] reduction partials
+  int* flags;               // [0] abort, [1] status
+  // control
+  int mode;  // 0 energy+gradient, 1 M_inv, 2 minimise (one field step)
+  double h, hdir[3], tol_fun, sqrt_tol, cbrt_tol, tol_u;
+  int precond_iter, hmag_on, mbar_current, max_pcg, max_ncg;
+  // results
+  double* resd;     // [0] energy, [1] mh
+  long long* resi;  // [0] ncg iters, [1] evals, [2] pcg iters, [3] ls shrinks, [4] minv iters
+};
+
+enum { MODE_EVAL = 0, MODE_MINV = 1, MODE_MINIMIZE = 2 };
+enum { FLAG_ABORT = 0, FLAG_STATUS = 1 };
+
+struct DevMesh {
+  int device = 0;
+  HostMesh h;
+  mm_options opt{};
+  cudaStream_t stream = nullptr;
+  std::vector<MatRow> mats;
+  int32_t ncolours = 0;
+  double V = 0.0;
+  // pattern + operators
+  int64_t* sl_off = nullptr;
+  int32_t* sl_w = nullptr;
+  int32_t* col = nullptr;
+  int32_t* rowlen = nullptr;
+  double* vals = nullptr;
+  double *diagS = nullptr, *invdS = nullptr, *Dex = nullptr, *meas = nullptr;
+  uint8_t* bnd = nullptr;
+  double* Xd = nullptr;
+  int32_t *econn = nullptr, *etag = nullptr;
+  MatRow* dmats = nullptr;
+  // state and workspace
+  double* ws = nullptr;  // all solver vectors
+  double *x, *x1, *g, *g1, *d, *gf, *mbar, *zp, *tr, *tz, *td, *tBd;
+  double *u, *pr, *pz, *pp, *pq;
+  unsigned long long* bar = nullptr;
+  double* red = nullptr;
+  int* flags = nullptr;
+  double* resd = nullptr;
+  long long* resi = nullptr;
+  // pinned host mirrors of the results
+  double* h_resd = nullptr;
+  long long* h_resi = nullptr;
+  int* h_flags = nullptr;
+  // launch shape of the persistent kernel
+  int grid = 0, block = 0;
+};
+
+// assemble.cu
+void assemble_operators(DevMesh& m);
+// solver.cu
+void solver_configure(DevMesh& m);
+cudaError_t solver_launch(DevMesh& m, const SolveArgs& a);
+SolveArgs solver_args(const DevMesh& m, int mode, double h, const mm_solver_params& sp);
+
+}  // namespace mumag

@@ -1,0 +1,821 @@
+// The persistent field-step kernel.
+//
+// One cooperative launch runs one whole field step of the reference's solver core on the
+// device: hestenes_stiefel_ncg (scripts/minimizers.py:140-190) with its line search
+// (:92-137), the M_inv preconditioner (scripts/loop.py:40-55, truncated PCG of
+// scripts/solvers.py:7-131) and, inside every energy evaluation (scripts/energies.py:67-99),
+// the Jacobi-PCG Poisson solve of jax.scipy.sparse.linalg.cg (scripts/solvers.py:221-231).
+//
+// Every CTA owns a contiguous range of SELL-32 slices (32 device-order rows each, one warp
+// per slice, lane = row).  Node-local vector work touches only the CTA's own rows;
+// operator rows gather neighbours written by other CTAs, so a grid barrier separates a
+// producer from the next gather.  Scalars come from grid reductions whose partials every
+// CTA sums in the same fixed order, so every CTA sees bit-identical scalars and takes the
+// same branches: the control flow of the reference runs redundantly in all CTAs.
+//
+// Two algebraic rewrites save one grid barrier per inner iteration; both are exact in
+// exact arithmetic: the PCG keeps q = S p up to date as q <- S z + beta q, and the
+// truncated CG keeps B d as B d <- -B z + beta B d.
+//
+// Every wait on another CTA is bounded; on timeout the kernel records MM_TIMEOUT, raises
+// the abort flag and all CTAs return.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cfloat>
+#include <cmath>
+#include <stdexcept>
+#include <string>
+
+#include "device_mesh.h"
+
+namespace mumag {
+
+namespace {
+
+constexpr unsigned kSpinLimit = 1u << 23;  // bounded wait per barrier (seconds)
+
+struct Sync {
+  unsigned long long* bar;
+  double* red;
+  int* flags;
+  unsigned long long epoch;
+  int nblk, blk, slot;
+};
+
+__device__ __forceinline__ unsigned long long ld_acquire_u64(const unsigned long long* p) {
+  unsigned long long v;
+  asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+  return v;
+}
+
+__device__ __forceinline__ void red_release_add_u64(unsigned long long* p, unsigned long long v) {
+  asm volatile("red.release.gpu.global.add.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
+
+// Grid-wide barrier; false if the kernel is aborting.
+__device__ bool grid_barrier(Sync& s) {
+  __shared__ int sh_abort;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    s.epoch += 1;
+    const unsigned long long target = s.epoch * (unsigned long long)s.nblk;
+    __threadfence();
+    red_release_add_u64(s.bar, 1ull);
+    int ab = 0;
+    unsigned it = 0;
+    while (ld_acquire_u64(s.bar) < target) {
+      if (*((volatile int*)&s.flags[FLAG_ABORT])) {
+        ab = 1;
+        break;
+      }
+      if (++it > kSpinLimit) {
+        atomicCAS(&s.flags[FLAG_STATUS], 0, (int)MM_TIMEOUT);
+        atomicExch(&s.flags[FLAG_ABORT], 1);
+        ab = 1;
+        break;
+      }
+      if (it > 32) __nanosleep(it > 4096 ? 256 : 32);
+    }
+    __threadfence();
+    sh_abort = ab;
+  }
+  __syncthreads();
+  return sh_abort == 0;
+}
+
+__device__ __forceinline__ double warp_sum(double v) {
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+__device__ __forceinline__ double warp_max(double v) {
+  for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+  return v;
+}
+
+// Deterministic grid reduction of K values; bit k of maxmask selects max instead of sum.
+// On return v[] holds the grid totals, identical in every thread of every CTA.
+template <int K>
+__device__ bool grid_reduce(Sync& s, double (&v)[K], unsigned maxmask) {
+  __shared__ double sh[32][kMaxRed];
+  __shared__ double res[kMaxRed];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+#pragma unroll
+  for (int k = 0; k < K; ++k) {
+    const double w = ((maxmask >> k) & 1) ? warp_max(v[k]) : warp_sum(v[k]);
+    if (lane == 0) sh[warp][k] = w;
+  }
+  __syncthreads();
+  if (threadIdx.x < K) {
+    const int k = threadIdx.x;
+    double a = sh[0][k];
+    for (int w = 1; w < nw; ++w) a = ((maxmask >> k) & 1) ? fmax(a, sh[w][k]) : a + sh[w][k];
+    s.red[((size_t)s.slot * kMaxRed + k) * s.nblk + s.blk] = a;
+  }
+  if (!grid_barrier(s)) return false;
+  if (warp == 0) {
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+      const bool mx = (maxmask >> k) & 1;
+      double a = mx ? 0.0 : 0.0;
+      const double* p = s.red + ((size_t)s.slot * kMaxRed + k) * s.nblk;
+      for (int b = lane; b < s.nblk; b += 32) {
+        const double t = __ldcg(p + b);
+        a = mx ? fmax(a, t) : a + t;
+      }
+      a = mx ? warp_max(a) : warp_sum(a);
+      if (lane == 0) res[k] = a;
+    }
+  }
+  __syncthreads();
+#pragma unroll
+  for (int k = 0; k < K; ++k) v[k] = res[k];
+  s.slot ^= 1;
+  return true;
+}
+
+// cross(m, cross(g, m)), scripts/energies.py:61-65
+__device__ __forceinline__ void project(const double m[3], const double g[3], double o[3]) {
+  const double c0 = g[1] * m[2] - g[2] * m[1];
+  const double c1 = g[2] * m[0] - g[0] * m[2];
+  const double c2 = g[0] * m[1] - g[1] * m[0];
+  o[0] = m[1] * c2 - m[2] * c1;
+  o[1] = m[2] * c0 - m[0] * c2;
+  o[2] = m[0] * c1 - m[1] * c0;
+}
+
+struct Ctx {
+  const SolveArgs& a;
+  Sync sy;
+  int s0, s1, warp, nwarps, lane;
+  long long evals = 0, pcg_iters = 0, minv_iters = 0, shrinks = 0;
+  __device__ Ctx(const SolveArgs& args) : a(args) {}
+};
+
+#define FOR_ROWS(c)                                                       \
+  for (int s_ = (c).s0 + (c).warp; s_ < (c).s1; s_ += (c).nwarps) {      \
+    const int i = s_ * 32 + (c).lane;                                     \
+    const int64_t off_ = (c).a.sl_off[s_] + (c).lane;                     \
+    const int w_ = (c).a.sl_w[s_];
+#define END_ROWS }
+#define ENTRY(k) (off_ + 32 * (int64_t)(k))
+#define CHECK(x) \
+  if (!(x)) return false
+
+__device__ __forceinline__ const double* plane(const SolveArgs& a, int p) { return a.vals + (size_t)p * a.nent; }
+
+// C v at row i (exchange scalar + anisotropy blocks), v a 3-vector
+__device__ __forceinline__ void apply_C_row(const SolveArgs& a, const double* v, int64_t off, int w,
+                                            double o[3]) {
+  const double* Aex = plane(a, P_AEX);
+  const double* K = plane(a, P_K);
+  const int64_t ps = a.nent;
+  const int n = a.Npad;
+  double o0 = 0, o1 = 0, o2 = 0;
+  for (int k = 0; k < w; ++k) {
+    const int64_t e = off + 32 * (int64_t)k;
+    const int j = __ldg(a.col + e);
+    const double v0 = v[j], v1 = v[n + j], v2 = v[2 * n + j];
+    const double ax = __ldg(Aex + e);
+    const double k0 = __ldg(K + e), k1 = __ldg(K + ps + e), k2 = __ldg(K + 2 * ps + e);
+    const double k3 = __ldg(K + 3 * ps + e), k4 = __ldg(K + 4 * ps + e), k5 = __ldg(K + 5 * ps + e);
+    o0 += ax * v0 + (k0 * v0 + k1 * v1 + k2 * v2);
+    o1 += ax * v1 + (k1 * v0 + k3 * v1 + k4 * v2);
+    o2 += ax * v2 + (k2 * v0 + k4 * v1 + k5 * v2);
+  }
+  o[0] = o0;
+  o[1] = o1;
+  o[2] = o2;
+}
+
+// ---------------------------------------------------------------------------------------
+// Poisson PCG (jax.scipy.sparse.linalg.cg semantics, M = x * (1/diag S))
+// ---------------------------------------------------------------------------------------
+// b = sum_k dk x_k, r = b - S u, z = r/diag, p = z; returns gamma = r.z, rr = r.r, bb = b.b
+__device__ bool pcg_begin(Ctx& c, const double* x, double& gamma, double& rr, double& bb) {
+  const SolveArgs& a = c.a;
+  const double* S = plane(a, P_S);
+  const double* Dk = plane(a, P_D);
+  const int64_t ps = a.nent;
+  const int n = a.Npad;
+  double pg = 0, pr2 = 0, pb = 0;
+  FOR_ROWS(c)
+  double b = 0, su = 0;
+  for (int k = 0; k < w_; ++k) {
+    const int64_t e = ENTRY(k);
+    const int j = __ldg(a.col + e);
+    b += __ldg(Dk + e) * x[j] + __ldg(Dk + ps + e) * x[n + j] + __ldg(Dk + 2 * ps + e) * x[2 * n + j];
+    su += __ldg(S + e) * a.u[j];
+  }
+  const double r = b - su;
+  const double z = r * __ldg(a.invdS + i);
+  a.pr[i] = r;
+  a.pz[i] = z;
+  a.pp[i] = z;
+  pg += r * z;
+  pr2 += r * r;
+  pb += b * b;
+  END_ROWS
+  double v[3] = {pg, pr2, pb};
+  CHECK(grid_reduce<3>(c.sy, v, 0u));
+  gamma = v[0];
+  rr = v[1];
+  bb = v[2];
+  return true;
+}
+
+// first: q = S p.  otherwise: q = S z + beta q, p = z + beta p.  returns p.q
+__device__ bool pcg_direction(Ctx& c, bool first, double beta, double& pq) {
+  const SolveArgs& a = c.a;
+  const double* S = plane(a, P_S);
+  const double* src = first ? a.pp : a.pz;
+  double part = 0;
+  FOR_ROWS(c)
+  double acc = 0;
+  for (int k = 0; k < w_; ++k) {
+    const int64_t e = ENTRY(k);
+    acc += __ldg(S + e) * src[__ldg(a.col + e)];
+  }
+  double p, q;
+  if (first) {
+    p = a.pp[i];
+    q = acc;
+  } else {
+    q = acc + beta * a.pq[i];
+    p = a.pz[i] + beta * a.pp[i];
+    a.pp[i] = p;
+  }
+  a.pq[i] = q;
+  part += p * q;
+  END_ROWS
+  double v[1] = {part};
+  CHECK(grid_reduce<1>(c.sy, v, 0u));
+  pq = v[0];
+  return true;
+}
+
+// u += alpha p, r -= alpha q, z = r/diag; returns gamma' = r.z, rr = r.r
+__device__ bool pcg_update(Ctx& c, double alpha, double& gamma, double& rr) {
+  const SolveArgs& a = c.a;
+  double pg = 0, pr2 = 0;
+  FOR_ROWS(c)
+  (void)off_;
+  (void)w_;
+  a.u[i] = a.u[i] + alpha * a.pp[i];
+  const double r = a.pr[i] - alpha * a.pq[i];
+  const double z = r * __ldg(a.invdS + i);
+  a.pr[i] = r;
+  a.pz[i] = z;
+  pg += r * z;
+  pr2 += r * r;
+  END_ROWS
+  double v[2] = {pg, pr2};
+  CHECK(grid_reduce<2>(c.sy, v, 0u));
+  gamma = v[0];
+  rr = v[1];
+  return true;
+}
+
+__device__ bool pcg_solve(Ctx& c, const double* x) {
+  const SolveArgs& a = c.a;
+  double gamma, rr, bb, pq;
+  CHECK(pcg_begin(c, x, gamma, rr, bb));
+  const double atol2 = fmax(a.tol_u * a.tol_u * bb, 0.0);
+  int k = 0;
+  if (!(rr > atol2 && k < a.max_pcg)) return true;
+  CHECK(pcg_direction(c, true, 0.0, pq));
+  for (;;) {
+    const double alpha = gamma / pq;
+    double g2;
+    CHECK(pcg_update(c, alpha, g2, rr));
+    ++k;
+    if (!(rr > atol2 && k < a.max_pcg)) break;
+    const double beta = g2 / gamma;
+    gamma = g2;
+    CHECK(pcg_direction(c, false, beta, pq));
+  }
+  c.pcg_iters += k;
+  return true;
+}
+
+// ---------------------------------------------------------------------------------------
+// total_eg, scripts/energies.py:67-99
+// ---------------------------------------------------------------------------------------
+struct EvalOut {
+  double E, gd, dxinf, xinf, ginf;
+};
+
+// Energy and gradient at x (all CTAs' x complete).  Writes gout = projected gradient and
+// gf = full gradient; u is the PCG solution (warm-started from the previous u).  Extras:
+// gd = gout.d (d may be null), dxinf = max|x - xref|, xinf = max|x|, ginf = max|gout|.
+__device__ bool eval(Ctx& c, const double* x, const double* xref, const double* d, double* gout, EvalOut& o) {
+  const SolveArgs& a = c.a;
+  if (a.hmag_on > 0) CHECK(pcg_solve(c, x));
+  const int n = a.Npad;
+  const double* G = plane(a, P_G);
+  const int64_t ps = a.nent;
+  const double cz0 = (-a.h * a.hdir[0]) / a.V;
+  const double cz1 = (-a.h * a.hdir[1]) / a.V;
+  const double cz2 = (-a.h * a.hdir[2]) / a.V;
+  double pE = 0, pgd = 0, pdx = 0, px = 0, pgi = 0;
+  FOR_ROWS(c)
+  double gc[3];
+  apply_C_row(a, x, off_, w_, gc);
+  double gh0 = 0, gh1 = 0, gh2 = 0;
+  if (a.hmag_on > 0) {
+    for (int k = 0; k < w_; ++k) {
+      const int64_t e = ENTRY(k);
+      const double uj = a.u[__ldg(a.col + e)];
+      gh0 += __ldg(G + e) * uj;
+      gh1 += __ldg(G + ps + e) * uj;
+      gh2 += __ldg(G + 2 * ps + e) * uj;
+    }
+  }
+  const double mi = __ldg(a.meas + i);
+  const double xi[3] = {x[i], x[n + i], x[2 * n + i]};
+  const double gz[3] = {cz0 * mi, cz1 * mi, cz2 * mi};
+  const double gh[3] = {gh0, gh1, gh2};
+  double gfl[3], gp[3];
+  for (int q = 0; q < 3; ++q) gfl[q] = (gz[q] + gc[q]) + gh[q];
+  pE += (xi[0] * gz[0] + xi[1] * gz[1] + xi[2] * gz[2]) +
+        0.5 * (xi[0] * gc[0] + xi[1] * gc[1] + xi[2] * gc[2]) +
+        0.5 * (xi[0] * gh[0] + xi[1] * gh[1] + xi[2] * gh[2]);
+  project(xi, gfl, gp);
+  for (int q = 0; q < 3; ++q) {
+    gout[q * n + i] = gp[q];
+    a.gf[q * n + i] = gfl[q];
+    if (d) pgd += gp[q] * d[q * n + i];
+    pdx = fmax(pdx, fabs(xi[q] - xref[q * n + i]));
+    px = fmax(px, fabs(xi[q]));
+    pgi = fmax(pgi, fabs(gp[q]));
+  }
+  END_ROWS
+  double v[5] = {pE, pgd, pdx, px, pgi};
+  CHECK(grid_reduce<5>(c.sy, v, 0x1Cu));
+  o.E = v[0];
+  o.gd = v[1];
+  o.dxinf = v[2];
+  o.xinf = v[3];
+  o.ginf = v[4];
+  c.evals += 1;
+  return true;
+}
+
+// xout = normalize(x + alpha d) per node (scripts/jax_tools.py:4-18), then a barrier so
+// the next operator gathers see all of xout.
+__device__ bool step_normalize(Ctx& c, double* xout, const double* x, double alpha, const double* d) {
+  const int n = c.a.Npad;
+  FOR_ROWS(c)
+  (void)off_;
+  (void)w_;
+  const double v0 = x[i] + alpha * d[i];
+  const double v1 = x[n + i] + alpha * d[n + i];
+  const double v2 = x[2 * n + i] + alpha * d[2 * n + i];
+  double nr = sqrt(v0 * v0 + v1 * v1 + v2 * v2);
+  if (nr == 0.0) nr = 1.0;
+  xout[i] = v0 / nr;
+  xout[n + i] = v1 / nr;
+  xout[2 * n + i] = v2 / nr;
+  END_ROWS
+  return grid_barrier(c.sy);
+}
+
+// ---------------------------------------------------------------------------------------
+// M_inv, scripts/loop.py:40-55 -> truncated_cg_diag_precond_jit, scripts/solvers.py:7-131
+// A v = mbar x ((C v) x mbar) - (mbar . gf) v,  D = exchange diagonal
+// ---------------------------------------------------------------------------------------
+__device__ __forceinline__ void apply_A_row(const SolveArgs& a, const double* mb, const double* v, int i,
+                                            int64_t off, int w, double o[3]) {
+  const int n = a.Npad;
+  double cv[3];
+  apply_C_row(a, v, off, w, cv);
+  const double m[3] = {mb[i], mb[n + i], mb[2 * n + i]};
+  const double md = m[0] * a.gf[i] + m[1] * a.gf[n + i] + m[2] * a.gf[2 * n + i];
+  double pr[3];
+  project(m, cv, pr);
+  o[0] = pr[0] - md * v[i];
+  o[1] = pr[1] - md * v[n + i];
+  o[2] = pr[2] - md * v[2 * n + i];
+}
+
+// zout = M_inv(g): p with A p ~ g, or g itself when p stays zero.
+__device__ bool minv(Ctx& c, const double* g, const double* mb, double* zout) {
+  const SolveArgs& a = c.a;
+  const int n = a.Npad;
+  if (a.precond_iter <= 0) {
+    FOR_ROWS(c)
+    (void)off_;
+    (void)w_;
+    for (int q = 0; q < 3; ++q) zout[q * n + i] = g[q * n + i];
+    END_ROWS
+    return true;
+  }
+  // r = -g, z = r/D, d = -z, p = 0
+  double gg = 0;
+  FOR_ROWS(c)
+  (void)off_;
+  (void)w_;
+  const double Di = __ldg(a.Dex + i);
+  for (int q = 0; q < 3; ++q) {
+    const double gi = g[q * n + i];
+    const double r = -gi;
+    const double z = r / Di;
+    a.tr[q * n + i] = r;
+    a.tz[q * n + i] = z;
+    a.td[q * n + i] = -z;
+    zout[q * n + i] = 0.0;
+    gg += gi * gi;
+  }
+  END_ROWS
+  {
+    double v[1] = {gg};
+    CHECK(grid_reduce<1>(c.sy, v, 0u));
+    gg = v[0];
+  }
+  const double ng = sqrt(gg);
+  const double eps = fmin(0.5, sqrt(ng) * ng);
+  // B d, d.Bd, r.z
+  double denom, rz;
+  {
+    double pd = 0, prz = 0;
+    FOR_ROWS(c)
+    double o[3];
+    apply_A_row(a, mb, a.td, i, off_, w_, o);
+    for (int q = 0; q < 3; ++q) {
+      a.tBd[q * n + i] = o[q];
+      pd += a.td[q * n + i] * o[q];
+      prz += a.tr[q * n + i] * a.tz[q * n + i];
+    }
+    END_ROWS
+    double v[2] = {pd, prz};
+    CHECK(grid_reduce<2>(c.sy, v, 0u));
+    denom = v[0];
+    rz = v[1];
+  }
+  bool any = false;
+  int it = 0;
+  for (;;) {
+    ++it;
+    if (denom <= 0.0) break;  // negative curvature: keep p
+    const double alpha = rz / denom;
+    any = any || (alpha != 0.0);
+    double prn = 0, przn = 0;
+    FOR_ROWS(c)
+    (void)off_;
+    (void)w_;
+    const double Di = __ldg(a.Dex + i);
+    for (int q = 0; q < 3; ++q) {
+      const int idx = q * n + i;
+      zout[idx] = zout[idx] + alpha * a.td[idx];
+      const double r = a.tr[idx] + alpha * a.tBd[idx];
+      const double z = r / Di;
+      a.tr[idx] = r;
+      a.tz[idx] = z;
+      prn += r * r;
+      przn += r * z;
+    }
+    END_ROWS
+    double v[2] = {prn, przn};
+    CHECK(grid_reduce<2>(c.sy, v, 0u));
+    if (sqrt(v[0]) <= eps) break;
+    if (it >= a.precond_iter) break;
+    const double beta = v[1] / (rz + 1e-16);
+    rz = v[1];
+    // d <- -z + beta d, B d <- -A z + beta B d
+    double pd = 0;
+    FOR_ROWS(c)
+    double o[3];
+    apply_A_row(a, mb, a.tz, i, off_, w_, o);
+    for (int q = 0; q < 3; ++q) {
+      const int idx = q * n + i;
+      const double dn = -a.tz[idx] + beta * a.td[idx];
+      const double bn = -o[q] + beta * a.tBd[idx];
+      a.td[idx] = dn;
+      a.tBd[idx] = bn;
+      pd += dn * bn;
+    }
+    END_ROWS
+    double v2[1] = {pd};
+    CHECK(grid_reduce<1>(c.sy, v2, 0u));
+    denom = v2[0];
+  }
+  c.minv_iters += it;
+  if (!any) {
+    FOR_ROWS(c)
+    (void)off_;
+    (void)w_;
+    for (int q = 0; q < 3; ++q) zout[q * n + i] = g[q * n + i];
+    END_ROWS
+  }
+  return true;
+}
+
+// ---------------------------------------------------------------------------------------
+// hestenes_stiefel_ncg + line_search, scripts/minimizers.py:16-190
+// ---------------------------------------------------------------------------------------
+__device__ bool minimize(Ctx& c) {
+  const SolveArgs& a = c.a;
+  const int n = a.Npad;
+  const double sqrt_eps = 1.4901161193847656e-08;  // sqrt(2^-52)
+  double* x = a.x;
+  double* x1 = a.x1;
+  double* g = a.g;
+  double* g1 = a.g1;
+  double* d = a.d;
+  const double tol = a.tol_fun;
+  double f0 = DBL_MAX;
+  EvalOut o;
+  CHECK(eval(c, x, x, nullptr, g, o));
+  double f = o.E, dxinf = 0.0, xinf = o.xinf, ginf = o.ginf;
+  CHECK(minv(c, g, a.mbar_current ? x : a.mbar, a.zp));
+  FOR_ROWS(c)
+  (void)off_;
+  (void)w_;
+  for (int q = 0; q < 3; ++q) d[q * n + i] = -a.zp[q * n + i];
+  END_ROWS
+  long long k = 1;
+  for (;;) {
+    const bool ca = (f0 - f) > tol * (1.0 + fabs(f));
+    const bool cb = dxinf > a.sqrt_tol * (1.0 + xinf);
+    const bool cc = ginf > a.cbrt_tol * (1.0 + fabs(f));
+    if (!((ca || cb || cc) && k < a.max_ncg)) break;
+    // restart test (Andrei 2.15) and the norms of compute_h
+    double dg, dd, gg, dinf, xx;
+    {
+      double p0 = 0, p1 = 0, p2 = 0, p3 = 0, p4 = 0;
+      FOR_ROWS(c)
+      (void)off_;
+      (void)w_;
+      for (int q = 0; q < 3; ++q) {
+        const double di = d[q * n + i], gi = g[q * n + i], xi = x[q * n + i];
+        p0 += di * gi;
+        p1 += di * di;
+        p2 += gi * gi;
+        p3 = fmax(p3, fabs(di));
+        p4 += xi * xi;
+      }
+      END_ROWS
+      double v[5] = {p0, p1, p2, p3, p4};
+      CHECK(grid_reduce<5>(c.sy, v, 0x08u));
+      dg = v[0];
+      dd = v[1];
+      gg = v[2];
+      dinf = v[3];
+      xx = v[4];
+    }
+    double gd = dg;
+    if (dg > -0.001 * sqrt(dd) * sqrt(gg)) {
+      FOR_ROWS(c)
+      (void)off_;
+      (void)w_;
+      for (int q = 0; q < 3; ++q) d[q * n + i] = -g[q * n + i];
+      END_ROWS
+      dd = gg;
+      dinf = ginf;
+      gd = -gg;
+    }
+    // line search
+    const double t1 = 2.0 * sqrt_eps * (1.0 + sqrt(xx)) / sqrt(dd);
+    const double t2 = sqrt_eps / dinf;
+    const double hh = t1 < t2 ? t1 : t2;
+    CHECK(step_normalize(c, x1, x, hh, d));
+    CHECK(eval(c, x1, x, d, g1, o));
+    double alpha;
+    {  // alpha_init, scripts/minimizers.py:34-57
+      double a1 = -hh * (gd / (o.gd - gd));
+      if (a1 < 0) a1 = 0.1 * fabs(a1);
+      double a2 = 2.0 * (f - f0) / gd;
+      if (a2 < 0) a2 = 1.0e30;
+      alpha = (a1 < 0.99 * a2) ? a1 : a2;
+    }
+    CHECK(step_normalize(c, x1, x, alpha, d));
+    CHECK(eval(c, x1, x, d, g1, o));
+    const double eps_k = 1e-6 * fabs(f);
+    for (int ls = 0;; ++ls) {
+      const bool wolfe = ((2.0 * 0.1 - 1.0) * gd >= o.gd) && (o.E <= f + eps_k);
+      if (wolfe || (o.E <= f + 1e-4 * alpha * gd) || ls > 20) break;
+      alpha *= 0.5;
+      c.shrinks += 1;
+      CHECK(step_normalize(c, x1, x, alpha, d));
+      CHECK(eval(c, x1, x, d, g1, o));
+    }
+    // direction update
+    CHECK(minv(c, g1, a.mbar_current ? x : a.mbar, a.zp));
+    double yz, yd;
+    {
+      double p0 = 0, p1 = 0;
+      FOR_ROWS(c)
+      (void)off_;
+      (void)w_;
+      for (int q = 0; q < 3; ++q) {
+        const int idx = q * n + i;
+        const double y = g1[idx] - g[idx];
+        p0 += y * a.zp[idx];
+        p1 += y * d[idx];
+      }
+      END_ROWS
+      double v[2] = {p0, p1};
+      CHECK(grid_reduce<2>(c.sy, v, 0u));
+      yz = v[0];
+      yd = v[1];
+    }
+    const double bq = yz / yd;
+    const double beta = (bq != bq) ? bq : fmax(bq, 0.0);
+    double ndg, ndd;
+    {
+      double p0 = 0, p1 = 0;
+      FOR_ROWS(c)
+      (void)off_;
+      (void)w_;
+      for (int q = 0; q < 3; ++q) {
+        const int idx = q * n + i;
+        const double dn = -a.zp[idx] + beta * d[idx];
+        p0 += dn * g[idx];
+        p1 += dn * dn;
+      }
+      END_ROWS
+      double v[2] = {p0, p1};
+      CHECK(grid_reduce<2>(c.sy, v, 0u));
+      ndg = v[0];
+      ndd = v[1];
+    }
+    const bool restart = ndg > -0.001 * sqrt(ndd) * sqrt(gg);
+    FOR_ROWS(c)
+    (void)off_;
+    (void)w_;
+    for (int q = 0; q < 3; ++q) {
+      const int idx = q * n + i;
+      d[idx] = restart ? -a.zp[idx] : (-a.zp[idx] + beta * d[idx]);
+    }
+    END_ROWS
+    k += 1;
+    f0 = f;
+    f = o.E;
+    double* t = x;
+    x = x1;
+    x1 = t;
+    t = g;
+    g = g1;
+    g1 = t;
+    dxinf = o.dxinf;
+    xinf = o.xinf;
+    ginf = o.ginf;
+  }
+  // the accepted state back into the canonical buffers
+  if (x != a.x) {
+    FOR_ROWS(c)
+    (void)off_;
+    (void)w_;
+    for (int q = 0; q < 3; ++q) {
+      a.x[q * n + i] = x[q * n + i];
+      a.g[q * n + i] = g[q * n + i];
+    }
+    END_ROWS
+  }
+  // mh, scripts/loop.py:25-38
+  double pm = 0;
+  FOR_ROWS(c)
+  (void)off_;
+  (void)w_;
+  pm += (a.hdir[0] * a.x[i] + a.hdir[1] * a.x[n + i] + a.hdir[2] * a.x[2 * n + i]) * __ldg(a.meas + i);
+  END_ROWS
+  double v[1] = {pm};
+  CHECK(grid_reduce<1>(c.sy, v, 0u));
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    a.resd[0] = f;
+    a.resd[1] = v[0] / a.V;
+    a.resi[0] = k;
+    if (!(f - f == 0.0)) atomicCAS(&a.flags[FLAG_STATUS], 0, (int)MM_NONFINITE);
+  }
+  return true;
+}
+
+__global__ void __launch_bounds__(512, 1) k_solve(const __grid_constant__ SolveArgs args) {
+  Ctx c(args);
+  c.sy.bar = args.bar;
+  c.sy.red = args.red;
+  c.sy.flags = args.flags;
+  c.sy.epoch = 0;
+  c.sy.nblk = gridDim.x;
+  c.sy.blk = blockIdx.x;
+  c.sy.slot = 0;
+  c.lane = threadIdx.x & 31;
+  c.warp = threadIdx.x >> 5;
+  c.nwarps = blockDim.x >> 5;
+  c.s0 = (int)(((long long)args.nslices * blockIdx.x) / gridDim.x);
+  c.s1 = (int)(((long long)args.nslices * (blockIdx.x + 1)) / gridDim.x);
+  bool ok = true;
+  if (args.mode == MODE_EVAL) {
+    EvalOut o;
+    ok = eval(c, args.x, args.x, nullptr, args.g, o);
+    if (ok && blockIdx.x == 0 && threadIdx.x == 0) {
+      args.resd[0] = o.E;
+      if (!(o.E - o.E == 0.0)) atomicCAS(&args.flags[FLAG_STATUS], 0, (int)MM_NONFINITE);
+    }
+  } else if (args.mode == MODE_MINV) {
+    ok = minv(c, args.g, args.mbar_current ? args.x : args.mbar, args.zp);
+  } else {
+    ok = minimize(c);
+  }
+  if (ok && blockIdx.x == 0 && threadIdx.x == 0) {
+    args.resi[1] = c.evals;
+    args.resi[2] = c.pcg_iters;
+    args.resi[3] = c.shrinks;
+    args.resi[4] = c.minv_iters;
+  }
+}
+
+}  // namespace
+
+void solver_configure(DevMesh& m) {
+  int dev = m.device;
+  cudaDeviceProp prop;
+  if (cudaGetDeviceProperties(&prop, dev) != cudaSuccess) throw std::runtime_error("cudaGetDeviceProperties failed");
+  int block = m.opt.block_threads > 0 ? m.opt.block_threads : 256;
+  block = std::max(32, std::min(512, (block / 32) * 32));
+  int occ = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_solve, block, 0) != cudaSuccess || occ < 1)
+    throw std::runtime_error("persistent solver kernel cannot be resident with " + std::to_string(block) +
+                             " threads per CTA");
+  const int maxgrid = occ * prop.multiProcessorCount;
+  const int warps = block / 32;
+  int grid = m.opt.grid_ctas > 0 ? m.opt.grid_ctas
+                                 : (int)std::min<int64_t>(prop.multiProcessorCount,
+                                                          (m.h.nslices + warps - 1) / warps);
+  grid = std::max(1, std::min(grid, maxgrid));
+  grid = (int)std::min<int64_t>(grid, m.h.nslices);
+  m.grid = grid;
+  m.block = block;
+}
+
+SolveArgs solver_args(const DevMesh& m, int mode, double h, const mm_solver_params& sp) {
+  SolveArgs a{};
+  a.sl_off = m.sl_off;
+  a.sl_w = m.sl_w;
+  a.col = m.col;
+  a.vals = m.vals;
+  a.nent = m.h.nent;
+  a.invdS = m.invdS;
+  a.Dex = m.Dex;
+  a.meas = m.meas;
+  a.nslices = (int32_t)m.h.nslices;
+  a.Npad = (int32_t)m.h.Npad;
+  a.V = m.V;
+  a.x = m.x;
+  a.x1 = m.x1;
+  a.g = m.g;
+  a.g1 = m.g1;
+  a.d = m.d;
+  a.gf = m.gf;
+  a.mbar = m.mbar;
+  a.zp = m.zp;
+  a.tr = m.tr;
+  a.tz = m.tz;
+  a.td = m.td;
+  a.tBd = m.tBd;
+  a.u = m.u;
+  a.pr = m.pr;
+  a.pz = m.pz;
+  a.pp = m.pp;
+  a.pq = m.pq;
+  a.bar = m.bar;
+  a.red = m.red;
+  a.flags = m.flags;
+  a.mode = mode;
+  a.h = h;
+  for (int q = 0; q < 3; ++q) a.hdir[q] = sp.hdir[q];
+  a.tol_fun = sp.tol_fun;
+  a.sqrt_tol = std::sqrt(sp.tol_fun);
+  a.cbrt_tol = std::cbrt(sp.tol_fun);
+  a.tol_u = sp.tol_u;
+  a.precond_iter = sp.precond_iter;
+  a.hmag_on = sp.hmag_on;
+  a.mbar_current = sp.mbar_mode;
+  a.max_pcg = sp.max_pcg_iter;
+  a.max_ncg = sp.max_ncg_iter;
+  a.resd = m.resd;
+  a.resi = m.resi;
+  return a;
+}
+
+cudaError_t solver_launch(DevMesh& m, const SolveArgs& a) {
+  cudaError_t e = cudaMemsetAsync(m.bar, 0, sizeof(unsigned long long), m.stream);
+  if (e != cudaSuccess) return e;
+  e = cudaMemsetAsync(m.flags, 0, 2 * sizeof(int), m.stream);
+  if (e != cudaSuccess) return e;
+  e = cudaMemsetAsync(m.resi, 0, 8 * sizeof(long long), m.stream);
+  if (e != cudaSuccess) return e;
+  cudaLaunchConfig_t cfg{};
+  cfg.gridDim = dim3(m.grid);
+  cfg.blockDim = dim3(m.block);
+  cfg.dynamicSmemBytes = 0;
+  cfg.stream = m.stream;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeCooperative;
+  attr[0].val.cooperative = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, k_solve, a);
+}
+
+}  // namespace mumag

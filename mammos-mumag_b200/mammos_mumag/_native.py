@@ -1,0 +1,362 @@
+"""ctypes binding of ``libmumag_b200.so`` (C ABI declared in ``include/mumag_b200.h``).
+
+The library is the only compute path: there is no CPU fallback.  If the shared object is
+missing or no sm_100 device is present, the calls raise.
+"""
+
+from __future__ import annotations
+
+import ctypes as C
+import pathlib
+
+import numpy as np
+
+LIB_PATH = pathlib.Path(__file__).resolve().parent / "lib" / "libmumag_b200.so"
+
+MM_OK, MM_BAD_INPUT, MM_CUDA_ERROR, MM_NONFINITE, MM_TIMEOUT, MM_NO_DEVICE = range(6)
+STATUS_NAMES = {
+    MM_OK: "OK",
+    MM_BAD_INPUT: "BAD_INPUT",
+    MM_CUDA_ERROR: "CUDA_ERROR",
+    MM_NONFINITE: "NONFINITE",
+    MM_TIMEOUT: "TIMEOUT",
+    MM_NO_DEVICE: "NO_DEVICE",
+}
+PREC_FP64, PREC_MIXED = 0, 1
+
+# every symbol include/mumag_b200.h declares
+EXPORTED = (
+    "mm_version",
+    "mm_last_error",
+    "mm_default_options",
+    "mm_default_solver_params",
+    "mm_device_count",
+    "mm_rcm_permutation",
+    "mm_color_elements",
+    "mm_mesh_create",
+    "mm_mesh_destroy",
+    "mm_mesh_get_info",
+    "mm_get_meas",
+    "mm_get_operator",
+    "mm_set_state",
+    "mm_get_state",
+    "mm_energy_grad",
+    "mm_apply_minv",
+    "mm_minimize",
+    "mm_loop",
+)
+
+
+class Material(C.Structure):
+    _fields_ = [(n, C.c_double) for n in ("theta", "phi", "K1", "K2", "Js", "A")]
+
+
+class Options(C.Structure):
+    _fields_ = [
+        ("size", C.c_double),
+        ("dirichlet_rhs", C.c_int),
+        ("precision", C.c_int),
+        ("device", C.c_int),
+        ("grid_ctas", C.c_int),
+        ("block_threads", C.c_int),
+        ("reorder", C.c_int),
+    ]
+
+
+class SolverParams(C.Structure):
+    _fields_ = [
+        ("hdir", C.c_double * 3),
+        ("tol_fun", C.c_double),
+        ("tol_u", C.c_double),
+        ("precond_iter", C.c_int),
+        ("hmag_on", C.c_int),
+        ("mbar_mode", C.c_int),
+        ("max_pcg_iter", C.c_int),
+        ("max_ncg_iter", C.c_int),
+    ]
+
+
+class StepResult(C.Structure):
+    _fields_ = [
+        ("energy", C.c_double),
+        ("mh", C.c_double),
+        ("ncg_iters", C.c_int64),
+        ("evals", C.c_int64),
+        ("pcg_iters", C.c_int64),
+        ("ls_shrinks", C.c_int64),
+        ("minv_iters", C.c_int64),
+        ("status", C.c_int),
+    ]
+
+    def as_dict(self):
+        return {n: getattr(self, n) for n, _ in self._fields_}
+
+
+class MeshInfo(C.Structure):
+    _fields_ = [
+        ("nodes", C.c_int64),
+        ("elements", C.c_int64),
+        ("sell_slices", C.c_int64),
+        ("sell_entries", C.c_int64),
+        ("nnz", C.c_int64),
+        ("colours", C.c_int32),
+        ("airbox", C.c_int32),
+        ("grid_ctas", C.c_int32),
+        ("block_threads", C.c_int32),
+        ("dirichlet_nodes", C.c_int64),
+        ("volume", C.c_double),
+        ("bandwidth_before", C.c_double),
+        ("bandwidth_after", C.c_double),
+    ]
+
+    def as_dict(self):
+        return {n: getattr(self, n) for n, _ in self._fields_}
+
+
+class LoopParams(C.Structure):
+    _fields_ = [
+        ("hstart", C.c_double),
+        ("hfinal", C.c_double),
+        ("hstep", C.c_double),
+        ("mstep", C.c_double),
+        ("mfinal", C.c_double),
+        ("max_steps", C.c_int32),
+    ]
+
+
+class Record(C.Structure):
+    _fields_ = [(n, C.c_double) for n in ("counter", "hext", "mh", "energy")]
+
+
+SNAPSHOT_CB = C.CFUNCTYPE(C.c_int, C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_double), C.c_int64, C.c_void_p)
+
+_D = C.POINTER(C.c_double)
+_I32 = C.POINTER(C.c_int32)
+_I64 = C.POINTER(C.c_int64)
+_lib = None
+
+
+def load():
+    """Load the shared library (once) and declare the signatures."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not LIB_PATH.exists():
+        raise RuntimeError(
+            f"{LIB_PATH} is missing: build it with `python mammos-mumag_b200/build.py` "
+            "(the CUDA path has no CPU fallback)"
+        )
+    lib = C.CDLL(str(LIB_PATH))
+    sig = {
+        "mm_version": (C.c_char_p, []),
+        "mm_last_error": (C.c_char_p, []),
+        "mm_default_options": (None, [C.POINTER(Options)]),
+        "mm_default_solver_params": (None, [C.POINTER(SolverParams)]),
+        "mm_device_count": (C.c_int, []),
+        "mm_rcm_permutation": (C.c_int, [C.c_int64, _I32, C.c_int64, _I32]),
+        "mm_color_elements": (C.c_int, [C.c_int64, _I32, C.c_int64, _I32, _I32]),
+        "mm_mesh_create": (
+            C.c_int,
+            [_D, C.c_int64, _I32, _I32, C.c_int64, C.POINTER(Material), C.c_int32, C.POINTER(Options), C.POINTER(C.c_void_p)],
+        ),
+        "mm_mesh_destroy": (C.c_int, [C.c_void_p]),
+        "mm_mesh_get_info": (C.c_int, [C.c_void_p, C.POINTER(MeshInfo)]),
+        "mm_get_meas": (C.c_int, [C.c_void_p, _D, _D]),
+        "mm_get_operator": (C.c_int, [C.c_void_p, C.c_int32, _I64, _I32, _I32, _D]),
+        "mm_set_state": (C.c_int, [C.c_void_p, _D, _D, _D]),
+        "mm_get_state": (C.c_int, [C.c_void_p, _D, _D, _D]),
+        "mm_energy_grad": (C.c_int, [C.c_void_p, C.c_double, C.POINTER(SolverParams), _D, _D, _I64]),
+        "mm_apply_minv": (C.c_int, [C.c_void_p, C.POINTER(SolverParams), _D, _D, _I64]),
+        "mm_minimize": (C.c_int, [C.c_void_p, C.c_double, C.POINTER(SolverParams), C.POINTER(StepResult)]),
+        "mm_loop": (
+            C.c_int,
+            [C.c_void_p, C.POINTER(LoopParams), C.POINTER(SolverParams), C.POINTER(Record), _I32,
+             C.POINTER(StepResult), SNAPSHOT_CB, C.c_void_p],
+        ),
+    }
+    for name, (res, args) in sig.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = lib
+    return lib
+
+
+class NativeError(RuntimeError):
+    def __init__(self, status, msg):
+        super().__init__(f"libmumag_b200 {STATUS_NAMES.get(status, status)}: {msg}")
+        self.status = status
+
+
+def check(status):
+    if status != MM_OK:
+        raise NativeError(status, load().mm_last_error().decode())
+
+
+def _dp(a):
+    return a.ctypes.data_as(_D) if a is not None else None
+
+
+def device_count() -> int:
+    return load().mm_device_count()
+
+
+def default_options(**kw) -> Options:
+    o = Options()
+    load().mm_default_options(C.byref(o))
+    for k, v in kw.items():
+        setattr(o, k, v)
+    return o
+
+
+def solver_params(hdir=(0.0, 0.0, 1.0), tol_fun=1e-10, tol_u=None, precond_iter=10, hmag_on=1,
+                  mbar_mode=0, max_pcg_iter=10000, max_ncg_iter=100000) -> SolverParams:
+    sp = SolverParams()
+    load().mm_default_solver_params(C.byref(sp))
+    for q in range(3):
+        sp.hdir[q] = float(hdir[q])
+    sp.tol_fun = tol_fun
+    sp.tol_u = tol_fun if tol_u is None else tol_u
+    sp.precond_iter = precond_iter
+    sp.hmag_on = hmag_on
+    sp.mbar_mode = mbar_mode
+    sp.max_pcg_iter = max_pcg_iter
+    sp.max_ncg_iter = max_ncg_iter
+    return sp
+
+
+def rcm_permutation(T: np.ndarray, N: int) -> np.ndarray:
+    T = np.ascontiguousarray(T, dtype=np.int32)
+    perm = np.empty(N, dtype=np.int32)
+    check(load().mm_rcm_permutation(N, T.ctypes.data_as(_I32), T.shape[0], perm.ctypes.data_as(_I32)))
+    return perm
+
+
+def color_elements(T: np.ndarray, N: int):
+    T = np.ascontiguousarray(T, dtype=np.int32)
+    col = np.empty(T.shape[0], dtype=np.int32)
+    n = C.c_int32()
+    check(load().mm_color_elements(N, T.ctypes.data_as(_I32), T.shape[0], col.ctypes.data_as(_I32), C.byref(n)))
+    return col, n.value
+
+
+class Mesh:
+    """Device operators of one mesh (an ``mm_mesh`` handle)."""
+
+    def __init__(self, X, T, tag, materials, size=1e-9, dirichlet_rhs=0, precision=PREC_FP64, device=0,
+                 grid_ctas=0, block_threads=0, reorder=1):
+        lib = load()
+        self.X = np.ascontiguousarray(X, dtype=np.float64)
+        self.T = np.ascontiguousarray(T, dtype=np.int32)
+        self.tag = np.ascontiguousarray(tag, dtype=np.int32)
+        self.N, self.E = self.X.shape[0], self.T.shape[0]
+        rows = [tuple(float(v) for v in r[:6]) for r in materials]
+        mats = (Material * max(1, len(rows)))(*[Material(*r) for r in rows])
+        opt = default_options(size=size, dirichlet_rhs=dirichlet_rhs, precision=precision, device=device,
+                              grid_ctas=grid_ctas, block_threads=block_threads, reorder=reorder)
+        h = C.c_void_p()
+        check(lib.mm_mesh_create(_dp(self.X), self.N, self.T.ctypes.data_as(_I32), self.tag.ctypes.data_as(_I32),
+                                 self.E, mats, len(rows), C.byref(opt), C.byref(h)))
+        self._h = h
+
+    def close(self):
+        if getattr(self, "_h", None):
+            load().mm_mesh_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def info(self) -> dict:
+        i = MeshInfo()
+        check(load().mm_mesh_get_info(self._h, C.byref(i)))
+        return i.as_dict()
+
+    def meas(self):
+        out = np.empty(self.N)
+        v = C.c_double()
+        check(load().mm_get_meas(self._h, _dp(out), C.byref(v)))
+        return out, v.value
+
+    def operator(self, which: int):
+        nnz = C.c_int64()
+        lib = load()
+        check(lib.mm_get_operator(self._h, which, C.byref(nnz), None, None, None))
+        r = np.empty(nnz.value, np.int32)
+        c = np.empty(nnz.value, np.int32)
+        v = np.empty(nnz.value)
+        check(lib.mm_get_operator(self._h, which, C.byref(nnz), r.ctypes.data_as(_I32), c.ctypes.data_as(_I32), _dp(v)))
+        return r, c, v
+
+    def set_state(self, m, u=None, mbar=None):
+        m = np.ascontiguousarray(m, dtype=np.float64).ravel()
+        u = None if u is None else np.ascontiguousarray(u, dtype=np.float64).ravel()
+        mbar = None if mbar is None else np.ascontiguousarray(mbar, dtype=np.float64).ravel()
+        if m.size != 3 * self.N or (u is not None and u.size != self.N) or (mbar is not None and mbar.size != 3 * self.N):
+            raise ValueError("state arrays have the wrong size")
+        check(load().mm_set_state(self._h, _dp(m), _dp(u), _dp(mbar)))
+
+    def get_state(self):
+        m = np.empty(3 * self.N)
+        u = np.empty(self.N)
+        g = np.empty(3 * self.N)
+        check(load().mm_get_state(self._h, _dp(m), _dp(u), _dp(g)))
+        return m, u, g
+
+    def energy_grad(self, h, sp):
+        e = C.c_double()
+        g = np.empty(3 * self.N)
+        it = C.c_int64()
+        check(load().mm_energy_grad(self._h, float(h), C.byref(sp), C.byref(e), _dp(g), C.byref(it)))
+        return e.value, g, it.value
+
+    def apply_minv(self, g, sp):
+        g = np.ascontiguousarray(g, dtype=np.float64).ravel()
+        z = np.empty(3 * self.N)
+        it = C.c_int64()
+        check(load().mm_apply_minv(self._h, C.byref(sp), _dp(g), _dp(z), C.byref(it)))
+        return z, it.value
+
+    def minimize(self, h, sp) -> dict:
+        r = StepResult()
+        check(load().mm_minimize(self._h, float(h), C.byref(sp), C.byref(r)))
+        return r.as_dict()
+
+    def loop(self, hstart, hfinal, hstep, mstep, mfinal, sp, snapshot=None, max_steps=0):
+        """Field sweep from the current state. Returns (rows [n,4], per-step dicts)."""
+        lp = LoopParams(hstart, hfinal, hstep, mstep, mfinal, max_steps)
+        nmax = int(abs(hfinal - hstart) / abs(hstep)) + 1
+        if max_steps > 0:
+            nmax = min(nmax, max_steps)
+        rec = (Record * nmax)()
+        steps = (StepResult * nmax)()
+        nrec = C.c_int32()
+        err = []
+
+        def _cb(counter, mp, up, n, _user):
+            try:
+                m = np.ctypeslib.as_array(mp, shape=(3 * n,)).copy()
+                u = np.ctypeslib.as_array(up, shape=(n,)).copy()
+                snapshot(counter, m, u)
+                return 0
+            except Exception as e:  # surfaced after the call
+                err.append(e)
+                return 1
+
+        cb = SNAPSHOT_CB(_cb) if snapshot is not None else SNAPSHOT_CB()
+        st = load().mm_loop(self._h, C.byref(lp), C.byref(sp), rec, C.byref(nrec), steps, cb, None)
+        if err:
+            raise err[0]
+        check(st)
+        n = nrec.value
+        rows = np.array([[rec[i].counter, rec[i].hext, rec[i].mh, rec[i].energy] for i in range(n)]).reshape(n, 4)
+        return rows, [steps[i].as_dict() for i in range(n)]

@@ -1,0 +1,107 @@
+"""Simulation class (``src/mammos_mumag/simulation.py`` of the reference).
+
+``run_loop`` keeps the reference's contract -- it writes ``<name>.fly``, ``<name>.krn`` and
+``<name>.p2`` into ``outdir`` and produces ``<name>.dat``, ``<name>_NNNN.vtu``,
+``<name>_stats.txt`` and ``info.json`` there -- but runs the loop in process on the GPU
+(``mammos_mumag.runner``) instead of ``run-escript scripts/loop.py <name>``.  Failures raise
+``RuntimeError("Simulation has failed. ...")`` as the reference's subprocess wrapper does
+(``simulation.py:437-458``).
+"""
+
+from __future__ import annotations
+
+import datetime
+import json
+import pathlib
+
+import mammos_mumag
+from mammos_mumag import fly, runner
+from mammos_mumag.materials import Materials
+from mammos_mumag.parameters import Parameters
+from mammos_mumag.tools import check_dir
+
+
+class Simulation:
+    """Holds the mesh path, the materials and the parameters of a run."""
+
+    def __init__(self, material_domain_list=None, mesh_filepath=None, materials_filepath=None,
+                 parameters_filepath=None, materials=None, parameters=None):
+        self.material_domain_list = material_domain_list
+        self.mesh_filepath = pathlib.Path(mesh_filepath) if mesh_filepath is not None else None
+        self.materials_filepath = materials_filepath
+        self.parameters_filepath = parameters_filepath
+        self.materials = materials
+        self.parameters = parameters
+        if isinstance(self.materials, dict) or isinstance(self.materials, list):
+            self.materials = Materials(domains=self.materials)
+        if material_domain_list is not None:
+            self.materials = Materials(domains=material_domain_list)
+        elif materials_filepath is not None:
+            self.materials = Materials(filepath=materials_filepath)
+        if parameters_filepath is not None:
+            self.parameters = Parameters(filepath=parameters_filepath)
+
+    def __repr__(self):
+        return f"Simulation(mesh_filepath={self.mesh_filepath!r}, materials={self.materials!r}, parameters={self.parameters!r})"
+
+    def check_attribute(self, *args) -> None:
+        for attr in args:
+            if getattr(self, attr) is None:
+                raise AttributeError(f"Attribute `{attr}` has not been defined yet.")
+
+    def _write_inputs(self, outdir, name, b200: dict | None = None):
+        self.check_attribute("mesh_filepath", "materials", "parameters")
+        fly.copy_as_fly(self.mesh_filepath, outdir / f"{name}.fly")
+        self.materials.write_krn(outdir / f"{name}.krn")
+        self.parameters.write_p2(outdir / f"{name}.p2")
+        if b200:
+            with open(outdir / f"{name}.p2", "a") as f:
+                f.write("\n[b200]\n" + "".join(f"{k} = {v}\n" for k, v in b200.items()))
+
+    def run_loop(self, outdir="loop", name="out", m0=None, precision=None, dirichlet_rhs=None, mbar=None,
+                 device=0):
+        r"""Compute the demagnetisation curve (the reference's ``loop`` script).
+
+        Extra keywords (absent from the reference): ``m0`` an explicit initial
+        magnetisation [3N]; ``precision`` ``"fp64"`` (default) or ``"mixed"``;
+        ``dirichlet_rhs`` ``"reference"`` (default) or ``"zero"``; ``mbar`` ``"reference"``
+        (default, M_inv projects with the initial m) or ``"current"``; ``device``.
+        """
+        outdir = check_dir(outdir)
+        b200 = {k: v for k, v in (("precision", precision), ("dirichlet_rhs", dirichlet_rhs), ("mbar", mbar)) if v}
+        self._write_inputs(outdir, name, b200)
+        try:
+            runner.run_loop(outdir, name, m0=m0, device=device)
+        except Exception as e:
+            raise RuntimeError(f"Simulation has failed. Exit with error: \n{e}") from e
+        with open(outdir / "info.json", "w") as f:
+            json.dump({
+                "datetime": datetime.datetime.now(datetime.UTC).astimezone().isoformat(timespec="seconds"),
+                "mammos_mumag_version": mammos_mumag.__version__,
+            }, f)
+
+    def _out_of_scope(self, what):
+        raise NotImplementedError(
+            f"run_{what} is an escript diagnostic of the reference and is not part of the B200 hysteresis path"
+        )
+
+    def run_exani(self, outdir="exani", name="out"):
+        self._out_of_scope("exani")
+
+    def run_external(self, outdir="external", name="out"):
+        self._out_of_scope("external")
+
+    def run_hmag(self, outdir="hmag", name="out"):
+        self._out_of_scope("hmag")
+
+    def run_magnetization(self, outdir="magnetization", name="out"):
+        self._out_of_scope("magnetization")
+
+    def run_mapping(self, outdir="magnetization", name="out"):
+        self._out_of_scope("mapping")
+
+    def run_materials(self, outdir="materials", name="out"):
+        self._out_of_scope("materials")
+
+    def run_store(self, outdir="magnetization", name="out"):
+        self._out_of_scope("store")

@@ -26,7 +26,7 @@ def golden():
 @pytest.fixture(scope="session")
 def cube_mesh():
     """The reference's ``tests/data/cube.fly``: 20 nm cube in a sphere shell (tags 1/2/3)."""
-    g = np.load(GOLDEN / "cube_mesh.npz")
+    g = np.load(ROOT / "mammos-mumag_b200" / "mammos_mumag" / "mesh" / "CUBE_20_nm.npz")
     return g["X"], g["T"], g["tag"].astype(np.int32)
 
 

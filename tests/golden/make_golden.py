@@ -5,8 +5,11 @@ The reference (mammos-mumag 0.7.1) ships its regression goldens as text files un
 and JAX), so the goldens it recorded are the pins for the oracle and for the CUDA path.
 This script reads them as plain text and stores compact copies here:
 
-* ``cube_mesh.npz``       -- ``tests/data/cube.fly`` (9,698 nodes, 53,275 Tet4, tags 1/2/3):
-                             X [N,3] f64 (nm), T [E,4] int32 (0-based), tag [E] int8.
+* ``mammos-mumag_b200/mammos_mumag/mesh/CUBE_20_nm.npz`` -- ``tests/data/cube.fly``
+                             (identical to the reference's packaged ``mesh/CUBE_20_nm.fly``;
+                             9,698 nodes, 53,275 Tet4, tags 1/2/3): X [N,3] f64 (nm),
+                             T [E,4] int32 (0-based), tag [E] int8.  It ships with the package
+                             as ``mammos_mumag.mesh.CUBE_20_nm``.
 * ``loop_cube.dat``       -- ``tests/data/loop/cube.dat`` verbatim (21 rows of the loop golden).
 * ``loop_cube.krn/.p2``   -- the material and parameter files of that loop run, verbatim.
 * ``loop_cube_0001.npz``  -- point data ``m`` [N,3] and ``u`` [N] of ``tests/data/loop/cube_0001.vtu``.
@@ -61,7 +64,9 @@ def read_energy_csv(path):
 def main(ref_root):
     data = pathlib.Path(ref_root) / "tests" / "data"
     X, T, tag = read_fly(data / "cube.fly")
-    np.savez_compressed(HERE / "cube_mesh.npz", X=X, T=T, tag=tag)
+    pkg_mesh = HERE.parent.parent / "mammos-mumag_b200" / "mammos_mumag" / "mesh"
+    pkg_mesh.mkdir(parents=True, exist_ok=True)
+    np.savez_compressed(pkg_mesh / "CUBE_20_nm.npz", X=X, T=T, tag=tag)
     shutil.copyfile(data / "loop" / "cube.dat", HERE / "loop_cube.dat")
     shutil.copyfile(data / "loop" / "cube.krn", HERE / "loop_cube.krn")
     shutil.copyfile(data / "loop" / "cube.p2", HERE / "loop_cube.p2")

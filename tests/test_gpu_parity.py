@@ -1,0 +1,173 @@
+"""Parity of the CUDA path (libmumag_b200.so via the C ABI) with the CPU oracle and the
+reference's goldens.  FP64 mode: energies and fields must agree to 1e-6 relative (the
+contract); the assertions below are tighter where FP64 allows."""
+
+import numpy as np
+import pytest
+import scipy.sparse as sp
+
+import oracle as O
+from mammos_mumag import _native, synthetic
+
+pytestmark = pytest.mark.gpu
+
+
+def _csr(r, c, v, n):
+    return sp.csr_matrix((v, (r, c)), shape=(n, n))
+
+
+def _relmax(a, b):
+    a, b = np.asarray(a), np.asarray(b)
+    return np.abs(a - b).max() / max(np.abs(b).max(), 1e-300)
+
+
+@pytest.fixture(scope="module", params=["shell", "airbox"])
+def case(request, cube_mesh, golden):
+    if request.param == "shell":
+        X, T, tag = cube_mesh
+        krn = O.read_krn_rows((golden / "loop_cube.krn").read_text())
+    else:
+        X, T, tag, krn, _ = synthetic.multigrain(n=8, L=20.0, grains=3, cone_deg=30.0, gb=2.0, seed=1)
+    P = O.Problem(X, T, tag, krn)
+    M = _native.Mesh(X, T, tag, krn)
+    yield P, M
+    M.close()
+
+
+def test_mesh_info(case):
+    P, M = case
+    info = M.info()
+    assert info["nodes"] == P.N and info["elements"] == P.E
+    assert info["airbox"] == int(P.airbox)
+    assert info["dirichlet_nodes"] == int(P.bnd.sum())
+    assert info["volume"] == pytest.approx(P.V, rel=1e-13)
+    assert info["bandwidth_after"] < info["bandwidth_before"]
+
+
+def test_operators_match_oracle(case):
+    P, M = case
+    N = P.N
+    S = _csr(*M.operator(0), N)
+    assert abs(S - P.S).max() <= 1e-12 * abs(P.S).max()
+    SA = _csr(*M.operator(1), N)
+    assert abs(SA - P.SA).max() <= 1e-12 * abs(P.SA).max()
+    # anisotropy blocks: C - kron(SA, I3)
+    Kani = (P.C - sp.kron(P.SA, sp.eye(3))).tocsr()
+    blocks = {(0, 0): 2, (0, 1): 3, (0, 2): 4, (1, 1): 5, (1, 2): 6, (2, 2): 7}
+    scale = max(abs(Kani).max(), 1e-300)
+    for (p, q), w in blocks.items():
+        Kw = _csr(*M.operator(w), N)
+        ref = Kani[p::3, q::3]
+        assert abs(Kw - ref).max() <= 1e-12 * scale, (p, q)
+    for k in range(3):
+        Dk = _csr(*M.operator(8 + k), N)
+        Gk = _csr(*M.operator(11 + k), N)
+        assert abs(Dk - P.dk[k]).max() <= 1e-12 * abs(P.dk[k]).max()
+        assert abs(Gk - P.gk[k]).max() <= 1e-12 * abs(P.gk[k]).max()
+    meas, V = M.meas()
+    np.testing.assert_allclose(meas, P.meas, rtol=1e-12, atol=1e-12 * P.meas.max())
+    assert V == pytest.approx(P.V, rel=1e-13)
+
+
+def _random_state(P, seed):
+    rng = np.random.default_rng(seed)
+    m = rng.standard_normal((P.N, 3)) + np.array([0, 0, 2.0])
+    m = O.normalize_vectors((m * P.mask[:, None]).ravel())
+    return m
+
+
+def test_energy_gradient_match_oracle(case):
+    P, M = case
+    m = _random_state(P, 7)
+    u0 = np.zeros(P.N)
+    hdir = [0.1, 0.0, 0.995]
+    hdir = list(np.array(hdir) / np.linalg.norm(hdir))
+    M.set_state(m, u0, m)
+    sp_ = _native.solver_params(hdir=hdir)
+    E, gp, it = M.energy_grad(0.7, sp_)
+    Eo, gpo, uo, gfo = O.total_eg(P, m, 0.7, hdir, u0, 1e-10)
+    assert E == pytest.approx(Eo, rel=1e-10)
+    assert _relmax(gp, gpo) < 1e-8
+    _, u, gf = M.get_state()
+    assert _relmax(u, uo) < 1e-8
+    assert _relmax(gf, gfo) < 1e-8
+    assert it > 0
+    # warm start: a second evaluation from the converged u needs (almost) no iterations
+    E2, _, it2 = M.energy_grad(0.7, sp_)
+    assert it2 <= 2 and E2 == pytest.approx(Eo, rel=1e-10)
+
+
+def test_minv_matches_oracle(case):
+    P, M = case
+    m = _random_state(P, 11)
+    hdir = [0.0, 0.0, 1.0]
+    M.set_state(m, None, m)
+    sp_ = _native.solver_params(hdir=hdir)
+    M.energy_grad(0.3, sp_)  # sets the full gradient M_inv uses
+    _, _, gf = M.get_state()
+    g = O.projection(m, gf)
+    z, it = M.apply_minv(g, sp_)
+    st = O.Stats()
+    zo = O.m_inv(P, g, gf, m, 10, st)
+    assert it == st.minv_iters
+    assert _relmax(z, zo) < 1e-8
+
+
+def test_field_step_matches_oracle(case):
+    P, M = case
+    m = _random_state(P, 3)
+    hdir = [0.0, 0.0, 1.0]
+    par = dict(tol_fun=1e-10, tol_u=1e-10, precond_iter=10, hmag_on=1)
+    M.set_state(m, None, m)
+    res = M.minimize(0.5, _native.solver_params(hdir=hdir))
+    st = O.Stats()
+    fo, xo, ko, uo, _ = O.hestenes_stiefel_ncg(P, m.copy(), 0.5, hdir, np.zeros(P.N), np.zeros(3 * P.N), m, par, st)
+    assert res["status"] == 0
+    assert res["energy"] == pytest.approx(fo, rel=1e-9)
+    assert res["mh"] == pytest.approx(O.compute_mh(P, xo, hdir), rel=1e-7)
+    x, u, _ = M.get_state()
+    assert np.abs(x - xo).max() < 1e-5
+    assert abs(res["ncg_iters"] - ko) <= max(2, ko // 5)
+
+
+def test_golden_loop_cube_dat(cube_mesh, golden):
+    """The reference's loop golden (tests/data/loop/cube.dat) on the GPU."""
+    X, T, tag = cube_mesh
+    krn = O.read_krn_rows((golden / "loop_cube.krn").read_text())
+    par = O.read_params((golden / "loop_cube.p2").read_text())
+    with _native.Mesh(X, T, tag, krn) as M:
+        meas, _ = M.meas()
+        P = O.Problem(X, T, tag, krn)
+        m0 = O.initial_m_uniform(P, par["m"])
+        M.set_state(m0, None, m0)
+        snaps = {}
+        rows, steps = M.loop(par["hstart"], par["hfinal"], par["hstep"], par["mstep"], par["mfinal"],
+                             _native.solver_params(hdir=par["hdir"]),
+                             snapshot=lambda c, m, u: snaps.setdefault(c, (m, u)))
+    gold = np.loadtxt(golden / "loop_cube.dat")
+    out = rows.copy()
+    out[:, 3] /= O.MU0_OUT
+    assert out.shape == gold.shape
+    assert np.array_equal(out[:, 0], gold[:, 0])
+    assert np.array_equal(out[:, 1], gold[:, 1])
+    np.testing.assert_allclose(out[:, 2], gold[:, 2], rtol=1e-9)
+    np.testing.assert_allclose(out[:, 3], gold[:, 3], rtol=1e-9)
+    v = np.load(golden / "loop_cube_0001.npz")
+    np.testing.assert_allclose(snaps[1][0].reshape(-1, 3), v["m"], rtol=1e-5, atol=2e-7)
+    assert sum(s["ncg_iters"] for s in steps) == pytest.approx(67, abs=3)
+
+
+def test_synthetic_multigrain_loop_matches_oracle():
+    X, T, tag, krn, m0 = synthetic.multigrain(n=6, L=20.0, grains=3, cone_deg=20.0, gb=2.0, seed=5)
+    hdir = list(np.array([np.sin(np.radians(1)), 0, np.cos(np.radians(1))]))
+    par = dict(hdir=hdir, hstart=2.0, hfinal=-2.0, hstep=-0.5, mstep=0.4, mfinal=-2.0,
+               tol_fun=1e-10, tol_u=1e-10, precond_iter=10, hmag_on=1, m=[0, 0, 1.0])
+    P = O.Problem(X, T, tag, krn)
+    rows_o, _ = O.run_loop(P, par, m0=m0)
+    with _native.Mesh(X, T, tag, krn) as M:
+        M.set_state(m0, None, m0)
+        rows, _ = M.loop(2.0, -2.0, -0.5, 0.4, -2.0, _native.solver_params(hdir=hdir))
+    assert rows.shape == rows_o.shape
+    np.testing.assert_array_equal(rows[:, 1], rows_o[:, 1])
+    np.testing.assert_allclose(rows[:, 2], rows_o[:, 2], rtol=1e-6)
+    np.testing.assert_allclose(rows[:, 3], rows_o[:, 3], rtol=1e-8)

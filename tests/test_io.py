@@ -1,0 +1,93 @@
+"""Host-side drop-in pieces: material/parameter files, .fly/.vtu I/O, synthetic meshes."""
+
+import numpy as np
+import pytest
+from pydantic import ValidationError
+
+import oracle as O
+from mammos_mumag import fly, runner, synthetic, vtu
+from mammos_mumag.materials import MaterialDomain, Materials
+from mammos_mumag.parameters import Parameters
+
+
+def test_materials_roundtrip(golden, tmp_path):
+    mat = Materials(filepath=golden / "io" / "cube.krn")
+    assert len(mat.domains) == 3
+    assert mat.domains[0].K1 == 4.9e6 and mat.domains[0].Js == pytest.approx(1.61)
+    mat.write_krn(tmp_path / "m.krn")
+    mat.write_yaml(tmp_path / "m.yaml")
+    for f in ("m.krn", "m.yaml"):
+        back = Materials(filepath=tmp_path / f)
+        for a, b in zip(mat.domains, back.domains):
+            for k in ("theta", "phi", "K1", "K2", "Ms", "A"):
+                assert getattr(a, k) == pytest.approx(getattr(b, k), rel=1e-12)
+    yml = Materials(filepath=golden / "io" / "materials.yaml")
+    assert yml.domains[0].Js == pytest.approx(1.61)
+    # the .krn the loop reads carries the same numbers
+    rows = runner.read_krn_rows(tmp_path / "m.krn")
+    assert rows[0][:6] == pytest.approx([0.0, 0.0, 4.9e6, 0.0, 1.61, 8e-11])
+    with pytest.raises(NotImplementedError):
+        Materials().read(golden / "io" / "cube.p2")
+
+
+def test_parameters_roundtrip_and_validation(golden, tmp_path):
+    for bad in (1, 1.0, [1], [1, 2], [1, 2, 3, 4]):
+        with pytest.raises(ValidationError):
+            Parameters(m_vect=bad)
+        with pytest.raises(ValidationError):
+            Parameters(h_vect=bad)
+    par = Parameters(m_vect=np.array([1, 2, 3]))
+    assert par.m == [1.0 / np.sqrt(14), 2.0 / np.sqrt(14), 3.0 / np.sqrt(14)]
+    par = Parameters(m=[1, 0, 0], hstart=8.0, hfinal=-1.5, hstep=-0.01, iter_max=5000)
+    par.write_p2(tmp_path / "p.p2")
+    par.write_yaml(tmp_path / "p.yaml")
+    for f in ("p.p2", "p.yaml"):
+        back = Parameters(filepath=tmp_path / f)
+        for k in ("hstart", "hfinal", "hstep", "iter_max", "tol_fun", "precond_iter"):
+            assert getattr(back, k) == getattr(par, k)
+        assert back.m == pytest.approx(par.m)
+    ref = Parameters(filepath=golden / "io" / "cube.p2")
+    assert ref.h == pytest.approx(np.array([0.01745, 0, 0.99984]) / np.linalg.norm([0.01745, 0, 0.99984]))
+    # the loop-script reader agrees with the oracle's restatement of scripts/tools.py
+    p = runner.read_script_params(golden / "loop_cube.p2")
+    q = O.read_params((golden / "loop_cube.p2").read_text())
+    for k in ("hdir", "hstart", "hfinal", "hstep", "mstep", "mfinal", "tol_fun", "tol_u", "precond_iter", "hmag_on"):
+        assert p[k] == q[k]
+
+
+def test_fly_roundtrip(cube_mesh, tmp_path):
+    X, T, tag = cube_mesh
+    fly.write_mesh(tmp_path / "c.fly", X, T, tag)
+    X2, T2, tag2 = fly.read_mesh(tmp_path / "c.fly")
+    assert np.array_equal(X, X2) and np.array_equal(T, T2) and np.array_equal(tag, tag2)
+
+
+def test_vtu_roundtrip(tmp_path):
+    X, T = synthetic.cube_grid(2, 4.0)
+    m = np.random.default_rng(1).standard_normal(3 * len(X))
+    u = np.arange(len(X), dtype=float)
+    vtu.write_vtu(tmp_path / "s_0001.vtu", X, T, np.ones(len(T)), {"m": m, "u": u})
+    pd = vtu.read_point_data(tmp_path / "s_0001.vtu")
+    np.testing.assert_allclose(pd["m"], m, rtol=1e-6)
+    np.testing.assert_allclose(pd["u"], u, rtol=1e-6)
+
+
+@pytest.mark.parametrize("n", [4, 7])
+def test_synthetic_cube_takes_airbox_branch(n):
+    X, T = synthetic.cube_grid(n, 20.0)
+    assert X.shape[0] == (n + 1) ** 3 and T.shape[0] == 6 * n**3
+    r = np.linalg.norm(X, axis=1)
+    assert (r == r.max()).sum() == 8
+    P = X[T]
+    det = np.einsum("ij,ij->i", P[:, 1] - P[:, 0], np.cross(P[:, 2] - P[:, 0], P[:, 3] - P[:, 0]))
+    assert (det > 0).all()
+    assert np.isclose(det.sum() / 6, 20.0**3)
+    P_ = O.Problem(X, T, np.ones(len(T), np.int32), [[0, 0, 4.3e6, 0, 1.61, 7.7e-12]])
+    assert P_.airbox and P_.bnd.sum() == (n + 1) ** 3 - (n - 1) ** 3
+
+
+def test_multigrain_labels():
+    X, T, tag, rows, m0 = synthetic.multigrain(n=12, L=40.0, grains=5, seed=3)
+    assert len(rows) == len(np.unique(tag))
+    assert tag.max() == 6 and (tag == 6).any()  # boundary phase present
+    assert np.allclose(np.linalg.norm(m0.reshape(-1, 3), axis=1), 1.0)
