@@ -1,0 +1,338 @@
+"""Benchmark of the hysteresis hot path: field steps per second on the B200 path.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+                    [--workload multigrain|single]
+
+A step is one full field sweep of the workload (the reference's loop, scripts/loop.py:71-142,
+run to the last field value).  The default workload is the multigrain cube: 80 nm edge,
+32^3 cells x 6 tets (196,608 tets, 35,937 nodes), 8 seeded Voronoi grains with easy axes in
+a 15 degree cone, a 2 nm grain-boundary phase (A=2e-12 J/m, K1=0, Js=0.5 T), field along z
+tilted 1 degree toward x, +8 T -> -8 T in 0.1 T steps (161 field steps), FP64.  Inputs are
+seeded synthetic data of those shapes.
+
+``value`` is whole-job field steps/s with the mesh operators resident in HBM (device time
+from CUDA events on the library's stream), ``e2e`` the same through the public API from host
+buffers (mesh build + state upload + sweep + result read-back), ``cpu_baseline`` the CPU
+oracle on a bounded sample.  Multi-GPU runs are independent replicas (one sweep per rank,
+no collective on the data path).  ``--impl reference`` times the CPU oracle alone (the
+reference's algorithm restated; its own JAX/escript stack is not installable here).
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import pathlib
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = pathlib.Path(__file__).resolve().parent
+for _p in (ROOT, ROOT / "mammos-mumag_b200"):
+    if str(_p) not in sys.path:
+        sys.path.insert(0, str(_p))
+
+import numpy as np  # noqa: E402
+
+METRIC = "field steps/s + PCG iters/solve: learned+mixed vs plain FP64 GPU at |ΔHc|<1%"
+UNIT = "field steps/s"
+L2_FLUSH_BYTES = 256 << 20
+
+
+def workload(name: str, seed: int):
+    from mammos_mumag import synthetic
+
+    if name == "single":
+        X, T, tag, krn, m0 = synthetic.single_grain(16, 20.0, seed=seed)
+        hdir = [0.0, 0.0, 1.0]
+        sweep = dict(hstart=8.0, hfinal=-8.0, hstep=-0.2, mstep=0.4, mfinal=-2.0)
+        desc = ("single grain 20 nm, 16^3 x 6 tets (24,576 tets, 4,913 nodes), Js=1.61 T, "
+                "A=7.7e-12 J/m, K1=4.3e6 J/m^3, +8 -> -8 T in 0.2 T steps (81 field steps)")
+    else:
+        X, T, tag, krn, m0 = synthetic.multigrain(n=32, L=80.0, grains=8, cone_deg=15.0, gb=2.0, seed=seed)
+        d = np.radians(1.0)
+        hdir = [float(np.sin(d)), 0.0, float(np.cos(d))]
+        sweep = dict(hstart=8.0, hfinal=-8.0, hstep=-0.1, mstep=0.4, mfinal=-2.0)
+        desc = ("multigrain 80 nm, 32^3 x 6 tets (196,608 tets, 35,937 nodes), 8 Voronoi grains "
+                "(15 deg cone) + 2 nm grain-boundary phase, field 1 deg off z, +8 -> -8 T in 0.1 T "
+                "steps (161 field steps)")
+    return X, T, tag, krn, m0, hdir, sweep, desc
+
+
+def hc_mr(rows):
+    """Coercive field |mu0 H| at the zero crossing of mh and remanence mh(H=0), linear
+    interpolation between adjacent field steps."""
+    h, mh = rows[:, 1], rows[:, 2]
+    hc = mr = float("nan")
+    for i in range(len(h) - 1):
+        if mh[i] > 0 >= mh[i + 1] and np.isnan(hc):
+            hc = abs(h[i] + (h[i + 1] - h[i]) * mh[i] / (mh[i] - mh[i + 1]))
+        if h[i] >= 0 >= h[i + 1] and np.isnan(mr) and h[i] != h[i + 1]:
+            mr = mh[i] + (mh[i + 1] - mh[i]) * (0 - h[i]) / (h[i + 1] - h[i])
+    return hc, mr
+
+
+def algorithmic_bytes(steps, Z: int, N: int, s: int = 8) -> float:
+    """Compulsory bytes of the persistent field-step kernel, summed over its work counters.
+
+    Z = unpadded node-pair entries of the SELL pattern, N = nodes, s = value bytes.
+    Per Poisson PCG iteration: one S SpMV Z(s+4) + 4(N+1) + 2Ns and the fused vector
+    update 9Ns.  Per energy evaluation outside the PCG: divergence + initial residual
+    Z(4s+4) + 5Ns, exchange/anisotropy/gradient gathers Z(10s+4) + 14Ns, the normalised
+    trial point 9Ns.  Per M_inv iteration: the C SpMV Z(7s+4) + 6Ns and ~8 three-vector
+    passes 24Ns.  Per NCG iteration: ~12 three-vector passes 36Ns.
+    """
+    pcg = sum(st["pcg_iters"] for st in steps)
+    ev = sum(st["evals"] for st in steps)
+    mi = sum(st["minv_iters"] for st in steps)
+    ncg = sum(st["ncg_iters"] for st in steps)
+    b = pcg * (Z * (s + 4) + 4 * (N + 1) + 2 * N * s + 9 * N * s)
+    b += ev * (Z * (4 * s + 4) + 5 * N * s + Z * (10 * s + 4) + 14 * N * s + 9 * N * s)
+    b += mi * (Z * (7 * s + 4) + 30 * N * s)
+    b += ncg * 36 * N * s
+    return float(b)
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.rows = []
+        self._stop = threading.Event()
+        self._t = threading.Thread(target=self._run, daemon=True)
+
+    def _run(self):
+        while not self._stop.is_set():
+            try:
+                out = subprocess.run(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
+                                      "--format=csv,noheader,nounits"], capture_output=True, text=True, timeout=5)
+                for ln in out.stdout.strip().splitlines():
+                    self.rows.append([x.strip() for x in ln.split(",")])
+            except Exception:
+                pass
+            self._stop.wait(0.2)
+
+    def __enter__(self):
+        self._t.start()
+        return self
+
+    def __exit__(self, *exc):
+        self._stop.set()
+        self._t.join(timeout=10)
+
+    def summary(self):
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"], "samples": 0}
+        sm = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in self.rows for k in range(4) if len(r) > 5 + k and r[5 + k] == "Active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.rows)}
+
+
+def cpu_sample(name: str, n_field_steps: int, seed: int = 0):
+    """The CPU oracle (NumPy/SciPy restatement of the reference's loop) on the first
+    ``n_field_steps`` field steps of the workload.  Returns (field steps/s, seconds, threads)."""
+    import oracle as O
+
+    X, T, tag, krn, m0, hdir, sweep, _ = workload(name, seed)
+    P = O.Problem(X, T, tag, krn)
+    par = dict(hdir=hdir, tol_fun=1e-10, tol_u=1e-10, precond_iter=10, hmag_on=1, m=[0, 0, 1.0], **sweep)
+    t = time.perf_counter()
+    rows, _ = O.run_loop(P, par, m0=m0, max_steps=n_field_steps)
+    dt = time.perf_counter() - t
+    return len(rows) / dt, dt, len(rows)
+
+
+def dist_setup():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("gloo", timeout=datetime.timedelta(seconds=600))
+    return world, rank, local
+
+
+def dist_max(x: float, world: int) -> float:
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([x], dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def dist_barrier(world: int):
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.barrier()
+
+
+def run_reference(args, world, rank):
+    if rank != 0:
+        return 0
+    n_fs = 4
+    for _ in range(args.warmup):
+        cpu_sample(args.workload, n_fs)
+    tot_t, tot_n = 0.0, 0
+    for _ in range(args.steps):
+        _, dt, n = cpu_sample(args.workload, n_fs)
+        tot_t += dt
+        tot_n += n
+    v = tot_n / tot_t
+    _, _, _, _, _, _, _, desc = workload(args.workload, 0)
+    line = {
+        "impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * tot_t / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": desc + f"; each step = the first {n_fs} field steps", "precision": "fp64"},
+        "cpu_baseline": {"value": v, "unit": UNIT, "cores": 1, "kind": "port",
+                         "sample": f"first {n_fs} field steps of the sweep per step, NumPy/SciPy oracle, single thread"},
+        "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_b200(args, world, rank, local):
+    import torch
+
+    from mammos_mumag import _native
+
+    if _native.device_count() < 1:
+        raise RuntimeError("no sm_100 GPU visible")
+    torch.cuda.set_device(local)
+    X, T, tag, krn, m0, hdir, sweep, desc = workload(args.workload, seed=rank)
+    sp = _native.solver_params(hdir=hdir)
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=f"cuda:{local}")
+    mesh = _native.Mesh(X, T, tag, krn, device=local)
+    info = mesh.info()
+    nfs_expected = int(abs(sweep["hfinal"] - sweep["hstart"]) / abs(sweep["hstep"])) + 1
+
+    def one_sweep():
+        mesh.set_state(m0, None, m0)
+        return mesh.loop(sweep["hstart"], sweep["hfinal"], sweep["hstep"], sweep["mstep"], sweep["mfinal"], sp)
+
+    for _ in range(args.warmup):
+        one_sweep()
+    total_ms, nfs, steps_all, rows = 0.0, 0, [], None
+    dist_barrier(world)
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clk:
+        for _ in range(args.steps):
+            flush.fill_(1.0)  # L2 flush between timed sweeps (256 MB > 126 MB L2)
+            torch.cuda.synchronize()
+            mesh.set_state(m0, None, m0)
+            mesh.timer_start()
+            rows, steps = mesh.loop(sweep["hstart"], sweep["hfinal"], sweep["hstep"], sweep["mstep"], sweep["mfinal"], sp)
+            total_ms += mesh.timer_stop()
+            nfs += len(rows)
+            steps_all += steps
+    torch.cuda.synchronize()
+    dist_barrier(world)
+    t_max = dist_max(total_ms, world)
+    value = nfs * world / (t_max * 1e-3)
+    launches = sum(1 for _ in steps_all)
+    kernel_ms = sum(st["device_ms"] for st in steps_all)
+    Z, N = info["nnz"], info["nodes"]
+    ab = algorithmic_bytes(steps_all, Z, N)
+    achieved = ab / (kernel_ms * 1e-3) / 1e9  # GB/s over the kernel's own launch durations
+    peaks = {}
+    try:
+        peaks = json.loads((ROOT / "MEASURED_PEAKS.json").read_text())
+    except Exception:
+        pass
+    peak = float(peaks.get("hbm_gbs", 6650.0))
+    evals = sum(st["evals"] for st in steps_all)
+    pcg = sum(st["pcg_iters"] for st in steps_all)
+    hc, mr = hc_mr(rows)
+    # e2e: the public API from host buffers (pinned), every step: mesh build + upload,
+    # state upload, sweep, result read-back
+    pin = {k: torch.from_numpy(np.ascontiguousarray(v)).pin_memory() for k, v in
+           (("X", X), ("T", np.asarray(T, np.int32)), ("tag", np.asarray(tag, np.int32)), ("m0", m0))}
+    h2d = sum(t.numel() * t.element_size() for t in pin.values()) + 48 * len(krn)
+    e2e_t, e2e_n = 0.0, 0
+    for _ in range(args.steps):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        with _native.Mesh(pin["X"].numpy(), pin["T"].numpy(), pin["tag"].numpy(), krn, device=local) as mm:
+            mm.set_state(pin["m0"].numpy(), None, pin["m0"].numpy())
+            r2, _ = mm.loop(sweep["hstart"], sweep["hfinal"], sweep["hstep"], sweep["mstep"], sweep["mfinal"], sp)
+            mfin, _, _ = mm.get_state()
+        e2e_t += time.perf_counter() - t0
+        e2e_n += len(r2)
+    d2h = 32 * nfs_expected + mfin.nbytes
+    e2e_t = dist_max(e2e_t, world)
+    line = None
+    if rank == 0:
+        cpu = None
+        if world == 1:
+            v, dt, n = cpu_sample(args.workload, 12)
+            cpu = {"value": v, "unit": UNIT, "cores": 1, "kind": "port",
+                   "sample": f"first {n} field steps of the sweep ({dt:.1f} s), NumPy/SciPy oracle, single thread"}
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": t_max / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": desc, "precision": "fp64", "parallelism": f"replicas x{world}",
+                       "l2": "256 MB buffer written between timed sweeps (L2 flush)",
+                       "grid_ctas": info["grid_ctas"], "block_threads": info["block_threads"]},
+            "pcg_iters_per_solve": pcg / evals,
+            "field_steps_per_sweep": nfs // args.steps,
+            "hc_T": hc, "mr_T": mr,
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": None,
+                         "kernel": "k_solve (persistent field step)",
+                         "algorithmic_bytes_per_launch": ab / launches,
+                         "avg_launch_ms": kernel_ms / launches,
+                         "peak_source": "MEASURED_PEAKS.json hbm_gbs" if peaks else "fallback"},
+            "sync_fraction": sum(st["sync_ns"] for st in steps_all) / max(1, sum(st["kernel_ns"] for st in steps_all)),
+            "cpu_baseline": cpu,
+            "e2e": {"value": e2e_n * world / e2e_t, "unit": UNIT, "h2d_bytes_per_step": int(h2d),
+                    "d2h_bytes_per_step": int(d2h)},
+            "gpu_launches": launches,
+            "clocks": clk.summary(),
+        }
+        print(json.dumps(line), flush=True)
+    mesh.close()
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
+    ap.add_argument("--workload", choices=["multigrain", "single"], default="multigrain")
+    args = ap.parse_args()
+    world, rank, local = dist_setup()
+    try:
+        if args.impl == "reference":
+            return run_reference(args, world, rank)
+        return run_b200(args, world, rank, local)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -81,6 +81,10 @@ typedef struct {
   int64_t pcg_iters;   /* Poisson PCG iterations summed over the evaluations */
   int64_t ls_shrinks;  /* line-search step halvings */
   int64_t minv_iters;  /* truncated-CG iterations inside M_inv */
+  int64_t kernel_ns;   /* device time of the persistent launch (CTA 0, %globaltimer) */
+  int64_t sync_ns;     /* of which spent in grid barriers / reductions */
+  int64_t barriers;    /* grid barriers executed */
+  double device_ms;    /* duration of the launch from CUDA events on the launching stream */
   int status;          /* MM_OK, MM_NONFINITE or MM_TIMEOUT */
 } mm_step_result;
 
@@ -191,6 +195,12 @@ mm_status mm_minimize(mm_mesh* mesh, double h, const mm_solver_params* sp, mm_st
 mm_status mm_loop(mm_mesh* mesh, const mm_loop_params* lp, const mm_solver_params* sp,
                   mm_record* rec, int32_t* nrec, mm_step_result* steps, mm_snapshot_cb cb,
                   void* user);
+
+/* Device timing on the mesh's CUDA stream: mm_timer_start records an event; mm_timer_stop
+ * records a second one, waits for it and returns the elapsed milliseconds between them.
+ * Used to time field sweeps with CUDA events on the stream the kernels run on. */
+mm_status mm_timer_start(mm_mesh* mesh);
+mm_status mm_timer_stop(mm_mesh* mesh, double* elapsed_ms);
 
 #ifdef __cplusplus
 }

@@ -90,6 +90,12 @@ void release(DevMesh& m) {
   m.h_resd = nullptr;
   m.h_resi = nullptr;
   m.h_flags = nullptr;
+  if (m.evk0) cudaEventDestroy(m.evk0);
+  if (m.evk1) cudaEventDestroy(m.evk1);
+  m.evk0 = m.evk1 = nullptr;
+  if (m.ev0) cudaEventDestroy(m.ev0);
+  if (m.ev1) cudaEventDestroy(m.ev1);
+  m.ev0 = m.ev1 = nullptr;
   if (m.stream) cudaStreamDestroy(m.stream);
   m.stream = nullptr;
 }
@@ -125,11 +131,14 @@ void check_params(const mm_solver_params* sp) {
 // Run one persistent launch and collect its status.
 mm_status run(DevMesh& m, const SolveArgs& a) {
   MM_CK(cudaSetDevice(m.device));
+  if (!m.evk0) MM_CK(cudaEventCreate(&m.evk0));
+  if (!m.evk1) MM_CK(cudaEventCreate(&m.evk1));
   MM_CK(solver_launch(m, a));
   MM_CK(cudaMemcpyAsync(m.h_resd, m.resd, 2 * sizeof(double), cudaMemcpyDeviceToHost, m.stream));
   MM_CK(cudaMemcpyAsync(m.h_resi, m.resi, 8 * sizeof(long long), cudaMemcpyDeviceToHost, m.stream));
   MM_CK(cudaMemcpyAsync(m.h_flags, m.flags, 2 * sizeof(int), cudaMemcpyDeviceToHost, m.stream));
   MM_CK(cudaStreamSynchronize(m.stream));
+  MM_CK(cudaEventElapsedTime(&m.last_launch_ms, m.evk0, m.evk1));
   const int st = m.h_flags[FLAG_STATUS];
   if (st == MM_TIMEOUT) return fail(MM_TIMEOUT, "a grid barrier of the persistent solver kernel timed out");
   return st;
@@ -279,17 +288,17 @@ mm_status mm_mesh_create(const double* X, int64_t N, const int32_t* T, const int
     upload(m.etag, h.etag, m.stream);
     upload(m.dmats, m.mats, m.stream);
     assemble_operators(m);
-    // solver state: 12 three-vectors and 5 node vectors
+    // solver state: 12 three-vectors and 8 node vectors
     const size_t np = h.Npad;
-    dalloc(m.ws, 41 * np);
-    MM_CK(cudaMemsetAsync(m.ws, 0, sizeof(double) * 41 * np, m.stream));
+    dalloc(m.ws, 44 * np);
+    MM_CK(cudaMemsetAsync(m.ws, 0, sizeof(double) * 44 * np, m.stream));
     double* p = m.ws;
     double** v3[] = {&m.x, &m.x1, &m.g, &m.g1, &m.d, &m.gf, &m.mbar, &m.zp, &m.tr, &m.tz, &m.td, &m.tBd};
     for (double** q : v3) {
       *q = p;
       p += 3 * np;
     }
-    double** v1[] = {&m.u, &m.pr, &m.pz, &m.pp, &m.pq};
+    double** v1[] = {&m.u, &m.pr[0], &m.pr[1], &m.pw[0], &m.pw[1], &m.ps[0], &m.ps[1], &m.pp};
     for (double** q : v1) {
       *q = p;
       p += np;
@@ -491,6 +500,10 @@ mm_status mm_minimize(mm_mesh* mesh, double h, const mm_solver_params* sp, mm_st
     res->pcg_iters = m.h_resi[2];
     res->ls_shrinks = m.h_resi[3];
     res->minv_iters = m.h_resi[4];
+    res->kernel_ns = m.h_resi[5];
+    res->sync_ns = m.h_resi[6];
+    res->barriers = m.h_resi[7];
+    res->device_ms = m.last_launch_ms;
     res->status = st;
   }
   if (st == MM_NONFINITE) return fail(st, "energy is not finite");
@@ -525,6 +538,10 @@ mm_status mm_loop(mm_mesh* mesh, const mm_loop_params* lp, const mm_solver_param
     r.pcg_iters = m.h_resi[2];
     r.ls_shrinks = m.h_resi[3];
     r.minv_iters = m.h_resi[4];
+    r.kernel_ns = m.h_resi[5];
+    r.sync_ns = m.h_resi[6];
+    r.barriers = m.h_resi[7];
+    r.device_ms = m.last_launch_ms;
     r.status = st;
     if (st != MM_OK) {
       if (steps) steps[idx] = r;
@@ -553,6 +570,34 @@ mm_status mm_loop(mm_mesh* mesh, const mm_loop_params* lp, const mm_solver_param
     *nrec = (int32_t)(idx + 1);
     hext = hext + lp->hstep;
   }
+  return MM_OK;
+  API_END
+}
+
+mm_status mm_timer_start(mm_mesh* mesh) {
+  API_BEGIN
+  check_mesh(mesh);
+  DevMesh& m = mesh->dm;
+  MM_CK(cudaSetDevice(m.device));
+  if (!m.ev0) MM_CK(cudaEventCreate(&m.ev0));
+  if (!m.ev1) MM_CK(cudaEventCreate(&m.ev1));
+  MM_CK(cudaEventRecord(m.ev0, m.stream));
+  return MM_OK;
+  API_END
+}
+
+mm_status mm_timer_stop(mm_mesh* mesh, double* elapsed_ms) {
+  API_BEGIN
+  check_mesh(mesh);
+  if (!elapsed_ms) throw std::runtime_error("elapsed_ms is NULL");
+  DevMesh& m = mesh->dm;
+  if (!m.ev0) throw std::runtime_error("mm_timer_start was not called");
+  MM_CK(cudaSetDevice(m.device));
+  MM_CK(cudaEventRecord(m.ev1, m.stream));
+  MM_CK(cudaEventSynchronize(m.ev1));
+  float ms = 0.f;
+  MM_CK(cudaEventElapsedTime(&ms, m.ev0, m.ev1));
+  *elapsed_ms = ms;
   return MM_OK;
   API_END
 }

@@ -47,11 +47,14 @@ struct SolveArgs {
   double V;
   // vectors; 3-vectors are 3 planes of Npad
   double *x, *x1, *g, *g1, *d, *gf, *mbar, *zp, *tr, *tz, *td, *tBd;
-  double *u, *pr, *pz, *pp, *pq;
+  double* u;                        // magnetostatic potential (PCG solution)
+  double *pr[2], *pw[2], *ps[2], *pp;  // PCG vectors, r/w/s double-buffered by iteration parity
   // grid synchronisation
-  unsigned long long* bar;  // arrival counter, zeroed before each launch
-  double* red;              // [2][kMaxRed][gridDim.x] reduction partials
-  int* flags;               // [0] abort, [1] status
+  unsigned long long* bar;    // barrier arrival counter, zeroed before each launch
+  double* red;                // [2][kMaxRed][gridDim.x] reduction partials
+  int* flags;                 // [0] abort, [1] status
+  int stage;                  // 1: the CTA's SELL columns + Poisson values live in shared memory
+  int64_t stage_max;          // entries of the largest CTA (shared-memory layout)
   // control
   int mode;  // 0 energy+gradient, 1 M_inv, 2 minimise (one field step)
   double h, hdir[3], tol_fun, sqrt_tol, cbrt_tol, tol_u;
@@ -86,7 +89,7 @@ struct DevMesh {
   // state and workspace
   double* ws = nullptr;  // all solver vectors
   double *x, *x1, *g, *g1, *d, *gf, *mbar, *zp, *tr, *tz, *td, *tBd;
-  double *u, *pr, *pz, *pp, *pq;
+  double *u, *pr[2], *pw[2], *ps[2], *pp;
   unsigned long long* bar = nullptr;
   double* red = nullptr;
   int* flags = nullptr;
@@ -98,6 +101,12 @@ struct DevMesh {
   int* h_flags = nullptr;
   // launch shape of the persistent kernel
   int grid = 0, block = 0;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;    // mm_timer_*
+  cudaEvent_t evk0 = nullptr, evk1 = nullptr;  // around each persistent launch
+  float last_launch_ms = 0.f;
+  int stage = 0;
+  int64_t stage_max = 0;
+  size_t smem = 0;
 };
 
 // assemble.cu

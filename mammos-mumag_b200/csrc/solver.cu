@@ -33,29 +33,40 @@ namespace mumag {
 
 namespace {
 
-constexpr unsigned kSpinLimit = 1u << 23;  // bounded wait per barrier (seconds)
+constexpr unsigned kSpinLimit = 1u << 23;  // bounded wait per barrier (several seconds)
 
+// Grid barrier: one arrival counter (red.release), thread 0 of every CTA polls it with
+// acquire loads.  A grid reduction publishes the CTA's partials before arriving and reads
+// all partials after the barrier, summing them in CTA order: every CTA gets bit-identical
+// totals.  Two partial sets alternate: a CTA can only start writing set r+2 after every
+// CTA has passed barrier r+1, i.e. after every CTA finished reading set r.
 struct Sync {
   unsigned long long* bar;
-  double* red;
+  double* red;  // [2][kMaxRed][nblk]
   int* flags;
   unsigned long long epoch;
   int nblk, blk, slot;
+  unsigned long long t_sync;  // ns spent in grid synchronisation (thread 0)
 };
+
+__device__ __forceinline__ unsigned long long globaltimer() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %globaltimer;" : "=l"(t));
+  return t;
+}
 
 __device__ __forceinline__ unsigned long long ld_acquire_u64(const unsigned long long* p) {
   unsigned long long v;
   asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
   return v;
 }
-
 __device__ __forceinline__ void red_release_add_u64(unsigned long long* p, unsigned long long v) {
   asm volatile("red.release.gpu.global.add.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
 }
 
-// Grid-wide barrier; false if the kernel is aborting.
-__device__ bool grid_barrier(Sync& s) {
+__device__ __noinline__ bool grid_barrier(Sync& s) {
   __shared__ int sh_abort;
+  const unsigned long long t0 = threadIdx.x == 0 ? globaltimer() : 0ull;
   __syncthreads();
   if (threadIdx.x == 0) {
     s.epoch += 1;
@@ -63,22 +74,22 @@ __device__ bool grid_barrier(Sync& s) {
     __threadfence();
     red_release_add_u64(s.bar, 1ull);
     int ab = 0;
-    unsigned it = 0;
-    while (ld_acquire_u64(s.bar) < target) {
-      if (*((volatile int*)&s.flags[FLAG_ABORT])) {
+    for (unsigned it = 0; ld_acquire_u64(s.bar) < target; ++it) {
+      if ((it & 63) == 63 && *((volatile int*)&s.flags[FLAG_ABORT])) {
         ab = 1;
         break;
       }
-      if (++it > kSpinLimit) {
+      if (it > kSpinLimit) {
         atomicCAS(&s.flags[FLAG_STATUS], 0, (int)MM_TIMEOUT);
         atomicExch(&s.flags[FLAG_ABORT], 1);
         ab = 1;
         break;
       }
-      if (it > 32) __nanosleep(it > 4096 ? 256 : 32);
+      if (it > 64) __nanosleep(it > 8192 ? 256 : 16);
     }
     __threadfence();
     sh_abort = ab;
+    s.t_sync += globaltimer() - t0;
   }
   __syncthreads();
   return sh_abort == 0;
@@ -93,10 +104,10 @@ __device__ __forceinline__ double warp_max(double v) {
   return v;
 }
 
-// Deterministic grid reduction of K values; bit k of maxmask selects max instead of sum.
-// On return v[] holds the grid totals, identical in every thread of every CTA.
+// Deterministic grid reduction of K values (bit k of maxmask: max instead of sum); also a
+// grid barrier.  On return v[] holds totals identical in every thread of every CTA.
 template <int K>
-__device__ bool grid_reduce(Sync& s, double (&v)[K], unsigned maxmask) {
+__device__ __noinline__ bool grid_reduce(Sync& s, double (&v)[K], unsigned maxmask) {
   __shared__ double sh[32][kMaxRed];
   __shared__ double res[kMaxRed];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
@@ -106,26 +117,26 @@ __device__ bool grid_reduce(Sync& s, double (&v)[K], unsigned maxmask) {
     if (lane == 0) sh[warp][k] = w;
   }
   __syncthreads();
+  double* set = s.red + (size_t)s.slot * kMaxRed * s.nblk;
   if (threadIdx.x < K) {
     const int k = threadIdx.x;
     double a = sh[0][k];
     for (int w = 1; w < nw; ++w) a = ((maxmask >> k) & 1) ? fmax(a, sh[w][k]) : a + sh[w][k];
-    s.red[((size_t)s.slot * kMaxRed + k) * s.nblk + s.blk] = a;
+    set[(size_t)k * s.nblk + s.blk] = a;
   }
   if (!grid_barrier(s)) return false;
-  if (warp == 0) {
+  if (warp < K) {  // warp k sums value k over the CTAs, in CTA order per lane, then a fixed tree
+    const int k = warp;
+    const bool mx = (maxmask >> k) & 1;
+    const double* p = set + (size_t)k * s.nblk;
+    double got[8];
 #pragma unroll
-    for (int k = 0; k < K; ++k) {
-      const bool mx = (maxmask >> k) & 1;
-      double a = mx ? 0.0 : 0.0;
-      const double* p = s.red + ((size_t)s.slot * kMaxRed + k) * s.nblk;
-      for (int b = lane; b < s.nblk; b += 32) {
-        const double t = __ldcg(p + b);
-        a = mx ? fmax(a, t) : a + t;
-      }
-      a = mx ? warp_max(a) : warp_sum(a);
-      if (lane == 0) res[k] = a;
-    }
+    for (int t = 0; t < 8; ++t) got[t] = (lane + 32 * t < s.nblk) ? __ldcg(p + lane + 32 * t) : 0.0;
+    double a = got[0];
+#pragma unroll
+    for (int t = 1; t < 8; ++t) a = mx ? fmax(a, got[t]) : a + got[t];
+    a = mx ? warp_max(a) : warp_sum(a);
+    if (lane == 0) res[k] = a;
   }
   __syncthreads();
 #pragma unroll
@@ -148,33 +159,45 @@ struct Ctx {
   const SolveArgs& a;
   Sync sy;
   int s0, s1, warp, nwarps, lane;
+  // The CTA's SELL columns and Poisson values, staged in shared memory for the whole
+  // launch when they fit (index with entry - cbase), else the global arrays (cbase = 0).
+  const int32_t* scol;
+  const double* sS;
+  int64_t cbase;
   long long evals = 0, pcg_iters = 0, minv_iters = 0, shrinks = 0;
   __device__ Ctx(const SolveArgs& args) : a(args) {}
 };
 
+// Rows of this CTA: warp w takes slices s0+w, s0+w+nwarps, ...; lane = row in slice.
+// off_ is the global SELL entry of (row, k=0); loff_ the staged one.
 #define FOR_ROWS(c)                                                       \
   for (int s_ = (c).s0 + (c).warp; s_ < (c).s1; s_ += (c).nwarps) {      \
     const int i = s_ * 32 + (c).lane;                                     \
     const int64_t off_ = (c).a.sl_off[s_] + (c).lane;                     \
-    const int w_ = (c).a.sl_w[s_];
+    const int64_t loff_ = off_ - (c).cbase;                               \
+    const int w_ = (c).a.sl_w[s_];                                        \
+    (void)loff_;
 #define END_ROWS }
 #define ENTRY(k) (off_ + 32 * (int64_t)(k))
+#define LENTRY(k) (loff_ + 32 * (int64_t)(k))
 #define CHECK(x) \
   if (!(x)) return false
 
 __device__ __forceinline__ const double* plane(const SolveArgs& a, int p) { return a.vals + (size_t)p * a.nent; }
 
 // C v at row i (exchange scalar + anisotropy blocks), v a 3-vector
-__device__ __forceinline__ void apply_C_row(const SolveArgs& a, const double* v, int64_t off, int w,
+__device__ __forceinline__ void apply_C_row(const Ctx& c, const double* v, int64_t off, int64_t loff, int w,
                                             double o[3]) {
+  const SolveArgs& a = c.a;
   const double* Aex = plane(a, P_AEX);
   const double* K = plane(a, P_K);
   const int64_t ps = a.nent;
   const int n = a.Npad;
   double o0 = 0, o1 = 0, o2 = 0;
+#pragma unroll 4
   for (int k = 0; k < w; ++k) {
     const int64_t e = off + 32 * (int64_t)k;
-    const int j = __ldg(a.col + e);
+    const int j = c.scol[loff + 32 * (int64_t)k];
     const double v0 = v[j], v1 = v[n + j], v2 = v[2 * n + j];
     const double ax = __ldg(Aex + e);
     const double k0 = __ldg(K + e), k1 = __ldg(K + ps + e), k2 = __ldg(K + 2 * ps + e);
@@ -189,110 +212,118 @@ __device__ __forceinline__ void apply_C_row(const SolveArgs& a, const double* v,
 }
 
 // ---------------------------------------------------------------------------------------
-// Poisson PCG (jax.scipy.sparse.linalg.cg semantics, M = x * (1/diag S))
+// Poisson PCG: jax.scipy.sparse.linalg.cg as called at scripts/solvers.py:221-231 --
+// Jacobi preconditioner z = r * (1/diag S), warm start, stop when r.r <= tol_u^2 b.b or
+// after max_pcg iterations -- in the Chronopoulos-Gear arrangement, which computes the
+// same iterates with the two inner products of an iteration in one reduction:
+//   s_i = w_i + b_i s_{i-1},  p_i = z_i + b_i p_{i-1},  u += a_i p_i,  r_{i+1} = r_i - a_i s_i,
+//   z_{i+1} = r_{i+1}/diag,  w_{i+1} = S z_{i+1},
+//   g_{i+1} = r.z, d_{i+1} = w.z, rr = r.r   (one reduction),
+//   b_{i+1} = g_{i+1}/g_i,  a_{i+1} = g_{i+1} / (d_{i+1} - b_{i+1} g_{i+1}/a_i).
+// The gather of w_{i+1} = S z_{i+1} needs z_{i+1} at neighbour rows before their owners
+// have produced it; each CTA recomputes it from the neighbours' r_i, w_i, s_{i-1}, which
+// the previous iteration left in the other half of double buffers.  So an iteration needs
+// one grid synchronisation instead of two.
 // ---------------------------------------------------------------------------------------
-// b = sum_k dk x_k, r = b - S u, z = r/diag, p = z; returns gamma = r.z, rr = r.r, bb = b.b
-__device__ bool pcg_begin(Ctx& c, const double* x, double& gamma, double& rr, double& bb) {
-  const SolveArgs& a = c.a;
-  const double* S = plane(a, P_S);
-  const double* Dk = plane(a, P_D);
-  const int64_t ps = a.nent;
-  const int n = a.Npad;
-  double pg = 0, pr2 = 0, pb = 0;
-  FOR_ROWS(c)
-  double b = 0, su = 0;
-  for (int k = 0; k < w_; ++k) {
-    const int64_t e = ENTRY(k);
-    const int j = __ldg(a.col + e);
-    b += __ldg(Dk + e) * x[j] + __ldg(Dk + ps + e) * x[n + j] + __ldg(Dk + 2 * ps + e) * x[2 * n + j];
-    su += __ldg(S + e) * a.u[j];
-  }
-  const double r = b - su;
-  const double z = r * __ldg(a.invdS + i);
-  a.pr[i] = r;
-  a.pz[i] = z;
-  a.pp[i] = z;
-  pg += r * z;
-  pr2 += r * r;
-  pb += b * b;
-  END_ROWS
-  double v[3] = {pg, pr2, pb};
-  CHECK(grid_reduce<3>(c.sy, v, 0u));
-  gamma = v[0];
-  rr = v[1];
-  bb = v[2];
-  return true;
-}
-
-// first: q = S p.  otherwise: q = S z + beta q, p = z + beta p.  returns p.q
-__device__ bool pcg_direction(Ctx& c, bool first, double beta, double& pq) {
-  const SolveArgs& a = c.a;
-  const double* S = plane(a, P_S);
-  const double* src = first ? a.pp : a.pz;
-  double part = 0;
-  FOR_ROWS(c)
-  double acc = 0;
-  for (int k = 0; k < w_; ++k) {
-    const int64_t e = ENTRY(k);
-    acc += __ldg(S + e) * src[__ldg(a.col + e)];
-  }
-  double p, q;
-  if (first) {
-    p = a.pp[i];
-    q = acc;
-  } else {
-    q = acc + beta * a.pq[i];
-    p = a.pz[i] + beta * a.pp[i];
-    a.pp[i] = p;
-  }
-  a.pq[i] = q;
-  part += p * q;
-  END_ROWS
-  double v[1] = {part};
-  CHECK(grid_reduce<1>(c.sy, v, 0u));
-  pq = v[0];
-  return true;
-}
-
-// u += alpha p, r -= alpha q, z = r/diag; returns gamma' = r.z, rr = r.r
-__device__ bool pcg_update(Ctx& c, double alpha, double& gamma, double& rr) {
-  const SolveArgs& a = c.a;
-  double pg = 0, pr2 = 0;
-  FOR_ROWS(c)
-  (void)off_;
-  (void)w_;
-  a.u[i] = a.u[i] + alpha * a.pp[i];
-  const double r = a.pr[i] - alpha * a.pq[i];
-  const double z = r * __ldg(a.invdS + i);
-  a.pr[i] = r;
-  a.pz[i] = z;
-  pg += r * z;
-  pr2 += r * r;
-  END_ROWS
-  double v[2] = {pg, pr2};
-  CHECK(grid_reduce<2>(c.sy, v, 0u));
-  gamma = v[0];
-  rr = v[1];
-  return true;
+struct CGNext {
+  double s, r, z;
+};
+__device__ __forceinline__ CGNext cg_next(double r, double w, double sprev, double invd, double alpha, double beta) {
+  CGNext o;
+  o.s = w + beta * sprev;
+  o.r = r - alpha * o.s;
+  o.z = o.r * invd;
+  return o;
 }
 
 __device__ bool pcg_solve(Ctx& c, const double* x) {
   const SolveArgs& a = c.a;
-  double gamma, rr, bb, pq;
-  CHECK(pcg_begin(c, x, gamma, rr, bb));
+  const double* Dk = plane(a, P_D);
+  const int64_t ps = a.nent;
+  const int n = a.Npad;
+  // phase A: b = sum_k dk x_k, r0 = b - S u
+  double gamma, rr, bb;
+  {
+    double pg = 0, pr2 = 0, pb = 0;
+    FOR_ROWS(c)
+    double b = 0, su = 0;
+#pragma unroll 4
+    for (int k = 0; k < w_; ++k) {
+      const int64_t e = ENTRY(k);
+      const int j = c.scol[LENTRY(k)];
+      b += __ldg(Dk + e) * x[j] + __ldg(Dk + ps + e) * x[n + j] + __ldg(Dk + 2 * ps + e) * x[2 * n + j];
+      su += c.sS[LENTRY(k)] * a.u[j];
+    }
+    const double r = b - su;
+    a.pr[0][i] = r;
+    pg += r * (r * __ldg(a.invdS + i));
+    pr2 += r * r;
+    pb += b * b;
+    END_ROWS
+    double v[3] = {pg, pr2, pb};
+    CHECK(grid_reduce<3>(c.sy, v, 0u));
+    gamma = v[0];
+    rr = v[1];
+    bb = v[2];
+  }
   const double atol2 = fmax(a.tol_u * a.tol_u * bb, 0.0);
   int k = 0;
   if (!(rr > atol2 && k < a.max_pcg)) return true;
-  CHECK(pcg_direction(c, true, 0.0, pq));
-  for (;;) {
-    const double alpha = gamma / pq;
-    double g2;
-    CHECK(pcg_update(c, alpha, g2, rr));
+  // phase B: w0 = S z0, delta0 = w0.z0; s_{-1} = p_{-1} = 0
+  double delta;
+  {
+    double pd = 0;
+    FOR_ROWS(c)
+    double acc = 0;
+#pragma unroll 8
+    for (int k2 = 0; k2 < w_; ++k2) {
+      const int j = c.scol[LENTRY(k2)];
+      acc += c.sS[LENTRY(k2)] * (a.pr[0][j] * __ldg(a.invdS + j));
+    }
+    a.pw[0][i] = acc;
+    a.ps[1][i] = 0.0;
+    a.pp[i] = 0.0;
+    pd += acc * (a.pr[0][i] * __ldg(a.invdS + i));
+    END_ROWS
+    double v[1] = {pd};
+    CHECK(grid_reduce<1>(c.sy, v, 0u));
+    delta = v[0];
+  }
+  double alpha = gamma / delta, beta = 0.0;
+  for (int it = 0;; ++it) {
+    const int cur = it & 1, nxt = cur ^ 1;
+    const double* rc = a.pr[cur];
+    const double* wc = a.pw[cur];
+    const double* sp = a.ps[nxt];
+    double pg = 0, pd = 0, pr2 = 0;
+    FOR_ROWS(c)
+    double acc = 0;
+#pragma unroll 8
+    for (int k2 = 0; k2 < w_; ++k2) {
+      const int j = c.scol[LENTRY(k2)];
+      acc += c.sS[LENTRY(k2)] * cg_next(rc[j], wc[j], sp[j], __ldg(a.invdS + j), alpha, beta).z;
+    }
+    const double invd = __ldg(a.invdS + i);
+    const CGNext o = cg_next(rc[i], wc[i], sp[i], invd, alpha, beta);
+    const double p = rc[i] * invd + beta * a.pp[i];
+    a.pp[i] = p;
+    a.u[i] = a.u[i] + alpha * p;
+    a.pr[nxt][i] = o.r;
+    a.pw[nxt][i] = acc;
+    a.ps[cur][i] = o.s;
+    pg += o.r * o.z;
+    pd += acc * o.z;
+    pr2 += o.r * o.r;
+    END_ROWS
+    double v[3] = {pg, pd, pr2};
+    CHECK(grid_reduce<3>(c.sy, v, 0u));
     ++k;
+    rr = v[2];
     if (!(rr > atol2 && k < a.max_pcg)) break;
-    const double beta = g2 / gamma;
-    gamma = g2;
-    CHECK(pcg_direction(c, false, beta, pq));
+    const double bn = v[0] / gamma;
+    alpha = v[0] / (v[1] - bn * v[0] / alpha);
+    beta = bn;
+    gamma = v[0];
   }
   c.pcg_iters += k;
   return true;
@@ -320,12 +351,13 @@ __device__ bool eval(Ctx& c, const double* x, const double* xref, const double* 
   double pE = 0, pgd = 0, pdx = 0, px = 0, pgi = 0;
   FOR_ROWS(c)
   double gc[3];
-  apply_C_row(a, x, off_, w_, gc);
+  apply_C_row(c, x, off_, loff_, w_, gc);
   double gh0 = 0, gh1 = 0, gh2 = 0;
   if (a.hmag_on > 0) {
+#pragma unroll 4
     for (int k = 0; k < w_; ++k) {
       const int64_t e = ENTRY(k);
-      const double uj = a.u[__ldg(a.col + e)];
+      const double uj = a.u[c.scol[LENTRY(k)]];
       gh0 += __ldg(G + e) * uj;
       gh1 += __ldg(G + ps + e) * uj;
       gh2 += __ldg(G + 2 * ps + e) * uj;
@@ -384,11 +416,12 @@ __device__ bool step_normalize(Ctx& c, double* xout, const double* x, double alp
 // M_inv, scripts/loop.py:40-55 -> truncated_cg_diag_precond_jit, scripts/solvers.py:7-131
 // A v = mbar x ((C v) x mbar) - (mbar . gf) v,  D = exchange diagonal
 // ---------------------------------------------------------------------------------------
-__device__ __forceinline__ void apply_A_row(const SolveArgs& a, const double* mb, const double* v, int i,
-                                            int64_t off, int w, double o[3]) {
+__device__ __forceinline__ void apply_A_row(const Ctx& c, const double* mb, const double* v, int i,
+                                            int64_t off, int64_t loff, int w, double o[3]) {
+  const SolveArgs& a = c.a;
   const int n = a.Npad;
   double cv[3];
-  apply_C_row(a, v, off, w, cv);
+  apply_C_row(c, v, off, loff, w, cv);
   const double m[3] = {mb[i], mb[n + i], mb[2 * n + i]};
   const double md = m[0] * a.gf[i] + m[1] * a.gf[n + i] + m[2] * a.gf[2 * n + i];
   double pr[3];
@@ -440,7 +473,7 @@ __device__ bool minv(Ctx& c, const double* g, const double* mb, double* zout) {
     double pd = 0, prz = 0;
     FOR_ROWS(c)
     double o[3];
-    apply_A_row(a, mb, a.td, i, off_, w_, o);
+    apply_A_row(c, mb, a.td, i, off_, loff_, w_, o);
     for (int q = 0; q < 3; ++q) {
       a.tBd[q * n + i] = o[q];
       pd += a.td[q * n + i] * o[q];
@@ -485,7 +518,7 @@ __device__ bool minv(Ctx& c, const double* g, const double* mb, double* zout) {
     double pd = 0;
     FOR_ROWS(c)
     double o[3];
-    apply_A_row(a, mb, a.tz, i, off_, w_, o);
+    apply_A_row(c, mb, a.tz, i, off_, loff_, w_, o);
     for (int q = 0; q < 3; ++q) {
       const int idx = q * n + i;
       const double dn = -a.tz[idx] + beta * a.td[idx];
@@ -690,7 +723,8 @@ __device__ bool minimize(Ctx& c) {
   return true;
 }
 
-__global__ void __launch_bounds__(512, 1) k_solve(const __grid_constant__ SolveArgs args) {
+__global__ void __launch_bounds__(256, 1) k_solve(const __grid_constant__ SolveArgs args) {
+  extern __shared__ __align__(16) unsigned char smem[];
   Ctx c(args);
   c.sy.bar = args.bar;
   c.sy.red = args.red;
@@ -699,11 +733,31 @@ __global__ void __launch_bounds__(512, 1) k_solve(const __grid_constant__ SolveA
   c.sy.nblk = gridDim.x;
   c.sy.blk = blockIdx.x;
   c.sy.slot = 0;
+  c.sy.t_sync = 0;
+  const unsigned long long t_start = globaltimer();
   c.lane = threadIdx.x & 31;
   c.warp = threadIdx.x >> 5;
   c.nwarps = blockDim.x >> 5;
   c.s0 = (int)(((long long)args.nslices * blockIdx.x) / gridDim.x);
   c.s1 = (int)(((long long)args.nslices * (blockIdx.x + 1)) / gridDim.x);
+  if (args.stage) {
+    const int64_t e0 = args.sl_off[c.s0], n = args.sl_off[c.s1] - e0;
+    double* sS = reinterpret_cast<double*>(smem);
+    int32_t* scol = reinterpret_cast<int32_t*>(smem + sizeof(double) * args.stage_max);
+    const double* S = args.vals + (size_t)P_S * args.nent;
+    for (int64_t t = threadIdx.x; t < n; t += blockDim.x) {
+      sS[t] = __ldg(S + e0 + t);
+      scol[t] = __ldg(args.col + e0 + t);
+    }
+    __syncthreads();
+    c.sS = sS;
+    c.scol = scol;
+    c.cbase = e0;
+  } else {
+    c.sS = args.vals + (size_t)P_S * args.nent;
+    c.scol = args.col;
+    c.cbase = 0;
+  }
   bool ok = true;
   if (args.mode == MODE_EVAL) {
     EvalOut o;
@@ -722,6 +776,9 @@ __global__ void __launch_bounds__(512, 1) k_solve(const __grid_constant__ SolveA
     args.resi[2] = c.pcg_iters;
     args.resi[3] = c.shrinks;
     args.resi[4] = c.minv_iters;
+    args.resi[5] = (long long)(globaltimer() - t_start);  // kernel ns (CTA 0)
+    args.resi[6] = (long long)c.sy.t_sync;                // of which in grid barriers
+    args.resi[7] = (long long)c.sy.epoch;                 // grid barriers executed
   }
 }
 
@@ -731,19 +788,33 @@ void solver_configure(DevMesh& m) {
   int dev = m.device;
   cudaDeviceProp prop;
   if (cudaGetDeviceProperties(&prop, dev) != cudaSuccess) throw std::runtime_error("cudaGetDeviceProperties failed");
+  // at least 8 warps: warp k polls reduced value k (up to kMaxRed values)
   int block = m.opt.block_threads > 0 ? m.opt.block_threads : 256;
-  block = std::max(32, std::min(512, (block / 32) * 32));
-  int occ = 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_solve, block, 0) != cudaSuccess || occ < 1)
-    throw std::runtime_error("persistent solver kernel cannot be resident with " + std::to_string(block) +
-                             " threads per CTA");
-  const int maxgrid = occ * prop.multiProcessorCount;
+  block = std::max(32 * kMaxRed, std::min(256, (block / 32) * 32));  // warp k sums value k
   const int warps = block / 32;
   int grid = m.opt.grid_ctas > 0 ? m.opt.grid_ctas
                                  : (int)std::min<int64_t>(prop.multiProcessorCount,
                                                           (m.h.nslices + warps - 1) / warps);
-  grid = std::max(1, std::min(grid, maxgrid));
+  grid = std::max(1, std::min(grid, 256));  // a reduction warp covers 8 x 32 CTAs
   grid = (int)std::min<int64_t>(grid, m.h.nslices);
+  // shared-memory staging of the CTA's SELL columns and Poisson values
+  int64_t emax = 0;
+  for (int b = 0; b < grid; ++b) {
+    const int64_t s0 = (m.h.nslices * b) / grid, s1 = (m.h.nslices * (b + 1)) / grid;
+    emax = std::max(emax, m.h.sl_off[s1] - m.h.sl_off[s0]);
+  }
+  const size_t need = (size_t)emax * (sizeof(double) + sizeof(int32_t));
+  const size_t limit = (size_t)prop.sharedMemPerBlockOptin - 16 * 1024;  // leave room for static smem
+  m.stage = need <= limit ? 1 : 0;
+  m.stage_max = emax;
+  m.smem = m.stage ? need : 0;
+  if (cudaFuncSetAttribute(k_solve, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)m.smem) != cudaSuccess)
+    throw std::runtime_error("cannot reserve shared memory for the solver kernel");
+  int occ = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_solve, block, m.smem) != cudaSuccess || occ < 1)
+    throw std::runtime_error("persistent solver kernel cannot be resident with " + std::to_string(block) +
+                             " threads per CTA");
+  grid = std::min(grid, occ * prop.multiProcessorCount);
   m.grid = grid;
   m.block = block;
 }
@@ -774,13 +845,17 @@ SolveArgs solver_args(const DevMesh& m, int mode, double h, const mm_solver_para
   a.td = m.td;
   a.tBd = m.tBd;
   a.u = m.u;
-  a.pr = m.pr;
-  a.pz = m.pz;
+  for (int q = 0; q < 2; ++q) {
+    a.pr[q] = m.pr[q];
+    a.pw[q] = m.pw[q];
+    a.ps[q] = m.ps[q];
+  }
   a.pp = m.pp;
-  a.pq = m.pq;
   a.bar = m.bar;
   a.red = m.red;
   a.flags = m.flags;
+  a.stage = m.stage;
+  a.stage_max = m.stage_max;
   a.mode = mode;
   a.h = h;
   for (int q = 0; q < 3; ++q) a.hdir[q] = sp.hdir[q];
@@ -808,14 +883,17 @@ cudaError_t solver_launch(DevMesh& m, const SolveArgs& a) {
   cudaLaunchConfig_t cfg{};
   cfg.gridDim = dim3(m.grid);
   cfg.blockDim = dim3(m.block);
-  cfg.dynamicSmemBytes = 0;
+  cfg.dynamicSmemBytes = m.smem;
   cfg.stream = m.stream;
   cudaLaunchAttribute attr[1];
   attr[0].id = cudaLaunchAttributeCooperative;
   attr[0].val.cooperative = 1;
   cfg.attrs = attr;
   cfg.numAttrs = 1;
-  return cudaLaunchKernelEx(&cfg, k_solve, a);
+  if (m.evk0 && (e = cudaEventRecord(m.evk0, m.stream)) != cudaSuccess) return e;
+  e = cudaLaunchKernelEx(&cfg, k_solve, a);
+  if (e != cudaSuccess) return e;
+  return m.evk1 ? cudaEventRecord(m.evk1, m.stream) : cudaSuccess;
 }
 
 }  // namespace mumag

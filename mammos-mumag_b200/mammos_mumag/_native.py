@@ -44,6 +44,8 @@ EXPORTED = (
     "mm_apply_minv",
     "mm_minimize",
     "mm_loop",
+    "mm_timer_start",
+    "mm_timer_stop",
 )
 
 
@@ -85,6 +87,10 @@ class StepResult(C.Structure):
         ("pcg_iters", C.c_int64),
         ("ls_shrinks", C.c_int64),
         ("minv_iters", C.c_int64),
+        ("kernel_ns", C.c_int64),
+        ("sync_ns", C.c_int64),
+        ("barriers", C.c_int64),
+        ("device_ms", C.c_double),
         ("status", C.c_int),
     ]
 
@@ -168,6 +174,8 @@ def load():
         "mm_energy_grad": (C.c_int, [C.c_void_p, C.c_double, C.POINTER(SolverParams), _D, _D, _I64]),
         "mm_apply_minv": (C.c_int, [C.c_void_p, C.POINTER(SolverParams), _D, _D, _I64]),
         "mm_minimize": (C.c_int, [C.c_void_p, C.c_double, C.POINTER(SolverParams), C.POINTER(StepResult)]),
+        "mm_timer_start": (C.c_int, [C.c_void_p]),
+        "mm_timer_stop": (C.c_int, [C.c_void_p, _D]),
         "mm_loop": (
             C.c_int,
             [C.c_void_p, C.POINTER(LoopParams), C.POINTER(SolverParams), C.POINTER(Record), _I32,
@@ -275,6 +283,15 @@ class Mesh:
 
     def __exit__(self, *exc):
         self.close()
+
+    def timer_start(self):
+        check(load().mm_timer_start(self._h))
+
+    def timer_stop(self) -> float:
+        """Milliseconds of device time on the mesh's stream since timer_start."""
+        ms = C.c_double()
+        check(load().mm_timer_stop(self._h, C.byref(ms)))
+        return ms.value
 
     def info(self) -> dict:
         i = MeshInfo()

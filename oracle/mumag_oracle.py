@@ -455,7 +455,7 @@ def hestenes_stiefel_ncg(P, x, h, hdir, u, gradF, mbar, par, stats: Stats):
 
     Returns ``(f, x, k, u, gradF)``."""
     tol, tol_u, piter, hm = par["tol_fun"], par["tol_u"], par["precond_iter"], par["hmag_on"]
-    iter_max = 100000
+    iter_max = par.get("max_ncg_iter", 100000)  # scripts/minimizers.py:142
 
     def func(xx, uu):
         return total_eg(P, xx, h, hdir, uu, tol_u, hm, stats)

@@ -113,6 +113,32 @@ def test_minv_matches_oracle(case):
     assert _relmax(z, zo) < 1e-8
 
 
+@pytest.mark.parametrize("kmax", [2, 4])
+def test_ncg_iterations_match_oracle(case, kmax):
+    """A capped number of NCG iterations (iter_max, scripts/minimizers.py:142) from the same
+    start follows the oracle's path: same evaluations, line-search halvings, restarts.
+
+    Values agree to ~1e-7, not to rounding: alpha_init (scripts/minimizers.py:34-57) divides
+    by g1.d - g.d taken across a finite-difference step h ~ 1e-8, which amplifies the
+    Poisson solve's permitted residual (tol_u = 1e-10, met by both solvers along different
+    rounding paths) by ~1/h."""
+    P, M = case
+    m = _random_state(P, 3)
+    hdir = [0.0, 0.0, 1.0]
+    par = dict(tol_fun=1e-10, tol_u=1e-10, precond_iter=10, hmag_on=1, max_ncg_iter=kmax)
+    M.set_state(m, None, m)
+    res = M.minimize(0.5, _native.solver_params(hdir=hdir, max_ncg_iter=kmax))
+    st = O.Stats()
+    fo, xo, ko, uo, _ = O.hestenes_stiefel_ncg(P, m.copy(), 0.5, hdir, np.zeros(P.N), np.zeros(3 * P.N), m, par, st)
+    assert res["status"] == 0
+    assert res["ncg_iters"] == ko == kmax
+    assert res["evals"] == st.evals
+    assert res["ls_shrinks"] == st.ls_shrinks
+    assert res["energy"] == pytest.approx(fo, rel=1e-6)
+    x, u, _ = M.get_state()
+    assert np.abs(x - xo).max() < 1e-3
+
+
 def test_field_step_matches_oracle(case):
     P, M = case
     m = _random_state(P, 3)
@@ -122,12 +148,14 @@ def test_field_step_matches_oracle(case):
     res = M.minimize(0.5, _native.solver_params(hdir=hdir))
     st = O.Stats()
     fo, xo, ko, uo, _ = O.hestenes_stiefel_ncg(P, m.copy(), 0.5, hdir, np.zeros(P.N), np.zeros(3 * P.N), m, par, st)
+    # A full minimisation from a random start ends where the reference's stopping rule
+    # (scripts/minimizers.py:164-166) lets it: successive energies within tol_fun(1+|f|) and
+    # |x0 - x|_inf <= sqrt(tol_fun)(1+|x|_inf), tol_fun = 1e-10.  The remaining descent at
+    # that point is not bounded by 1e-10, so two implementations whose roundings differ stop
+    # at different points of a slow tail (here up to ~2e-6 apart from a random start).
     assert res["status"] == 0
-    assert res["energy"] == pytest.approx(fo, rel=1e-9)
-    assert res["mh"] == pytest.approx(O.compute_mh(P, xo, hdir), rel=1e-7)
-    x, u, _ = M.get_state()
-    assert np.abs(x - xo).max() < 1e-5
-    assert abs(res["ncg_iters"] - ko) <= max(2, ko // 5)
+    assert res["energy"] == pytest.approx(fo, rel=1e-5)
+    assert res["mh"] == pytest.approx(O.compute_mh(P, xo, hdir), rel=1e-4)
 
 
 def test_golden_loop_cube_dat(cube_mesh, golden):
@@ -169,5 +197,6 @@ def test_synthetic_multigrain_loop_matches_oracle():
         rows, _ = M.loop(2.0, -2.0, -0.5, 0.4, -2.0, _native.solver_params(hdir=hdir))
     assert rows.shape == rows_o.shape
     np.testing.assert_array_equal(rows[:, 1], rows_o[:, 1])
-    np.testing.assert_allclose(rows[:, 2], rows_o[:, 2], rtol=1e-6)
+    # loop tolerance from the NCG stopping rule (see test_field_step_matches_oracle)
+    np.testing.assert_allclose(rows[:, 2], rows_o[:, 2], rtol=2e-5)
     np.testing.assert_allclose(rows[:, 3], rows_o[:, 3], rtol=1e-8)
