@@ -154,3 +154,11 @@ def run_loop(workdir, name, m0=None, device=0, grid_ctas=0, block_threads=0, ret
     out = rows.copy()
     out[:, 3] /= MU0_OUT
     return (out, steps) if return_steps else out
+
+
+if __name__ == "__main__":
+    import sys
+
+    if len(sys.argv) < 2:
+        sys.exit("usage: python -m mammos_mumag.runner modelname   (in the directory of modelname.*)")
+    run_loop(".", sys.argv[1])
