@@ -202,6 +202,31 @@ mm_status mm_loop(mm_mesh* mesh, const mm_loop_params* lp, const mm_solver_param
 mm_status mm_timer_start(mm_mesh* mesh);
 mm_status mm_timer_stop(mm_mesh* mesh, double* elapsed_ms);
 
+/* ---- allocation-free Poisson solve ------------------------------------------------------
+ *
+ * No counterpart in the reference: an extra entry point of this library for callers that
+ * cannot allocate device memory -- code running while a CUDA graph is captured, plug-ins
+ * whose host application owns every device byte through its own pool, services that
+ * forbid allocation on their serving path.  It solves A x = b (A symmetric positive
+ * definite, CSR) by Jacobi-preconditioned CG with the mesh path's iteration (the
+ * reference's jax.scipy.sparse.linalg.cg: stop when r.r <= tol^2 b.b or after max_iter
+ * iterations), x holding the initial guess on entry and the solution on return.
+ *
+ * row_ptr [n+1], col [nnz], val [nnz], b [n], x [n] are device pointers the caller owns;
+ * iters (may be NULL) is a host pointer.  The call allocates nothing: every intermediate
+ * lives in one static device array sized for at most 65,536 rows (about 4.8 MB, held by each
+ * GPU that loads the library until exit); n outside [1, 65536] is rejected with
+ * MM_BAD_INPUT, as is a CSR structure with out-of-range row pointers or columns.  All calls
+ * on a device share that array, which keeps the last call's contents; each call clears
+ * what must start at zero.  Calls that overlap on the GPU race on the array: serialise them.
+ * The first call on a device does a one-time set-up there (the array's device address,
+ * the kernel's occupancy); make it before any stream capture.  The call runs on `stream`
+ * (a cudaStream_t; NULL = the legacy default stream) of the current device and returns
+ * when the solve has finished. */
+mm_status mm_poisson_pcg_noalloc(int32_t n, int32_t nnz, const int32_t* row_ptr, const int32_t* col,
+                                 const double* val, const double* b, double* x, double tol,
+                                 int32_t max_iter, int32_t* iters, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

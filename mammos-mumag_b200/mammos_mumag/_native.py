@@ -46,6 +46,7 @@ EXPORTED = (
     "mm_loop",
     "mm_timer_start",
     "mm_timer_stop",
+    "mm_poisson_pcg_noalloc",
 )
 
 
@@ -174,6 +175,11 @@ def load():
         "mm_energy_grad": (C.c_int, [C.c_void_p, C.c_double, C.POINTER(SolverParams), _D, _D, _I64]),
         "mm_apply_minv": (C.c_int, [C.c_void_p, C.POINTER(SolverParams), _D, _D, _I64]),
         "mm_minimize": (C.c_int, [C.c_void_p, C.c_double, C.POINTER(SolverParams), C.POINTER(StepResult)]),
+        "mm_poisson_pcg_noalloc": (
+            C.c_int,
+            [C.c_int32, C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_double,
+             C.c_int32, _I32, C.c_void_p],
+        ),
         "mm_timer_start": (C.c_int, [C.c_void_p]),
         "mm_timer_stop": (C.c_int, [C.c_void_p, _D]),
         "mm_loop": (
@@ -231,6 +237,17 @@ def solver_params(hdir=(0.0, 0.0, 1.0), tol_fun=1e-10, tol_u=None, precond_iter=
     sp.max_pcg_iter = max_pcg_iter
     sp.max_ncg_iter = max_ncg_iter
     return sp
+
+
+def poisson_pcg_noalloc(n, nnz, row_ptr, col, val, b, x, tol=1e-10, max_iter=10000, stream=0) -> int:
+    """Allocation-free Jacobi-PCG solve (``mm_poisson_pcg_noalloc``) on device pointers
+    (integers); ``x`` holds the initial guess and receives the solution.  Returns the
+    iteration count."""
+    it = C.c_int32()
+    check(load().mm_poisson_pcg_noalloc(n, nnz, C.c_void_p(row_ptr), C.c_void_p(col), C.c_void_p(val),
+                                        C.c_void_p(b), C.c_void_p(x), float(tol), int(max_iter), C.byref(it),
+                                        C.c_void_p(stream)))
+    return it.value
 
 
 def rcm_permutation(T: np.ndarray, N: int) -> np.ndarray:
