@@ -200,6 +200,12 @@ mm_status mm_loop(mm_mesh* mesh, const mm_loop_params* lp, const mm_solver_param
  * records a second one, waits for it and returns the elapsed milliseconds between them.
  * Used to time field sweeps with CUDA events on the stream the kernels run on. */
 mm_status mm_timer_start(mm_mesh* mesh);
+
+/* Diagnostic per-CTA phase timers, collected only when the environment variable
+ * MUMAG_PROFILE is set at mm_mesh_create: out [nctas][4] ns accumulated since the last read
+ * (Poisson-PCG row phases, reduction before the grid barrier, barrier wait, partial read
+ * after the barrier); the counters are reset.  *nctas = 0 when profiling is off. */
+mm_status mm_profile_read(mm_mesh* mesh, long long* out, int32_t* nctas);
 mm_status mm_timer_stop(mm_mesh* mesh, double* elapsed_ms);
 
 /* ---- allocation-free Poisson solve ------------------------------------------------------

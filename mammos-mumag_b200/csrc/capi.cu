@@ -5,6 +5,7 @@
 #include <cuda_runtime.h>
 
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <memory>
 #include <new>
@@ -84,6 +85,7 @@ void release(DevMesh& m) {
   dfree(m.flags);
   dfree(m.resd);
   dfree(m.resi);
+  dfree(m.prof);
   if (m.h_resd) cudaFreeHost(m.h_resd);
   if (m.h_resi) cudaFreeHost(m.h_resi);
   if (m.h_flags) cudaFreeHost(m.h_flags);
@@ -141,6 +143,8 @@ mm_status run(DevMesh& m, const SolveArgs& a) {
   MM_CK(cudaEventElapsedTime(&m.last_launch_ms, m.evk0, m.evk1));
   const int st = m.h_flags[FLAG_STATUS];
   if (st == MM_TIMEOUT) return fail(MM_TIMEOUT, "a grid barrier of the persistent solver kernel timed out");
+  if (st != MM_OK && st != MM_NONFINITE)
+    return fail(MM_CUDA_ERROR, "the solver kernel left an invalid status word (" + std::to_string(st) + ")");
   return st;
 }
 
@@ -288,27 +292,39 @@ mm_status mm_mesh_create(const double* X, int64_t N, const int32_t* T, const int
     upload(m.etag, h.etag, m.stream);
     upload(m.dmats, m.mats, m.stream);
     assemble_operators(m);
-    // solver state: 12 three-vectors and 8 node vectors
+    // solver state: 12 three-vectors, 2 node vectors, 2 x Npad PCG records (4 doubles each);
+    // the total is computed from the same list that carves the buffer
     const size_t np = h.Npad;
-    dalloc(m.ws, 44 * np);
-    MM_CK(cudaMemsetAsync(m.ws, 0, sizeof(double) * 44 * np, m.stream));
-    double* p = m.ws;
     double** v3[] = {&m.x, &m.x1, &m.g, &m.g1, &m.d, &m.gf, &m.mbar, &m.zp, &m.tr, &m.tz, &m.td, &m.tBd};
+    double** v1[] = {&m.u, &m.pp};
+    constexpr int kRecDoubles = (int)(sizeof(PcgRec) / sizeof(double));
+    const size_t total = (sizeof(v3) / sizeof(v3[0])) * 3 * np + (sizeof(v1) / sizeof(v1[0])) * np + 2 * kRecDoubles * np;
+    dalloc(m.ws, total);
+    MM_CK(cudaMemsetAsync(m.ws, 0, sizeof(double) * total, m.stream));
+    double* p = m.ws;
     for (double** q : v3) {
       *q = p;
       p += 3 * np;
     }
-    double** v1[] = {&m.u, &m.pr[0], &m.pr[1], &m.pw[0], &m.pw[1], &m.ps[0], &m.ps[1], &m.pp};
     for (double** q : v1) {
       *q = p;
       p += np;
     }
+    for (int q = 0; q < 2; ++q) {  // 32-byte aligned: every preceding part is a multiple of 256 bytes
+      m.rec[q] = reinterpret_cast<PcgRec*>(p);
+      p += kRecDoubles * np;
+    }
+    if (p != m.ws + total) throw std::logic_error("solver workspace carve does not match its size");
     solver_configure(m);
     dalloc(m.bar, 1);
     dalloc(m.red, (size_t)2 * kMaxRed * m.grid);
     dalloc(m.flags, 2);
     dalloc(m.resd, 2);
     dalloc(m.resi, 8);
+    if (std::getenv("MUMAG_PROFILE")) {  // diagnostic per-CTA phase timers
+      dalloc(m.prof, 4 * (size_t)m.grid);
+      MM_CK(cudaMemsetAsync(m.prof, 0, sizeof(long long) * 4 * m.grid, m.stream));
+    }
     MM_CK(cudaHostAlloc(reinterpret_cast<void**>(&m.h_resd), 2 * sizeof(double), cudaHostAllocDefault));
     MM_CK(cudaHostAlloc(reinterpret_cast<void**>(&m.h_resi), 8 * sizeof(long long), cudaHostAllocDefault));
     MM_CK(cudaHostAlloc(reinterpret_cast<void**>(&m.h_flags), 2 * sizeof(int), cudaHostAllocDefault));
@@ -570,6 +586,20 @@ mm_status mm_loop(mm_mesh* mesh, const mm_loop_params* lp, const mm_solver_param
     *nrec = (int32_t)(idx + 1);
     hext = hext + lp->hstep;
   }
+  return MM_OK;
+  API_END
+}
+
+mm_status mm_profile_read(mm_mesh* mesh, long long* out, int32_t* nctas) {
+  API_BEGIN
+  check_mesh(mesh);
+  DevMesh& m = mesh->dm;
+  if (!nctas) throw std::runtime_error("nctas is NULL");
+  *nctas = m.prof ? m.grid : 0;
+  if (!m.prof || !out) return MM_OK;
+  MM_CK(cudaSetDevice(m.device));
+  MM_CK(cudaMemcpy(out, m.prof, sizeof(long long) * 4 * m.grid, cudaMemcpyDeviceToHost));
+  MM_CK(cudaMemset(m.prof, 0, sizeof(long long) * 4 * m.grid));
   return MM_OK;
   API_END
 }

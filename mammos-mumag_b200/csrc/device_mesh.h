@@ -32,6 +32,12 @@ struct MatRow {
   double Js, K, A, u[3];
 };
 
+// One node's Poisson-PCG state in the Chronopoulos-Gear iteration: r_i, w_i = S z_i,
+// s_{i-1} and 1/diag S.  32 bytes, so a neighbour's record is one sector of one gather.
+struct __align__(32) PcgRec {
+  double r, w, s, invd;
+};
+
 // Arguments of the persistent solver kernel (passed by value, __grid_constant__).
 struct SolveArgs {
   // SELL-32 pattern and operator planes (plane stride nent)
@@ -47,8 +53,9 @@ struct SolveArgs {
   double V;
   // vectors; 3-vectors are 3 planes of Npad
   double *x, *x1, *g, *g1, *d, *gf, *mbar, *zp, *tr, *tz, *td, *tBd;
-  double* u;                        // magnetostatic potential (PCG solution)
-  double *pr[2], *pw[2], *ps[2], *pp;  // PCG vectors, r/w/s double-buffered by iteration parity
+  double* u;        // magnetostatic potential (PCG solution)
+  PcgRec* rec[2];   // PCG records, double-buffered by iteration parity
+  double* pp;       // PCG search direction
   // grid synchronisation
   unsigned long long* bar;    // barrier arrival counter, zeroed before each launch
   double* red;                // [2][kMaxRed][gridDim.x] reduction partials
@@ -59,6 +66,9 @@ struct SolveArgs {
   int mode;  // 0 energy+gradient, 1 M_inv, 2 minimise (one field step)
   double h, hdir[3], tol_fun, sqrt_tol, cbrt_tol, tol_u;
   int precond_iter, hmag_on, mbar_current, max_pcg, max_ncg;
+  // optional per-CTA timing [gridDim.x][4] ns (null = off): PCG row phases, reduction
+  // before the barrier, barrier wait, partial read after the barrier
+  long long* prof;
   // results
   double* resd;     // [0] energy, [1] mh
   long long* resi;  // [0] ncg iters, [1] evals, [2] pcg iters, [3] ls shrinks, [4] minv iters
@@ -89,12 +99,14 @@ struct DevMesh {
   // state and workspace
   double* ws = nullptr;  // all solver vectors
   double *x, *x1, *g, *g1, *d, *gf, *mbar, *zp, *tr, *tz, *td, *tBd;
-  double *u, *pr[2], *pw[2], *ps[2], *pp;
+  double *u, *pp;
+  PcgRec* rec[2];
   unsigned long long* bar = nullptr;
   double* red = nullptr;
   int* flags = nullptr;
   double* resd = nullptr;
   long long* resi = nullptr;
+  long long* prof = nullptr;  // [grid][4] when MUMAG_PROFILE is set
   // pinned host mirrors of the results
   double* h_resd = nullptr;
   long long* h_resi = nullptr;

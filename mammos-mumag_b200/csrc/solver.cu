@@ -47,6 +47,7 @@ struct Sync {
   unsigned long long epoch;
   int nblk, blk, slot;
   unsigned long long t_sync;  // ns spent in grid synchronisation (thread 0)
+  unsigned long long t_pre, t_bar, t_post;  // phase timers (thread 0): see SolveArgs::prof
 };
 
 __device__ __forceinline__ unsigned long long globaltimer() {
@@ -111,6 +112,7 @@ __device__ __noinline__ bool grid_reduce(Sync& s, double (&v)[K], unsigned maxma
   __shared__ double sh[32][kMaxRed];
   __shared__ double res[kMaxRed];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  const unsigned long long tr0 = threadIdx.x == 0 ? globaltimer() : 0ull;
 #pragma unroll
   for (int k = 0; k < K; ++k) {
     const double w = ((maxmask >> k) & 1) ? warp_max(v[k]) : warp_sum(v[k]);
@@ -124,7 +126,9 @@ __device__ __noinline__ bool grid_reduce(Sync& s, double (&v)[K], unsigned maxma
     for (int w = 1; w < nw; ++w) a = ((maxmask >> k) & 1) ? fmax(a, sh[w][k]) : a + sh[w][k];
     set[(size_t)k * s.nblk + s.blk] = a;
   }
+  const unsigned long long tr1 = threadIdx.x == 0 ? globaltimer() : 0ull;
   if (!grid_barrier(s)) return false;
+  const unsigned long long tr2 = threadIdx.x == 0 ? globaltimer() : 0ull;
   if (warp < K) {  // warp k sums value k over the CTAs, in CTA order per lane, then a fixed tree
     const int k = warp;
     const bool mx = (maxmask >> k) & 1;
@@ -142,6 +146,12 @@ __device__ __noinline__ bool grid_reduce(Sync& s, double (&v)[K], unsigned maxma
 #pragma unroll
   for (int k = 0; k < K; ++k) v[k] = res[k];
   s.slot ^= 1;
+  if (threadIdx.x == 0) {
+    const unsigned long long tr3 = globaltimer();
+    s.t_pre += tr1 - tr0;
+    s.t_bar += tr2 - tr1;
+    s.t_post += tr3 - tr2;
+  }
   return true;
 }
 
@@ -165,6 +175,7 @@ struct Ctx {
   const double* sS;
   int64_t cbase;
   long long evals = 0, pcg_iters = 0, minv_iters = 0, shrinks = 0;
+  unsigned long long t_phase_start = 0, t_pcg_phase = 0;
   __device__ Ctx(const SolveArgs& args) : a(args) {}
 };
 
@@ -228,11 +239,11 @@ __device__ __forceinline__ void apply_C_row(const Ctx& c, const double* v, int64
 struct CGNext {
   double s, r, z;
 };
-__device__ __forceinline__ CGNext cg_next(double r, double w, double sprev, double invd, double alpha, double beta) {
+__device__ __forceinline__ CGNext cg_next(const PcgRec& q, double alpha, double beta) {
   CGNext o;
-  o.s = w + beta * sprev;
-  o.r = r - alpha * o.s;
-  o.z = o.r * invd;
+  o.s = q.w + beta * q.s;
+  o.r = q.r - alpha * o.s;
+  o.z = o.r * q.invd;
   return o;
 }
 
@@ -241,7 +252,7 @@ __device__ bool pcg_solve(Ctx& c, const double* x) {
   const double* Dk = plane(a, P_D);
   const int64_t ps = a.nent;
   const int n = a.Npad;
-  // phase A: b = sum_k dk x_k, r0 = b - S u
+  // phase A: b = sum_k dk x_k, r0 = b - S u; record {r0, -, s_{-1} = 0, 1/diag}
   double gamma, rr, bb;
   {
     double pg = 0, pr2 = 0, pb = 0;
@@ -255,8 +266,9 @@ __device__ bool pcg_solve(Ctx& c, const double* x) {
       su += c.sS[LENTRY(k)] * a.u[j];
     }
     const double r = b - su;
-    a.pr[0][i] = r;
-    pg += r * (r * __ldg(a.invdS + i));
+    const double invd = __ldg(a.invdS + i);
+    a.rec[0][i] = PcgRec{r, 0.0, 0.0, invd};
+    pg += r * (r * invd);
     pr2 += r * r;
     pb += b * b;
     END_ROWS
@@ -269,21 +281,21 @@ __device__ bool pcg_solve(Ctx& c, const double* x) {
   const double atol2 = fmax(a.tol_u * a.tol_u * bb, 0.0);
   int k = 0;
   if (!(rr > atol2 && k < a.max_pcg)) return true;
-  // phase B: w0 = S z0, delta0 = w0.z0; s_{-1} = p_{-1} = 0
+  // phase B: w0 = S z0, delta0 = w0.z0; p_{-1} = 0
   double delta;
   {
     double pd = 0;
+    const PcgRec* r0 = a.rec[0];
     FOR_ROWS(c)
     double acc = 0;
 #pragma unroll 8
     for (int k2 = 0; k2 < w_; ++k2) {
       const int j = c.scol[LENTRY(k2)];
-      acc += c.sS[LENTRY(k2)] * (a.pr[0][j] * __ldg(a.invdS + j));
+      acc += c.sS[LENTRY(k2)] * (r0[j].r * r0[j].invd);
     }
-    a.pw[0][i] = acc;
-    a.ps[1][i] = 0.0;
+    a.rec[0][i].w = acc;
     a.pp[i] = 0.0;
-    pd += acc * (a.pr[0][i] * __ldg(a.invdS + i));
+    pd += acc * (r0[i].r * r0[i].invd);
     END_ROWS
     double v[1] = {pd};
     CHECK(grid_reduce<1>(c.sy, v, 0u));
@@ -291,31 +303,29 @@ __device__ bool pcg_solve(Ctx& c, const double* x) {
   }
   double alpha = gamma / delta, beta = 0.0;
   for (int it = 0;; ++it) {
-    const int cur = it & 1, nxt = cur ^ 1;
-    const double* rc = a.pr[cur];
-    const double* wc = a.pw[cur];
-    const double* sp = a.ps[nxt];
+    if (threadIdx.x == 0) c.t_phase_start = globaltimer();
+    const PcgRec* rc = a.rec[it & 1];
+    PcgRec* rn = a.rec[(it & 1) ^ 1];
     double pg = 0, pd = 0, pr2 = 0;
     FOR_ROWS(c)
     double acc = 0;
 #pragma unroll 8
     for (int k2 = 0; k2 < w_; ++k2) {
       const int j = c.scol[LENTRY(k2)];
-      acc += c.sS[LENTRY(k2)] * cg_next(rc[j], wc[j], sp[j], __ldg(a.invdS + j), alpha, beta).z;
+      acc += c.sS[LENTRY(k2)] * cg_next(rc[j], alpha, beta).z;
     }
-    const double invd = __ldg(a.invdS + i);
-    const CGNext o = cg_next(rc[i], wc[i], sp[i], invd, alpha, beta);
-    const double p = rc[i] * invd + beta * a.pp[i];
+    const PcgRec q = rc[i];
+    const CGNext o = cg_next(q, alpha, beta);
+    const double p = q.r * q.invd + beta * a.pp[i];
     a.pp[i] = p;
     a.u[i] = a.u[i] + alpha * p;
-    a.pr[nxt][i] = o.r;
-    a.pw[nxt][i] = acc;
-    a.ps[cur][i] = o.s;
+    rn[i] = PcgRec{o.r, acc, o.s, q.invd};
     pg += o.r * o.z;
     pd += acc * o.z;
     pr2 += o.r * o.r;
     END_ROWS
     double v[3] = {pg, pd, pr2};
+    if (threadIdx.x == 0) c.t_pcg_phase += globaltimer() - c.t_phase_start;
     CHECK(grid_reduce<3>(c.sy, v, 0u));
     ++k;
     rr = v[2];
@@ -734,6 +744,7 @@ __global__ void __launch_bounds__(256, 1) k_solve(const __grid_constant__ SolveA
   c.sy.blk = blockIdx.x;
   c.sy.slot = 0;
   c.sy.t_sync = 0;
+  c.sy.t_pre = c.sy.t_bar = c.sy.t_post = 0;
   const unsigned long long t_start = globaltimer();
   c.lane = threadIdx.x & 31;
   c.warp = threadIdx.x >> 5;
@@ -779,6 +790,13 @@ __global__ void __launch_bounds__(256, 1) k_solve(const __grid_constant__ SolveA
     args.resi[5] = (long long)(globaltimer() - t_start);  // kernel ns (CTA 0)
     args.resi[6] = (long long)c.sy.t_sync;                // of which in grid barriers
     args.resi[7] = (long long)c.sy.epoch;                 // grid barriers executed
+  }
+  if (args.prof && threadIdx.x == 0) {
+    long long* p = args.prof + 4 * blockIdx.x;
+    p[0] += (long long)c.t_pcg_phase;
+    p[1] += (long long)c.sy.t_pre;
+    p[2] += (long long)c.sy.t_bar;
+    p[3] += (long long)c.sy.t_post;
   }
 }
 
@@ -845,11 +863,8 @@ SolveArgs solver_args(const DevMesh& m, int mode, double h, const mm_solver_para
   a.td = m.td;
   a.tBd = m.tBd;
   a.u = m.u;
-  for (int q = 0; q < 2; ++q) {
-    a.pr[q] = m.pr[q];
-    a.pw[q] = m.pw[q];
-    a.ps[q] = m.ps[q];
-  }
+  a.rec[0] = m.rec[0];
+  a.rec[1] = m.rec[1];
   a.pp = m.pp;
   a.bar = m.bar;
   a.red = m.red;
@@ -870,6 +885,7 @@ SolveArgs solver_args(const DevMesh& m, int mode, double h, const mm_solver_para
   a.max_ncg = sp.max_ncg_iter;
   a.resd = m.resd;
   a.resi = m.resi;
+  a.prof = m.prof;
   return a;
 }
 

@@ -46,6 +46,7 @@ EXPORTED = (
     "mm_loop",
     "mm_timer_start",
     "mm_timer_stop",
+    "mm_profile_read",
     "mm_poisson_pcg_noalloc",
 )
 
@@ -180,6 +181,7 @@ def load():
             [C.c_int32, C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_double,
              C.c_int32, _I32, C.c_void_p],
         ),
+        "mm_profile_read": (C.c_int, [C.c_void_p, _I64, _I32]),
         "mm_timer_start": (C.c_int, [C.c_void_p]),
         "mm_timer_stop": (C.c_int, [C.c_void_p, _D]),
         "mm_loop": (
@@ -309,6 +311,16 @@ class Mesh:
         ms = C.c_double()
         check(load().mm_timer_stop(self._h, C.byref(ms)))
         return ms.value
+
+    def profile(self):
+        """Per-CTA phase timers [nctas, 4] ns (MUMAG_PROFILE set at creation), else None."""
+        n = C.c_int32()
+        check(load().mm_profile_read(self._h, None, C.byref(n)))
+        if n.value == 0:
+            return None
+        out = np.zeros((n.value, 4), np.int64)
+        check(load().mm_profile_read(self._h, out.ctypes.data_as(_I64), C.byref(n)))
+        return out
 
     def info(self) -> dict:
         i = MeshInfo()
