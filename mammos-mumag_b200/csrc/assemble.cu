@@ -220,6 +220,12 @@ __global__ void k_finalize(const int64_t* __restrict__ sl_off, const int32_t* __
   Dex[i] = (meas[i] == 0.0) ? 1.0 : dA;
 }
 
+// FP32 copies of the planes the mixed-precision iterations read (S, Aex, K[6]).
+__global__ void k_to_f32(const double* __restrict__ vals, float* __restrict__ v32, int64_t nent) {
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < 8 * nent; t += (int64_t)gridDim.x * blockDim.x)
+    v32[t] = (float)vals[t];  // planes 0..7 of vals are S, Aex, K[6] in that order
+}
+
 }  // namespace
 
 void assemble_operators(DevMesh& m) {
@@ -270,6 +276,11 @@ void assemble_operators(DevMesh& m) {
       m.sl_off, m.sl_w, m.col, m.rowlen, m.bnd, m.vals, h.nent, m.meas, m.diagS, m.invdS, m.Dex,
       (int)h.Npad, m.opt.dirichlet_rhs == MM_DIRICHLET_RHS_ZERO);
   CK(cudaGetLastError());
+  if (m.vals32) {
+    static_assert(P_S == 0 && P_AEX == 1 && P_K == 2, "FP32 planes mirror the first 8 FP64 planes");
+    k_to_f32<<<592, 256, 0, st>>>(m.vals, m.vals32, h.nent);
+    CK(cudaGetLastError());
+  }
   CK(cudaStreamSynchronize(st));
 }
 

@@ -70,6 +70,7 @@ void release(DevMesh& m) {
   dfree(m.col);
   dfree(m.rowlen);
   dfree(m.vals);
+  dfree(m.vals32);
   dfree(m.diagS);
   dfree(m.invdS);
   dfree(m.Dex);
@@ -282,6 +283,7 @@ mm_status mm_mesh_create(const double* X, int64_t N, const int32_t* T, const int
     dalloc(m.econn, h.econn.size());
     dalloc(m.etag, h.etag.size());
     dalloc(m.dmats, m.mats.size());
+    if (o.precision == MM_PREC_MIXED) dalloc(m.vals32, (size_t)kNumPlanes32 * h.nent);
     upload(m.sl_off, h.sl_off, m.stream);
     upload(m.sl_w, h.sl_w, m.stream);
     upload(m.col, h.col, m.stream);
@@ -296,9 +298,12 @@ mm_status mm_mesh_create(const double* X, int64_t N, const int32_t* T, const int
     // the total is computed from the same list that carves the buffer
     const size_t np = h.Npad;
     double** v3[] = {&m.x, &m.x1, &m.g, &m.g1, &m.d, &m.gf, &m.mbar, &m.zp, &m.tr, &m.tz, &m.td, &m.tBd};
-    double** v1[] = {&m.u, &m.pp};
+    double** v1[] = {&m.u, &m.pp, &m.r64};
     constexpr int kRecDoubles = (int)(sizeof(PcgRec) / sizeof(double));
-    const size_t total = (sizeof(v3) / sizeof(v3[0])) * 3 * np + (sizeof(v1) / sizeof(v1[0])) * np + 2 * kRecDoubles * np;
+    constexpr int kRec32Doubles = (int)(sizeof(PcgRec32) / sizeof(double));
+    // + 2 x Npad FP32 records and the FP32 inner vectors pp32, e32 (one Npad of doubles)
+    const size_t total = (sizeof(v3) / sizeof(v3[0])) * 3 * np + (sizeof(v1) / sizeof(v1[0])) * np +
+                         2 * kRecDoubles * np + 2 * kRec32Doubles * np + np;
     dalloc(m.ws, total);
     MM_CK(cudaMemsetAsync(m.ws, 0, sizeof(double) * total, m.stream));
     double* p = m.ws;
@@ -314,6 +319,13 @@ mm_status mm_mesh_create(const double* X, int64_t N, const int32_t* T, const int
       m.rec[q] = reinterpret_cast<PcgRec*>(p);
       p += kRecDoubles * np;
     }
+    for (int q = 0; q < 2; ++q) {
+      m.rec32[q] = reinterpret_cast<PcgRec32*>(p);
+      p += kRec32Doubles * np;
+    }
+    m.pp32 = reinterpret_cast<float*>(p);
+    m.e32 = m.pp32 + np;
+    p += np;
     if (p != m.ws + total) throw std::logic_error("solver workspace carve does not match its size");
     solver_configure(m);
     dalloc(m.bar, 1);

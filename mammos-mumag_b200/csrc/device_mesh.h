@@ -38,6 +38,13 @@ struct __align__(32) PcgRec {
   double r, w, s, invd;
 };
 
+// The same record in FP32, for the inner iterations of the mixed-precision solve.
+struct __align__(16) PcgRec32 {
+  float r, w, s, invd;
+};
+
+constexpr int kNumPlanes32 = 8;  // FP32 copies of S, Aex, K[6] (mixed precision)
+
 // Arguments of the persistent solver kernel (passed by value, __grid_constant__).
 struct SolveArgs {
   // SELL-32 pattern and operator planes (plane stride nent)
@@ -56,6 +63,12 @@ struct SolveArgs {
   double* u;        // magnetostatic potential (PCG solution)
   PcgRec* rec[2];   // PCG records, double-buffered by iteration parity
   double* pp;       // PCG search direction
+  // mixed precision: FP32 operator planes and inner-solve state
+  int mixed;
+  const float* vals32;  // [kNumPlanes32][nent]: S, Aex, K[6]
+  PcgRec32* rec32[2];
+  float *pp32, *e32;    // inner search direction and correction
+  double* r64;          // FP64 residual of the outer refinement
   // grid synchronisation
   unsigned long long* bar;    // barrier arrival counter, zeroed before each launch
   double* red;                // [2][kMaxRed][gridDim.x] reduction partials
@@ -101,6 +114,10 @@ struct DevMesh {
   double *x, *x1, *g, *g1, *d, *gf, *mbar, *zp, *tr, *tz, *td, *tBd;
   double *u, *pp;
   PcgRec* rec[2];
+  float* vals32 = nullptr;
+  PcgRec32* rec32[2] = {nullptr, nullptr};
+  float *pp32 = nullptr, *e32 = nullptr;
+  double* r64 = nullptr;
   unsigned long long* bar = nullptr;
   double* red = nullptr;
   int* flags = nullptr;

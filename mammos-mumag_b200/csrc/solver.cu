@@ -173,6 +173,7 @@ struct Ctx {
   // launch when they fit (index with entry - cbase), else the global arrays (cbase = 0).
   const int32_t* scol;
   const double* sS;
+  const float* sS32;  // FP32 Poisson values (mixed precision)
   int64_t cbase;
   long long evals = 0, pcg_iters = 0, minv_iters = 0, shrinks = 0;
   unsigned long long t_phase_start = 0, t_pcg_phase = 0;
@@ -197,11 +198,10 @@ struct Ctx {
 __device__ __forceinline__ const double* plane(const SolveArgs& a, int p) { return a.vals + (size_t)p * a.nent; }
 
 // C v at row i (exchange scalar + anisotropy blocks), v a 3-vector
-__device__ __forceinline__ void apply_C_row(const Ctx& c, const double* v, int64_t off, int64_t loff, int w,
-                                            double o[3]) {
+template <class VT>
+__device__ __forceinline__ void apply_C_row_t(const Ctx& c, const VT* Aex, const VT* K, const double* v, int64_t off,
+                                              int64_t loff, int w, double o[3]) {
   const SolveArgs& a = c.a;
-  const double* Aex = plane(a, P_AEX);
-  const double* K = plane(a, P_K);
   const int64_t ps = a.nent;
   const int n = a.Npad;
   double o0 = 0, o1 = 0, o2 = 0;
@@ -210,9 +210,9 @@ __device__ __forceinline__ void apply_C_row(const Ctx& c, const double* v, int64
     const int64_t e = off + 32 * (int64_t)k;
     const int j = c.scol[loff + 32 * (int64_t)k];
     const double v0 = v[j], v1 = v[n + j], v2 = v[2 * n + j];
-    const double ax = __ldg(Aex + e);
-    const double k0 = __ldg(K + e), k1 = __ldg(K + ps + e), k2 = __ldg(K + 2 * ps + e);
-    const double k3 = __ldg(K + 3 * ps + e), k4 = __ldg(K + 4 * ps + e), k5 = __ldg(K + 5 * ps + e);
+    const double ax = (double)__ldg(Aex + e);
+    const double k0 = (double)__ldg(K + e), k1 = (double)__ldg(K + ps + e), k2 = (double)__ldg(K + 2 * ps + e);
+    const double k3 = (double)__ldg(K + 3 * ps + e), k4 = (double)__ldg(K + 4 * ps + e), k5 = (double)__ldg(K + 5 * ps + e);
     o0 += ax * v0 + (k0 * v0 + k1 * v1 + k2 * v2);
     o1 += ax * v1 + (k1 * v0 + k3 * v1 + k4 * v2);
     o2 += ax * v2 + (k2 * v0 + k4 * v1 + k5 * v2);
@@ -220,6 +220,12 @@ __device__ __forceinline__ void apply_C_row(const Ctx& c, const double* v, int64
   o[0] = o0;
   o[1] = o1;
   o[2] = o2;
+}
+
+// C v in FP64 (energies and gradients)
+__device__ __forceinline__ void apply_C_row(const Ctx& c, const double* v, int64_t off, int64_t loff, int w,
+                                            double o[3]) {
+  apply_C_row_t<double>(c, plane(c.a, P_AEX), plane(c.a, P_K), v, off, loff, w, o);
 }
 
 // ---------------------------------------------------------------------------------------
@@ -339,6 +345,141 @@ __device__ bool pcg_solve(Ctx& c, const double* x) {
   return true;
 }
 
+// Mixed precision (MM_PREC_MIXED): the same Chronopoulos-Gear iteration runs on FP32 Poisson
+// values and FP32 node records, with FP64 partial sums, and is wrapped in FP64 residual
+// refinement: r = b - S u in FP64 -> inner FP32 solve S e = r to 1e-5 relative -> u += e,
+// r -= S e in FP64 -> repeat until the FP64 residual meets the reference's test
+// r.r <= tol_u^2 b.b.  The inner iterations are counted as PCG iterations.
+struct CGNext32 {
+  float s, r, z;
+};
+__device__ __forceinline__ CGNext32 cg_next32(const PcgRec32& q, float alpha, float beta) {
+  CGNext32 o;
+  o.s = q.w + beta * q.s;
+  o.r = q.r - alpha * o.s;
+  o.z = o.r * q.invd;
+  return o;
+}
+
+__device__ bool pcg_solve_mixed(Ctx& c, const double* x) {
+  const SolveArgs& a = c.a;
+  const double* Dk = plane(a, P_D);
+  const double* S64 = plane(a, P_S);
+  const int64_t ps = a.nent;
+  const int n = a.Npad;
+  double rr, bb, rin2, gin;
+  {  // FP64 residual of the warm start; FP32 inner record
+    double p0 = 0, p1 = 0, p2 = 0, p3 = 0;
+    FOR_ROWS(c)
+    double b = 0, su = 0;
+#pragma unroll 4
+    for (int k = 0; k < w_; ++k) {
+      const int64_t e = ENTRY(k);
+      const int j = c.scol[LENTRY(k)];
+      b += __ldg(Dk + e) * x[j] + __ldg(Dk + ps + e) * x[n + j] + __ldg(Dk + 2 * ps + e) * x[2 * n + j];
+      su += c.sS[LENTRY(k)] * a.u[j];
+    }
+    const double r = b - su;
+    const float rf = (float)r, inv = (float)__ldg(a.invdS + i);
+    a.r64[i] = r;
+    a.rec32[0][i] = PcgRec32{rf, 0.f, 0.f, inv};
+    p0 += r * r;
+    p1 += b * b;
+    p2 += (double)rf * (double)rf;
+    p3 += (double)rf * (double)(rf * inv);
+    END_ROWS
+    double v[4] = {p0, p1, p2, p3};
+    CHECK(grid_reduce<4>(c.sy, v, 0u));
+    rr = v[0];
+    bb = v[1];
+    rin2 = v[2];
+    gin = v[3];
+  }
+  const double atol2 = fmax(a.tol_u * a.tol_u * bb, 0.0);
+  int k = 0;
+  for (int outer = 0; rr > atol2 && k < a.max_pcg && outer < 32; ++outer) {
+    const double inner_tol2 = fmax(1e-10 * rin2, 0.25 * atol2);  // 1e-5 relative, or the outer target
+    double gamma = gin, delta;
+    {  // w0 = S32 z0; reset the inner vectors
+      double pd = 0;
+      const PcgRec32* r0 = a.rec32[0];
+      FOR_ROWS(c)
+      float acc = 0.f;
+#pragma unroll 8
+      for (int k2 = 0; k2 < w_; ++k2) {
+        const int j = c.scol[LENTRY(k2)];
+        acc += c.sS32[LENTRY(k2)] * (r0[j].r * r0[j].invd);
+      }
+      a.rec32[0][i].w = acc;
+      a.pp32[i] = 0.f;
+      a.e32[i] = 0.f;
+      pd += (double)acc * (double)(r0[i].r * r0[i].invd);
+      END_ROWS
+      double v[1] = {pd};
+      CHECK(grid_reduce<1>(c.sy, v, 0u));
+      delta = v[0];
+    }
+    double alpha = gamma / delta, beta = 0.0;
+    int last = 0;
+    for (int it = 0;; ++it) {
+      const PcgRec32* rc = a.rec32[it & 1];
+      PcgRec32* rn = a.rec32[(it & 1) ^ 1];
+      const float af = (float)alpha, bf = (float)beta;
+      double pg = 0, pd = 0, pr2 = 0;
+      FOR_ROWS(c)
+      float acc = 0.f;
+#pragma unroll 8
+      for (int k2 = 0; k2 < w_; ++k2) {
+        const int j = c.scol[LENTRY(k2)];
+        acc += c.sS32[LENTRY(k2)] * cg_next32(rc[j], af, bf).z;
+      }
+      const PcgRec32 q = rc[i];
+      const CGNext32 o = cg_next32(q, af, bf);
+      const float p = q.r * q.invd + bf * a.pp32[i];
+      a.pp32[i] = p;
+      a.e32[i] = a.e32[i] + af * p;
+      rn[i] = PcgRec32{o.r, acc, o.s, q.invd};
+      pg += (double)o.r * (double)o.z;
+      pd += (double)acc * (double)o.z;
+      pr2 += (double)o.r * (double)o.r;
+      END_ROWS
+      double v[3] = {pg, pd, pr2};
+      CHECK(grid_reduce<3>(c.sy, v, 0u));
+      ++k;
+      last = it;
+      if (!(v[2] > inner_tol2 && k < a.max_pcg)) break;
+      const double bn = v[0] / gamma;
+      alpha = v[0] / (v[1] - bn * v[0] / alpha);
+      beta = bn;
+      gamma = v[0];
+    }
+    (void)last;
+    {  // u += e, r -= S e in FP64; next inner record
+      double p0 = 0, p2 = 0, p3 = 0;
+      FOR_ROWS(c)
+      double se = 0;
+#pragma unroll 8
+      for (int k2 = 0; k2 < w_; ++k2) se += c.sS[LENTRY(k2)] * (double)a.e32[c.scol[LENTRY(k2)]];
+      a.u[i] = a.u[i] + (double)a.e32[i];
+      const double r = a.r64[i] - se;
+      a.r64[i] = r;
+      const float rf = (float)r, inv = (float)__ldg(a.invdS + i);
+      a.rec32[0][i] = PcgRec32{rf, 0.f, 0.f, inv};
+      p0 += r * r;
+      p2 += (double)rf * (double)rf;
+      p3 += (double)rf * (double)(rf * inv);
+      END_ROWS
+      double v[3] = {p0, p2, p3};
+      CHECK(grid_reduce<3>(c.sy, v, 0u));
+      rr = v[0];
+      rin2 = v[1];
+      gin = v[2];
+    }
+  }
+  c.pcg_iters += k;
+  return true;
+}
+
 // ---------------------------------------------------------------------------------------
 // total_eg, scripts/energies.py:67-99
 // ---------------------------------------------------------------------------------------
@@ -351,7 +492,7 @@ struct EvalOut {
 // gd = gout.d (d may be null), dxinf = max|x - xref|, xinf = max|x|, ginf = max|gout|.
 __device__ bool eval(Ctx& c, const double* x, const double* xref, const double* d, double* gout, EvalOut& o) {
   const SolveArgs& a = c.a;
-  if (a.hmag_on > 0) CHECK(pcg_solve(c, x));
+  if (a.hmag_on > 0) CHECK(a.mixed ? pcg_solve_mixed(c, x) : pcg_solve(c, x));
   const int n = a.Npad;
   const double* G = plane(a, P_G);
   const int64_t ps = a.nent;
@@ -431,7 +572,10 @@ __device__ __forceinline__ void apply_A_row(const Ctx& c, const double* mb, cons
   const SolveArgs& a = c.a;
   const int n = a.Npad;
   double cv[3];
-  apply_C_row(c, v, off, loff, w, cv);
+  if (a.mixed)
+    apply_C_row_t<float>(c, a.vals32 + (size_t)P_AEX * a.nent, a.vals32 + (size_t)P_K * a.nent, v, off, loff, w, cv);
+  else
+    apply_C_row(c, v, off, loff, w, cv);
   const double m[3] = {mb[i], mb[n + i], mb[2 * n + i]};
   const double md = m[0] * a.gf[i] + m[1] * a.gf[n + i] + m[2] * a.gf[2 * n + i];
   double pr[3];
@@ -755,17 +899,21 @@ __global__ void __launch_bounds__(256, 1) k_solve(const __grid_constant__ SolveA
     const int64_t e0 = args.sl_off[c.s0], n = args.sl_off[c.s1] - e0;
     double* sS = reinterpret_cast<double*>(smem);
     int32_t* scol = reinterpret_cast<int32_t*>(smem + sizeof(double) * args.stage_max);
+    float* sS32 = reinterpret_cast<float*>(smem + (sizeof(double) + sizeof(int32_t)) * args.stage_max);
     const double* S = args.vals + (size_t)P_S * args.nent;
     for (int64_t t = threadIdx.x; t < n; t += blockDim.x) {
       sS[t] = __ldg(S + e0 + t);
       scol[t] = __ldg(args.col + e0 + t);
+      if (args.mixed) sS32[t] = __ldg(args.vals32 + e0 + t);
     }
     __syncthreads();
     c.sS = sS;
+    c.sS32 = sS32;
     c.scol = scol;
     c.cbase = e0;
   } else {
     c.sS = args.vals + (size_t)P_S * args.nent;
+    c.sS32 = args.vals32;
     c.scol = args.col;
     c.cbase = 0;
   }
@@ -821,7 +969,7 @@ void solver_configure(DevMesh& m) {
     const int64_t s0 = (m.h.nslices * b) / grid, s1 = (m.h.nslices * (b + 1)) / grid;
     emax = std::max(emax, m.h.sl_off[s1] - m.h.sl_off[s0]);
   }
-  const size_t need = (size_t)emax * (sizeof(double) + sizeof(int32_t));
+  const size_t need = (size_t)emax * (sizeof(double) + sizeof(int32_t) + (m.vals32 ? sizeof(float) : 0));
   const size_t limit = (size_t)prop.sharedMemPerBlockOptin - 16 * 1024;  // leave room for static smem
   m.stage = need <= limit ? 1 : 0;
   m.stage_max = emax;
@@ -866,6 +1014,13 @@ SolveArgs solver_args(const DevMesh& m, int mode, double h, const mm_solver_para
   a.rec[0] = m.rec[0];
   a.rec[1] = m.rec[1];
   a.pp = m.pp;
+  a.mixed = m.vals32 != nullptr;
+  a.vals32 = m.vals32;
+  a.rec32[0] = m.rec32[0];
+  a.rec32[1] = m.rec32[1];
+  a.pp32 = m.pp32;
+  a.e32 = m.e32;
+  a.r64 = m.r64;
   a.bar = m.bar;
   a.red = m.red;
   a.flags = m.flags;
