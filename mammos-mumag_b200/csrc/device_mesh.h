@@ -33,7 +33,7 @@ struct MatRow {
 };
 
 // One node's Poisson-PCG state in the Chronopoulos-Gear iteration: r_i, w_i = S z_i,
-// s_{i-1} and 1/diag S.  32 bytes, so a neighbour's record is one sector of one gather.
+// s_{i-1} and 1/diag S.  Stored as four planes of a buffer (solver.cu rec_load/rec_store).
 struct __align__(32) PcgRec {
   double r, w, s, invd;
 };
@@ -75,6 +75,7 @@ struct SolveArgs {
   int* flags;                 // [0] abort, [1] status
   int stage;                  // 1: the CTA's SELL columns + Poisson values live in shared memory
   int64_t stage_max;          // entries of the largest CTA (shared-memory layout)
+  int64_t meta_max;           // slices of the largest CTA (shared-memory slice metadata)
   // control
   int mode;  // 0 energy+gradient, 1 M_inv, 2 minimise (one field step)
   double h, hdir[3], tol_fun, sqrt_tol, cbrt_tol, tol_u;
@@ -134,7 +135,7 @@ struct DevMesh {
   cudaEvent_t evk0 = nullptr, evk1 = nullptr;  // around each persistent launch
   float last_launch_ms = 0.f;
   int stage = 0;
-  int64_t stage_max = 0;
+  int64_t stage_max = 0, meta_max = 0;
   size_t smem = 0;
 };
 

@@ -48,6 +48,7 @@ struct Sync {
   int nblk, blk, slot;
   unsigned long long t_sync;  // ns spent in grid synchronisation (thread 0)
   unsigned long long t_pre, t_bar, t_post;  // phase timers (thread 0): see SolveArgs::prof
+  bool timing;                              // read %globaltimer only when profiling
 };
 
 __device__ __forceinline__ unsigned long long globaltimer() {
@@ -67,7 +68,7 @@ __device__ __forceinline__ void red_release_add_u64(unsigned long long* p, unsig
 
 __device__ __noinline__ bool grid_barrier(Sync& s) {
   __shared__ int sh_abort;
-  const unsigned long long t0 = threadIdx.x == 0 ? globaltimer() : 0ull;
+  const unsigned long long t0 = (s.timing && threadIdx.x == 0) ? globaltimer() : 0ull;
   __syncthreads();
   if (threadIdx.x == 0) {
     s.epoch += 1;
@@ -90,7 +91,7 @@ __device__ __noinline__ bool grid_barrier(Sync& s) {
     }
     __threadfence();
     sh_abort = ab;
-    s.t_sync += globaltimer() - t0;
+    if (s.timing) s.t_sync += globaltimer() - t0;
   }
   __syncthreads();
   return sh_abort == 0;
@@ -112,7 +113,7 @@ __device__ __noinline__ bool grid_reduce(Sync& s, double (&v)[K], unsigned maxma
   __shared__ double sh[32][kMaxRed];
   __shared__ double res[kMaxRed];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
-  const unsigned long long tr0 = threadIdx.x == 0 ? globaltimer() : 0ull;
+  const unsigned long long tr0 = (s.timing && threadIdx.x == 0) ? globaltimer() : 0ull;
 #pragma unroll
   for (int k = 0; k < K; ++k) {
     const double w = ((maxmask >> k) & 1) ? warp_max(v[k]) : warp_sum(v[k]);
@@ -126,9 +127,9 @@ __device__ __noinline__ bool grid_reduce(Sync& s, double (&v)[K], unsigned maxma
     for (int w = 1; w < nw; ++w) a = ((maxmask >> k) & 1) ? fmax(a, sh[w][k]) : a + sh[w][k];
     set[(size_t)k * s.nblk + s.blk] = a;
   }
-  const unsigned long long tr1 = threadIdx.x == 0 ? globaltimer() : 0ull;
+  const unsigned long long tr1 = (s.timing && threadIdx.x == 0) ? globaltimer() : 0ull;
   if (!grid_barrier(s)) return false;
-  const unsigned long long tr2 = threadIdx.x == 0 ? globaltimer() : 0ull;
+  const unsigned long long tr2 = (s.timing && threadIdx.x == 0) ? globaltimer() : 0ull;
   if (warp < K) {  // warp k sums value k over the CTAs, in CTA order per lane, then a fixed tree
     const int k = warp;
     const bool mx = (maxmask >> k) & 1;
@@ -146,7 +147,7 @@ __device__ __noinline__ bool grid_reduce(Sync& s, double (&v)[K], unsigned maxma
 #pragma unroll
   for (int k = 0; k < K; ++k) v[k] = res[k];
   s.slot ^= 1;
-  if (threadIdx.x == 0) {
+  if (s.timing && threadIdx.x == 0) {
     const unsigned long long tr3 = globaltimer();
     s.t_pre += tr1 - tr0;
     s.t_bar += tr2 - tr1;
@@ -174,6 +175,8 @@ struct Ctx {
   const int32_t* scol;
   const double* sS;
   const float* sS32;  // FP32 Poisson values (mixed precision)
+  const int64_t* soff;  // SELL offsets and widths of the CTA's slices (shared memory)
+  const int32_t* sw;
   int64_t cbase;
   long long evals = 0, pcg_iters = 0, minv_iters = 0, shrinks = 0;
   unsigned long long t_phase_start = 0, t_pcg_phase = 0;
@@ -185,9 +188,9 @@ struct Ctx {
 #define FOR_ROWS(c)                                                       \
   for (int s_ = (c).s0 + (c).warp; s_ < (c).s1; s_ += (c).nwarps) {      \
     const int i = s_ * 32 + (c).lane;                                     \
-    const int64_t off_ = (c).a.sl_off[s_] + (c).lane;                     \
+    const int64_t off_ = (c).soff[s_ - (c).s0] + (c).lane;                \
     const int64_t loff_ = off_ - (c).cbase;                               \
-    const int w_ = (c).a.sl_w[s_];                                        \
+    const int w_ = (c).sw[s_ - (c).s0];                                   \
     (void)loff_;
 #define END_ROWS }
 #define ENTRY(k) (off_ + 32 * (int64_t)(k))
@@ -242,6 +245,25 @@ __device__ __forceinline__ void apply_C_row(const Ctx& c, const double* v, int64
 // the previous iteration left in the other half of double buffers.  So an iteration needs
 // one grid synchronisation instead of two.
 // ---------------------------------------------------------------------------------------
+// Node state of the Chronopoulos-Gear PCG: four planes r, w, s, 1/diag of Npad doubles in
+// one buffer per iteration parity.  Planes measured faster than 32-byte node records on
+// the B200 (96 vs 89 field steps/s on the 80 nm multigrain sweep): the four coalesced
+// 8-byte stores and gathers beat the 32-byte struct accesses.
+__device__ __forceinline__ PcgRec rec_load(const PcgRec* b, int j, int np) {
+  const double* p = reinterpret_cast<const double*>(b);
+  return PcgRec{p[j], p[np + j], p[2 * np + j], p[3 * np + j]};
+}
+__device__ __forceinline__ void rec_store(PcgRec* b, int j, int np, const PcgRec& q) {
+  double* p = reinterpret_cast<double*>(b);
+  p[j] = q.r;
+  p[np + j] = q.w;
+  p[2 * np + j] = q.s;
+  p[3 * np + j] = q.invd;
+}
+__device__ __forceinline__ void rec_store_w(PcgRec* b, int j, int np, double w) {
+  reinterpret_cast<double*>(b)[np + j] = w;
+}
+
 struct CGNext {
   double s, r, z;
 };
@@ -273,7 +295,7 @@ __device__ bool pcg_solve(Ctx& c, const double* x) {
     }
     const double r = b - su;
     const double invd = __ldg(a.invdS + i);
-    a.rec[0][i] = PcgRec{r, 0.0, 0.0, invd};
+    rec_store(a.rec[0], i, n, PcgRec{r, 0.0, 0.0, invd});
     pg += r * (r * invd);
     pr2 += r * r;
     pb += b * b;
@@ -297,11 +319,13 @@ __device__ bool pcg_solve(Ctx& c, const double* x) {
 #pragma unroll 8
     for (int k2 = 0; k2 < w_; ++k2) {
       const int j = c.scol[LENTRY(k2)];
-      acc += c.sS[LENTRY(k2)] * (r0[j].r * r0[j].invd);
+      const PcgRec q = rec_load(r0, j, n);
+      acc += c.sS[LENTRY(k2)] * (q.r * q.invd);
     }
-    a.rec[0][i].w = acc;
+    const PcgRec qi = rec_load(r0, i, n);
+    rec_store_w(a.rec[0], i, n, acc);
     a.pp[i] = 0.0;
-    pd += acc * (r0[i].r * r0[i].invd);
+    pd += acc * (qi.r * qi.invd);
     END_ROWS
     double v[1] = {pd};
     CHECK(grid_reduce<1>(c.sy, v, 0u));
@@ -309,29 +333,30 @@ __device__ bool pcg_solve(Ctx& c, const double* x) {
   }
   double alpha = gamma / delta, beta = 0.0;
   for (int it = 0;; ++it) {
-    if (threadIdx.x == 0) c.t_phase_start = globaltimer();
+    if (c.sy.timing && threadIdx.x == 0) c.t_phase_start = globaltimer();
     const PcgRec* rc = a.rec[it & 1];
     PcgRec* rn = a.rec[(it & 1) ^ 1];
     double pg = 0, pd = 0, pr2 = 0;
     FOR_ROWS(c)
+    const PcgRec q = rec_load(rc, i, n);
+    const double pold = a.pp[i], uold = a.u[i];
     double acc = 0;
 #pragma unroll 8
     for (int k2 = 0; k2 < w_; ++k2) {
       const int j = c.scol[LENTRY(k2)];
-      acc += c.sS[LENTRY(k2)] * cg_next(rc[j], alpha, beta).z;
+      acc += c.sS[LENTRY(k2)] * cg_next(rec_load(rc, j, n), alpha, beta).z;
     }
-    const PcgRec q = rc[i];
     const CGNext o = cg_next(q, alpha, beta);
-    const double p = q.r * q.invd + beta * a.pp[i];
+    const double p = q.r * q.invd + beta * pold;
     a.pp[i] = p;
-    a.u[i] = a.u[i] + alpha * p;
-    rn[i] = PcgRec{o.r, acc, o.s, q.invd};
+    a.u[i] = uold + alpha * p;
+    rec_store(rn, i, n, PcgRec{o.r, acc, o.s, q.invd});
     pg += o.r * o.z;
     pd += acc * o.z;
     pr2 += o.r * o.r;
     END_ROWS
     double v[3] = {pg, pd, pr2};
-    if (threadIdx.x == 0) c.t_pcg_phase += globaltimer() - c.t_phase_start;
+    if (c.sy.timing && threadIdx.x == 0) c.t_pcg_phase += globaltimer() - c.t_phase_start;
     CHECK(grid_reduce<3>(c.sy, v, 0u));
     ++k;
     rr = v[2];
@@ -889,12 +914,25 @@ __global__ void __launch_bounds__(256, 1) k_solve(const __grid_constant__ SolveA
   c.sy.slot = 0;
   c.sy.t_sync = 0;
   c.sy.t_pre = c.sy.t_bar = c.sy.t_post = 0;
+  c.sy.timing = args.prof != nullptr;
   const unsigned long long t_start = globaltimer();
   c.lane = threadIdx.x & 31;
   c.warp = threadIdx.x >> 5;
   c.nwarps = blockDim.x >> 5;
   c.s0 = (int)(((long long)args.nslices * blockIdx.x) / gridDim.x);
   c.s1 = (int)(((long long)args.nslices * (blockIdx.x + 1)) / gridDim.x);
+  {  // slice metadata of this CTA, after the staged operator entries
+    const size_t staged = args.stage ? (size_t)args.stage_max * (sizeof(double) + sizeof(int32_t) + (args.mixed ? sizeof(float) : 0)) : 0;
+    int64_t* soff = reinterpret_cast<int64_t*>(smem + ((staged + 15) & ~(size_t)15));
+    int32_t* sw = reinterpret_cast<int32_t*>(soff + args.meta_max);
+    for (int t = threadIdx.x; t < c.s1 - c.s0; t += blockDim.x) {
+      soff[t] = args.sl_off[c.s0 + t];
+      sw[t] = args.sl_w[c.s0 + t];
+    }
+    c.soff = soff;
+    c.sw = sw;
+    __syncthreads();
+  }
   if (args.stage) {
     const int64_t e0 = args.sl_off[c.s0], n = args.sl_off[c.s1] - e0;
     double* sS = reinterpret_cast<double*>(smem);
@@ -969,11 +1007,16 @@ void solver_configure(DevMesh& m) {
     const int64_t s0 = (m.h.nslices * b) / grid, s1 = (m.h.nslices * (b + 1)) / grid;
     emax = std::max(emax, m.h.sl_off[s1] - m.h.sl_off[s0]);
   }
+  int64_t smax = 0;
+  for (int b = 0; b < grid; ++b)
+    smax = std::max(smax, (m.h.nslices * (b + 1)) / grid - (m.h.nslices * b) / grid);
+  const size_t meta = (size_t)smax * (sizeof(int64_t) + sizeof(int32_t));
   const size_t need = (size_t)emax * (sizeof(double) + sizeof(int32_t) + (m.vals32 ? sizeof(float) : 0));
-  const size_t limit = (size_t)prop.sharedMemPerBlockOptin - 16 * 1024;  // leave room for static smem
+  const size_t limit = (size_t)prop.sharedMemPerBlockOptin - 16 * 1024 - meta - 16;  // room for static smem
   m.stage = need <= limit ? 1 : 0;
   m.stage_max = emax;
-  m.smem = m.stage ? need : 0;
+  m.meta_max = smax;
+  m.smem = (m.stage ? ((need + 15) & ~(size_t)15) : 0) + meta;
   if (cudaFuncSetAttribute(k_solve, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)m.smem) != cudaSuccess)
     throw std::runtime_error("cannot reserve shared memory for the solver kernel");
   int occ = 0;
@@ -1026,6 +1069,7 @@ SolveArgs solver_args(const DevMesh& m, int mode, double h, const mm_solver_para
   a.flags = m.flags;
   a.stage = m.stage;
   a.stage_max = m.stage_max;
+  a.meta_max = m.meta_max;
   a.mode = mode;
   a.h = h;
   for (int q = 0; q < 3; ++q) a.hdir[q] = sp.hdir[q];

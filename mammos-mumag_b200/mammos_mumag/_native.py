@@ -11,7 +11,9 @@ import pathlib
 
 import numpy as np
 
-LIB_PATH = pathlib.Path(__file__).resolve().parent / "lib" / "libmumag_b200.so"
+import os
+
+LIB_PATH = pathlib.Path(os.environ.get("MUMAG_LIB") or pathlib.Path(__file__).resolve().parent / "lib" / "libmumag_b200.so")
 
 MM_OK, MM_BAD_INPUT, MM_CUDA_ERROR, MM_NONFINITE, MM_TIMEOUT, MM_NO_DEVICE = range(6)
 STATUS_NAMES = {
