@@ -42,6 +42,23 @@ UNIT = "field steps/s"
 L2_FLUSH_BYTES = 256 << 20
 
 
+def batch_workload(count: int = 64, seed: int = 0):
+    """64 independent loops on seeded meshes of uneven size: structured grids of 12..40 cells
+    per edge (h = 1.25 nm), 6 tets per cell, 1..27 Voronoi grains with easy axes in a cone of
+    up to 30 degrees, the single-grain material, a 2 nm grain-boundary phase."""
+    from mammos_mumag import synthetic
+
+    rng = np.random.default_rng(seed)
+    out = []
+    for q in range(count):
+        n = int(rng.integers(12, 41))
+        grains = int(rng.integers(1, 28))
+        cone = float(rng.uniform(0.0, 30.0))
+        out.append(synthetic.multigrain(n=n, L=1.25 * n, grains=grains, cone_deg=cone, gb=2.0 if grains > 1 else 0.0,
+                                        seed=seed * 1000 + q))
+    return out
+
+
 def workload(name: str, seed: int):
     from mammos_mumag import synthetic
 

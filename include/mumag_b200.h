@@ -196,10 +196,40 @@ mm_status mm_loop(mm_mesh* mesh, const mm_loop_params* lp, const mm_solver_param
                   mm_record* rec, int32_t* nrec, mm_step_result* steps, mm_snapshot_cb cb,
                   void* user);
 
+/* ---- batched persistent launch ----------------------------------------------------------
+ *
+ * Several independent meshes stepped together in ONE cooperative launch: mesh q runs on a
+ * group of CTAs sized in proportion to its rows, with barriers and reductions local to the
+ * group, so the meshes' iterations proceed independently inside the launch.  This is the
+ * batched form of mm_minimize / mm_loop (no counterpart in the reference, which runs one
+ * loop per process); each mesh keeps its own state (mm_set_state / mm_get_state). */
+typedef struct mm_batch mm_batch;
+
+/* The meshes must live on one device; count <= number of SMs.  The handles stay owned by
+ * the caller and must outlive the batch. */
+mm_status mm_batch_create(mm_mesh* const* meshes, int32_t count, mm_batch** out);
+mm_status mm_batch_destroy(mm_batch* batch);
+/* CTAs assigned to mesh q (group[q+1]-group[q]); group has count+1 entries. */
+mm_status mm_batch_groups(const mm_batch* batch, int32_t* group);
+
+/* One field step of every mesh: h[q], sp[q], res[q] (count each). */
+mm_status mm_batch_minimize(mm_batch* batch, const double* h, const mm_solver_params* sp, mm_step_result* res);
+
+/* The field sweep of every mesh in lockstep (all share lp; sp[q] per mesh): rec holds
+ * count x max_steps rows (mesh-major), nrec[q] the rows written for mesh q, steps (may be
+ * NULL) count x max_steps results.  A mesh whose mh falls below mfinal stops (idles in
+ * the later launches); the sweep ends when all have stopped or the field range is done.
+ * No snapshot callback. */
+mm_status mm_batch_loop(mm_batch* batch, const mm_loop_params* lp, const mm_solver_params* sp, int32_t max_steps,
+                        mm_record* rec, int32_t* nrec, mm_step_result* steps);
+
 /* Device timing on the mesh's CUDA stream: mm_timer_start records an event; mm_timer_stop
  * records a second one, waits for it and returns the elapsed milliseconds between them.
  * Used to time field sweeps with CUDA events on the stream the kernels run on. */
 mm_status mm_timer_start(mm_mesh* mesh);
+/* The same for a batch's stream. */
+mm_status mm_batch_timer_start(mm_batch* batch);
+mm_status mm_batch_timer_stop(mm_batch* batch, double* elapsed_ms);
 
 /* Diagnostic per-CTA phase timers, collected only when the environment variable
  * MUMAG_PROFILE is set at mm_mesh_create: out [nctas][4] ns accumulated since the last read

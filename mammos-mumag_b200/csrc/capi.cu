@@ -19,6 +19,17 @@ struct mm_mesh {
   mumag::DevMesh dm;
 };
 
+struct mm_batch {
+  std::vector<mm_mesh*> meshes;
+  mumag::BatchPlan plan;
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  mumag::SolveArgs* d_args = nullptr;
+  int* d_group = nullptr;
+  std::vector<mumag::SolveArgs> h_args;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+};
+
 namespace mumag {
 
 namespace {
@@ -639,6 +650,194 @@ mm_status mm_timer_stop(mm_mesh* mesh, double* elapsed_ms) {
   MM_CK(cudaEventSynchronize(m.ev1));
   float ms = 0.f;
   MM_CK(cudaEventElapsedTime(&ms, m.ev0, m.ev1));
+  *elapsed_ms = ms;
+  return MM_OK;
+  API_END
+}
+
+namespace {
+void batch_release(mm_batch* b) {
+  cudaSetDevice(b->device);
+  if (b->d_args) cudaFree(b->d_args);
+  if (b->d_group) cudaFree(b->d_group);
+  if (b->ev0) cudaEventDestroy(b->ev0);
+  if (b->ev1) cudaEventDestroy(b->ev1);
+  if (b->stream) cudaStreamDestroy(b->stream);
+}
+
+// One batched launch: args[q] with mode MINIMIZE (h[q]) or IDLE (active[q] == 0).
+mm_status batch_run(mm_batch* b, const double* h, const mm_solver_params* sp, const std::vector<char>& active) {
+  const int count = (int)b->meshes.size();
+  MM_CK(cudaSetDevice(b->device));
+  for (int q = 0; q < count; ++q) {
+    DevMesh& m = b->meshes[q]->dm;
+    SolveArgs a = solver_args(m, active[q] ? MODE_MINIMIZE : MODE_IDLE, h[q], sp[q]);
+    a.stage = b->plan.stage[q];
+    a.stage_max = b->plan.stage_max[q];
+    a.meta_max = b->plan.meta_max[q];
+    a.prof = nullptr;
+    b->h_args[q] = a;
+    MM_CK(launch_prep(m, b->stream));
+  }
+  MM_CK(cudaMemcpyAsync(b->d_args, b->h_args.data(), sizeof(SolveArgs) * count, cudaMemcpyHostToDevice, b->stream));
+  MM_CK(batch_launch(b->plan, b->d_args, b->d_group, count, b->stream));
+  for (int q = 0; q < count; ++q) {
+    DevMesh& m = b->meshes[q]->dm;
+    MM_CK(cudaMemcpyAsync(m.h_resd, m.resd, 2 * sizeof(double), cudaMemcpyDeviceToHost, b->stream));
+    MM_CK(cudaMemcpyAsync(m.h_resi, m.resi, 8 * sizeof(long long), cudaMemcpyDeviceToHost, b->stream));
+    MM_CK(cudaMemcpyAsync(m.h_flags, m.flags, 2 * sizeof(int), cudaMemcpyDeviceToHost, b->stream));
+  }
+  MM_CK(cudaStreamSynchronize(b->stream));
+  mm_status worst = MM_OK;
+  for (int q = 0; q < count; ++q) {
+    const int st = b->meshes[q]->dm.h_flags[FLAG_STATUS];
+    if (st == MM_TIMEOUT) return fail(MM_TIMEOUT, "a grid barrier of the batched solver kernel timed out");
+    if (st != MM_OK && st != MM_NONFINITE)
+      return fail(MM_CUDA_ERROR, "the batched solver kernel left an invalid status word");
+    if (st == MM_NONFINITE) worst = MM_NONFINITE;
+  }
+  return worst;
+}
+
+void fill_result(const DevMesh& m, mm_status st, mm_step_result& r) {
+  r.energy = m.h_resd[0];
+  r.mh = m.h_resd[1];
+  r.ncg_iters = m.h_resi[0];
+  r.evals = m.h_resi[1];
+  r.pcg_iters = m.h_resi[2];
+  r.ls_shrinks = m.h_resi[3];
+  r.minv_iters = m.h_resi[4];
+  r.kernel_ns = m.h_resi[5];
+  r.sync_ns = m.h_resi[6];
+  r.barriers = m.h_resi[7];
+  r.device_ms = 0.0;
+  r.status = st;
+}
+}  // namespace
+
+mm_status mm_batch_create(mm_mesh* const* meshes, int32_t count, mm_batch** out) {
+  API_BEGIN
+  if (!out || !meshes || count < 1) throw std::runtime_error("invalid batch arguments");
+  *out = nullptr;
+  std::unique_ptr<mm_batch> b(new mm_batch());
+  std::vector<DevMesh*> ms;
+  for (int q = 0; q < count; ++q) {
+    check_mesh(meshes[q]);
+    b->meshes.push_back(meshes[q]);
+    ms.push_back(&meshes[q]->dm);
+  }
+  b->device = ms[0]->device;
+  try {
+    MM_CK(cudaSetDevice(b->device));
+    batch_configure(ms, b->plan);
+    MM_CK(cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking));
+    MM_CK(cudaMalloc(reinterpret_cast<void**>(&b->d_args), sizeof(SolveArgs) * count));
+    MM_CK(cudaMalloc(reinterpret_cast<void**>(&b->d_group), sizeof(int) * (count + 1)));
+    MM_CK(cudaMemcpy(b->d_group, b->plan.group.data(), sizeof(int) * (count + 1), cudaMemcpyHostToDevice));
+    b->h_args.resize(count);
+  } catch (...) {
+    batch_release(b.get());
+    throw;
+  }
+  *out = b.release();
+  return MM_OK;
+  API_END
+}
+
+mm_status mm_batch_destroy(mm_batch* batch) {
+  if (!batch) return MM_OK;
+  batch_release(batch);
+  delete batch;
+  return MM_OK;
+}
+
+mm_status mm_batch_groups(const mm_batch* batch, int32_t* group) {
+  API_BEGIN
+  if (!batch || !group) throw std::runtime_error("NULL batch or output");
+  for (size_t q = 0; q < batch->plan.group.size(); ++q) group[q] = batch->plan.group[q];
+  return MM_OK;
+  API_END
+}
+
+mm_status mm_batch_minimize(mm_batch* batch, const double* h, const mm_solver_params* sp, mm_step_result* res) {
+  API_BEGIN
+  if (!batch || !h || !sp) throw std::runtime_error("NULL batch argument");
+  const int count = (int)batch->meshes.size();
+  for (int q = 0; q < count; ++q) check_params(&sp[q]);
+  std::vector<char> active(count, 1);
+  mm_status st = batch_run(batch, h, sp, active);
+  if (res)
+    for (int q = 0; q < count; ++q) fill_result(batch->meshes[q]->dm, st, res[q]);
+  return st;
+  API_END
+}
+
+mm_status mm_batch_loop(mm_batch* batch, const mm_loop_params* lp, const mm_solver_params* sp, int32_t max_steps,
+                        mm_record* rec, int32_t* nrec, mm_step_result* steps) {
+  API_BEGIN
+  if (!batch || !lp || !sp || !rec || !nrec || max_steps < 1) throw std::runtime_error("invalid batch loop arguments");
+  if (!(lp->hstep != 0.0)) throw std::runtime_error("invalid field sweep");
+  const int count = (int)batch->meshes.size();
+  for (int q = 0; q < count; ++q) check_params(&sp[q]);
+  int64_t nmax = (int64_t)(std::fabs(lp->hfinal - lp->hstart) / std::fabs(lp->hstep)) + 1;
+  if (lp->max_steps > 0) nmax = std::min<int64_t>(nmax, lp->max_steps);
+  nmax = std::min<int64_t>(nmax, max_steps);
+  std::vector<double> mh(count, 1.7976931348623157e308), last(count, 1.7976931348623157e308), hv(count);
+  std::vector<int> counter(count, 0);
+  std::vector<char> active(count, 1);
+  for (int q = 0; q < count; ++q) nrec[q] = 0;
+  double hext = lp->hstart;
+  for (int64_t idx = 0; idx < nmax; ++idx) {
+    bool any = false;
+    for (int q = 0; q < count; ++q) {
+      active[q] = active[q] && mh[q] > lp->mfinal;
+      any = any || active[q];
+      hv[q] = hext;
+    }
+    if (!any) break;
+    mm_status st = batch_run(batch, hv.data(), sp, active);
+    if (st != MM_OK) return st == MM_NONFINITE ? fail(st, "energy is not finite at field " + std::to_string(hext)) : st;
+    for (int q = 0; q < count; ++q) {
+      if (!active[q]) continue;
+      DevMesh& m = batch->meshes[q]->dm;
+      mh[q] = m.h_resd[1];
+      if ((last[q] - mh[q]) > lp->mstep) {
+        counter[q] += 1;
+        last[q] = mh[q];
+      }
+      mm_record& r = rec[(size_t)q * max_steps + idx];
+      r.counter = counter[q];
+      r.hext = hext;
+      r.mh = mh[q];
+      r.energy = m.h_resd[0];
+      if (steps) fill_result(m, MM_OK, steps[(size_t)q * max_steps + idx]);
+      nrec[q] = (int32_t)(idx + 1);
+    }
+    hext = hext + lp->hstep;
+  }
+  return MM_OK;
+  API_END
+}
+
+mm_status mm_batch_timer_start(mm_batch* batch) {
+  API_BEGIN
+  if (!batch) throw std::runtime_error("NULL batch");
+  MM_CK(cudaSetDevice(batch->device));
+  if (!batch->ev0) MM_CK(cudaEventCreate(&batch->ev0));
+  if (!batch->ev1) MM_CK(cudaEventCreate(&batch->ev1));
+  MM_CK(cudaEventRecord(batch->ev0, batch->stream));
+  return MM_OK;
+  API_END
+}
+
+mm_status mm_batch_timer_stop(mm_batch* batch, double* elapsed_ms) {
+  API_BEGIN
+  if (!batch || !elapsed_ms || !batch->ev0) throw std::runtime_error("timer not started");
+  MM_CK(cudaSetDevice(batch->device));
+  MM_CK(cudaEventRecord(batch->ev1, batch->stream));
+  MM_CK(cudaEventSynchronize(batch->ev1));
+  float ms = 0.f;
+  MM_CK(cudaEventElapsedTime(&ms, batch->ev0, batch->ev1));
   *elapsed_ms = ms;
   return MM_OK;
   API_END

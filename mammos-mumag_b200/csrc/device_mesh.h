@@ -88,7 +88,7 @@ struct SolveArgs {
   long long* resi;  // [0] ncg iters, [1] evals, [2] pcg iters, [3] ls shrinks, [4] minv iters
 };
 
-enum { MODE_EVAL = 0, MODE_MINV = 1, MODE_MINIMIZE = 2 };
+enum { MODE_EVAL = 0, MODE_MINV = 1, MODE_MINIMIZE = 2, MODE_IDLE = 3 };
 enum { FLAG_ABORT = 0, FLAG_STATUS = 1 };
 
 struct DevMesh {
@@ -139,11 +139,25 @@ struct DevMesh {
   size_t smem = 0;
 };
 
+// A batched persistent launch over several meshes: mesh q runs on CTAs
+// [group[q], group[q+1]) with its own staging decision for that group size.
+struct BatchPlan {
+  std::vector<int> group;
+  std::vector<int> stage;
+  std::vector<int64_t> stage_max, meta_max;
+  int grid = 0, block = 256;
+  size_t smem = 0;
+};
+
 // assemble.cu
 void assemble_operators(DevMesh& m);
 // solver.cu
 void solver_configure(DevMesh& m);
 cudaError_t solver_launch(DevMesh& m, const SolveArgs& a);
 SolveArgs solver_args(const DevMesh& m, int mode, double h, const mm_solver_params& sp);
+cudaError_t launch_prep(DevMesh& m, cudaStream_t st);
+void batch_configure(const std::vector<DevMesh*>& ms, BatchPlan& plan);
+cudaError_t batch_launch(const BatchPlan& plan, const SolveArgs* d_args, const int* d_group, int count,
+                         cudaStream_t st);
 
 }  // namespace mumag

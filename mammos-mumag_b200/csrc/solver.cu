@@ -893,7 +893,7 @@ __device__ bool minimize(Ctx& c) {
   END_ROWS
   double v[1] = {pm};
   CHECK(grid_reduce<1>(c.sy, v, 0u));
-  if (blockIdx.x == 0 && threadIdx.x == 0) {
+  if (c.sy.blk == 0 && threadIdx.x == 0) {
     a.resd[0] = f;
     a.resd[1] = v[0] / a.V;
     a.resi[0] = k;
@@ -902,15 +902,17 @@ __device__ bool minimize(Ctx& c) {
   return true;
 }
 
-__global__ void __launch_bounds__(256, 1) k_solve(const __grid_constant__ SolveArgs args) {
-  extern __shared__ __align__(16) unsigned char smem[];
+// One field step (or one evaluation / M_inv application) of one mesh, run by a group of
+// nblk CTAs of which this is number blk.
+__device__ __forceinline__ void solve_body(const SolveArgs& args, int nblk, int blk, unsigned char* smem) {
+  if (args.mode == MODE_IDLE) return;
   Ctx c(args);
   c.sy.bar = args.bar;
   c.sy.red = args.red;
   c.sy.flags = args.flags;
   c.sy.epoch = 0;
-  c.sy.nblk = gridDim.x;
-  c.sy.blk = blockIdx.x;
+  c.sy.nblk = nblk;
+  c.sy.blk = blk;
   c.sy.slot = 0;
   c.sy.t_sync = 0;
   c.sy.t_pre = c.sy.t_bar = c.sy.t_post = 0;
@@ -919,8 +921,8 @@ __global__ void __launch_bounds__(256, 1) k_solve(const __grid_constant__ SolveA
   c.lane = threadIdx.x & 31;
   c.warp = threadIdx.x >> 5;
   c.nwarps = blockDim.x >> 5;
-  c.s0 = (int)(((long long)args.nslices * blockIdx.x) / gridDim.x);
-  c.s1 = (int)(((long long)args.nslices * (blockIdx.x + 1)) / gridDim.x);
+  c.s0 = (int)(((long long)args.nslices * blk) / nblk);
+  c.s1 = (int)(((long long)args.nslices * (blk + 1)) / nblk);
   {  // slice metadata of this CTA, after the staged operator entries
     const size_t staged = args.stage ? (size_t)args.stage_max * (sizeof(double) + sizeof(int32_t) + (args.mixed ? sizeof(float) : 0)) : 0;
     int64_t* soff = reinterpret_cast<int64_t*>(smem + ((staged + 15) & ~(size_t)15));
@@ -959,7 +961,7 @@ __global__ void __launch_bounds__(256, 1) k_solve(const __grid_constant__ SolveA
   if (args.mode == MODE_EVAL) {
     EvalOut o;
     ok = eval(c, args.x, args.x, nullptr, args.g, o);
-    if (ok && blockIdx.x == 0 && threadIdx.x == 0) {
+    if (ok && blk == 0 && threadIdx.x == 0) {
       args.resd[0] = o.E;
       if (!(o.E - o.E == 0.0)) atomicCAS(&args.flags[FLAG_STATUS], 0, (int)MM_NONFINITE);
     }
@@ -968,7 +970,7 @@ __global__ void __launch_bounds__(256, 1) k_solve(const __grid_constant__ SolveA
   } else {
     ok = minimize(c);
   }
-  if (ok && blockIdx.x == 0 && threadIdx.x == 0) {
+  if (ok && blk == 0 && threadIdx.x == 0) {
     args.resi[1] = c.evals;
     args.resi[2] = c.pcg_iters;
     args.resi[3] = c.shrinks;
@@ -978,7 +980,7 @@ __global__ void __launch_bounds__(256, 1) k_solve(const __grid_constant__ SolveA
     args.resi[7] = (long long)c.sy.epoch;                 // grid barriers executed
   }
   if (args.prof && threadIdx.x == 0) {
-    long long* p = args.prof + 4 * blockIdx.x;
+    long long* p = args.prof + 4 * blk;
     p[0] += (long long)c.t_pcg_phase;
     p[1] += (long long)c.sy.t_pre;
     p[2] += (long long)c.sy.t_bar;
@@ -986,37 +988,72 @@ __global__ void __launch_bounds__(256, 1) k_solve(const __grid_constant__ SolveA
   }
 }
 
+__global__ void __launch_bounds__(256, 1) k_solve(const __grid_constant__ SolveArgs args) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  solve_body(args, gridDim.x, blockIdx.x, smem);
+}
+
+// Batched persistent launch: mesh q owns CTAs [group[q], group[q+1]); each group runs its
+// mesh's field step with group-local barriers and reductions (the mesh's own counter and
+// partials), independent of the other groups.
+__global__ void __launch_bounds__(256, 1) k_solve_batch(const SolveArgs* __restrict__ args, const int* __restrict__ group,
+                                                        int count) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  int lo = 0, hi = count;  // largest q with group[q] <= blockIdx.x
+  while (hi - lo > 1) {
+    const int mid = (lo + hi) / 2;
+    if (group[mid] <= (int)blockIdx.x) lo = mid; else hi = mid;
+  }
+  solve_body(args[lo], group[lo + 1] - group[lo], (int)blockIdx.x - group[lo], smem);
+}
+
+}  // namespace
+
+namespace {
+// Shared-memory plan of one mesh run by `grid` CTAs: staged SELL entries of the largest
+// CTA, slice metadata of the largest CTA, and whether the staging fits under `limit`.
+struct StagePlan {
+  int stage;
+  int64_t stage_max, meta_max;
+  size_t smem;
+};
+StagePlan stage_plan(const DevMesh& m, int grid, size_t limit) {
+  int64_t emax = 0, smax = 0;
+  for (int b = 0; b < grid; ++b) {
+    const int64_t s0 = (m.h.nslices * b) / grid, s1 = (m.h.nslices * (b + 1)) / grid;
+    emax = std::max(emax, m.h.sl_off[s1] - m.h.sl_off[s0]);
+    smax = std::max(smax, s1 - s0);
+  }
+  const size_t meta = (size_t)smax * (sizeof(int64_t) + sizeof(int32_t));
+  const size_t need = (size_t)emax * (sizeof(double) + sizeof(int32_t) + (m.vals32 ? sizeof(float) : 0));
+  StagePlan p;
+  p.stage = (need + meta + 16 <= limit) ? 1 : 0;
+  p.stage_max = emax;
+  p.meta_max = smax;
+  p.smem = (p.stage ? ((need + 15) & ~(size_t)15) : 0) + meta;
+  return p;
+}
 }  // namespace
 
 void solver_configure(DevMesh& m) {
   int dev = m.device;
   cudaDeviceProp prop;
   if (cudaGetDeviceProperties(&prop, dev) != cudaSuccess) throw std::runtime_error("cudaGetDeviceProperties failed");
-  // at least 8 warps: warp k polls reduced value k (up to kMaxRed values)
+  // at least 8 warps: warp k sums reduced value k (up to kMaxRed values)
   int block = m.opt.block_threads > 0 ? m.opt.block_threads : 256;
-  block = std::max(32 * kMaxRed, std::min(256, (block / 32) * 32));  // warp k sums value k
+  block = std::max(32 * kMaxRed, std::min(256, (block / 32) * 32));
   const int warps = block / 32;
   int grid = m.opt.grid_ctas > 0 ? m.opt.grid_ctas
                                  : (int)std::min<int64_t>(prop.multiProcessorCount,
                                                           (m.h.nslices + warps - 1) / warps);
   grid = std::max(1, std::min(grid, 256));  // a reduction warp covers 8 x 32 CTAs
   grid = (int)std::min<int64_t>(grid, m.h.nslices);
-  // shared-memory staging of the CTA's SELL columns and Poisson values
-  int64_t emax = 0;
-  for (int b = 0; b < grid; ++b) {
-    const int64_t s0 = (m.h.nslices * b) / grid, s1 = (m.h.nslices * (b + 1)) / grid;
-    emax = std::max(emax, m.h.sl_off[s1] - m.h.sl_off[s0]);
-  }
-  int64_t smax = 0;
-  for (int b = 0; b < grid; ++b)
-    smax = std::max(smax, (m.h.nslices * (b + 1)) / grid - (m.h.nslices * b) / grid);
-  const size_t meta = (size_t)smax * (sizeof(int64_t) + sizeof(int32_t));
-  const size_t need = (size_t)emax * (sizeof(double) + sizeof(int32_t) + (m.vals32 ? sizeof(float) : 0));
-  const size_t limit = (size_t)prop.sharedMemPerBlockOptin - 16 * 1024 - meta - 16;  // room for static smem
-  m.stage = need <= limit ? 1 : 0;
-  m.stage_max = emax;
-  m.meta_max = smax;
-  m.smem = (m.stage ? ((need + 15) & ~(size_t)15) : 0) + meta;
+  const size_t limit = (size_t)prop.sharedMemPerBlockOptin - 16 * 1024;  // room for static smem
+  const StagePlan sp = stage_plan(m, grid, limit);
+  m.stage = sp.stage;
+  m.stage_max = sp.stage_max;
+  m.meta_max = sp.meta_max;
+  m.smem = sp.smem;
   if (cudaFuncSetAttribute(k_solve, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)m.smem) != cudaSuccess)
     throw std::runtime_error("cannot reserve shared memory for the solver kernel");
   int occ = 0;
@@ -1026,6 +1063,88 @@ void solver_configure(DevMesh& m) {
   grid = std::min(grid, occ * prop.multiProcessorCount);
   m.grid = grid;
   m.block = block;
+}
+
+void batch_configure(const std::vector<DevMesh*>& ms, BatchPlan& plan) {
+  const int count = (int)ms.size();
+  if (count < 1) throw std::runtime_error("empty batch");
+  const int dev = ms[0]->device;
+  for (auto* m : ms)
+    if (m->device != dev) throw std::runtime_error("all meshes of a batch must live on one device");
+  cudaDeviceProp prop;
+  if (cudaGetDeviceProperties(&prop, dev) != cudaSuccess) throw std::runtime_error("cudaGetDeviceProperties failed");
+  const int total = prop.multiProcessorCount;  // one CTA per SM
+  if (count > total) throw std::runtime_error("a batch holds at most one mesh per SM");
+  // CTAs proportional to the mesh's slices, at least one, at most its standalone grid
+  double wsum = 0;
+  for (auto* m : ms) wsum += (double)m->h.nslices;
+  std::vector<int> g(count);
+  int used = 0;
+  for (int q = 0; q < count; ++q) {
+    g[q] = std::max(1, (int)std::floor(total * (double)ms[q]->h.nslices / wsum));
+    g[q] = std::min({g[q], ms[q]->grid, (int)ms[q]->h.nslices});
+    used += g[q];
+  }
+  while (used > total) {  // trim the largest groups
+    int qm = (int)(std::max_element(g.begin(), g.end()) - g.begin());
+    g[qm] -= 1;
+    used -= 1;
+  }
+  for (bool grew = true; grew && used < total;) {  // hand spare SMs to the most loaded groups
+    grew = false;
+    int best = -1;
+    double load = 0;
+    for (int q = 0; q < count; ++q)
+      if (g[q] < ms[q]->grid && g[q] < ms[q]->h.nslices) {
+        const double l = (double)ms[q]->h.nslices / g[q];
+        if (l > load) {
+          load = l;
+          best = q;
+        }
+      }
+    if (best >= 0) {
+      g[best] += 1;
+      used += 1;
+      grew = true;
+    }
+  }
+  const size_t limit = (size_t)prop.sharedMemPerBlockOptin - 16 * 1024;
+  plan.group.assign(count + 1, 0);
+  plan.stage.resize(count);
+  plan.stage_max.resize(count);
+  plan.meta_max.resize(count);
+  plan.smem = 0;
+  for (int q = 0; q < count; ++q) {
+    plan.group[q + 1] = plan.group[q] + g[q];
+    const StagePlan sp = stage_plan(*ms[q], g[q], limit);
+    plan.stage[q] = sp.stage;
+    plan.stage_max[q] = sp.stage_max;
+    plan.meta_max[q] = sp.meta_max;
+    plan.smem = std::max(plan.smem, sp.smem);
+  }
+  plan.grid = plan.group[count];
+  plan.block = 256;
+  if (cudaFuncSetAttribute(k_solve_batch, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)plan.smem) != cudaSuccess)
+    throw std::runtime_error("cannot reserve shared memory for the batched solver kernel");
+  int occ = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_solve_batch, plan.block, plan.smem) != cudaSuccess ||
+      occ * prop.multiProcessorCount < plan.grid)
+    throw std::runtime_error("batched solver kernel cannot keep all its CTAs resident");
+}
+
+cudaError_t batch_launch(const BatchPlan& plan, const SolveArgs* d_args, const int* d_group, int count,
+                         cudaStream_t st) {
+  cudaLaunchConfig_t cfg{};
+  cfg.gridDim = dim3(plan.grid);
+  cfg.blockDim = dim3(plan.block);
+  cfg.dynamicSmemBytes = plan.smem;
+  cfg.stream = st;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeCooperative;
+  attr[0].val.cooperative = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, k_solve_batch, d_args, d_group, count);
 }
 
 SolveArgs solver_args(const DevMesh& m, int mode, double h, const mm_solver_params& sp) {
@@ -1088,12 +1207,15 @@ SolveArgs solver_args(const DevMesh& m, int mode, double h, const mm_solver_para
   return a;
 }
 
+cudaError_t launch_prep(DevMesh& m, cudaStream_t st) {
+  cudaError_t e = cudaMemsetAsync(m.bar, 0, sizeof(unsigned long long), st);
+  if (e == cudaSuccess) e = cudaMemsetAsync(m.flags, 0, 2 * sizeof(int), st);
+  if (e == cudaSuccess) e = cudaMemsetAsync(m.resi, 0, 8 * sizeof(long long), st);
+  return e;
+}
+
 cudaError_t solver_launch(DevMesh& m, const SolveArgs& a) {
-  cudaError_t e = cudaMemsetAsync(m.bar, 0, sizeof(unsigned long long), m.stream);
-  if (e != cudaSuccess) return e;
-  e = cudaMemsetAsync(m.flags, 0, 2 * sizeof(int), m.stream);
-  if (e != cudaSuccess) return e;
-  e = cudaMemsetAsync(m.resi, 0, 8 * sizeof(long long), m.stream);
+  cudaError_t e = launch_prep(m, m.stream);
   if (e != cudaSuccess) return e;
   cudaLaunchConfig_t cfg{};
   cfg.gridDim = dim3(m.grid);

@@ -48,6 +48,13 @@ EXPORTED = (
     "mm_loop",
     "mm_timer_start",
     "mm_timer_stop",
+    "mm_batch_create",
+    "mm_batch_destroy",
+    "mm_batch_groups",
+    "mm_batch_minimize",
+    "mm_batch_loop",
+    "mm_batch_timer_start",
+    "mm_batch_timer_stop",
     "mm_profile_read",
     "mm_poisson_pcg_noalloc",
 )
@@ -184,6 +191,17 @@ def load():
              C.c_int32, _I32, C.c_void_p],
         ),
         "mm_profile_read": (C.c_int, [C.c_void_p, _I64, _I32]),
+        "mm_batch_create": (C.c_int, [C.POINTER(C.c_void_p), C.c_int32, C.POINTER(C.c_void_p)]),
+        "mm_batch_destroy": (C.c_int, [C.c_void_p]),
+        "mm_batch_groups": (C.c_int, [C.c_void_p, _I32]),
+        "mm_batch_minimize": (C.c_int, [C.c_void_p, _D, C.POINTER(SolverParams), C.POINTER(StepResult)]),
+        "mm_batch_loop": (
+            C.c_int,
+            [C.c_void_p, C.POINTER(LoopParams), C.POINTER(SolverParams), C.c_int32, C.POINTER(Record), _I32,
+             C.POINTER(StepResult)],
+        ),
+        "mm_batch_timer_start": (C.c_int, [C.c_void_p]),
+        "mm_batch_timer_stop": (C.c_int, [C.c_void_p, _D]),
         "mm_timer_start": (C.c_int, [C.c_void_p]),
         "mm_timer_stop": (C.c_int, [C.c_void_p, _D]),
         "mm_loop": (
@@ -408,3 +426,72 @@ class Mesh:
         n = nrec.value
         rows = np.array([[rec[i].counter, rec[i].hext, rec[i].mh, rec[i].energy] for i in range(n)]).reshape(n, 4)
         return rows, [steps[i].as_dict() for i in range(n)]
+
+
+class Batch:
+    """Several meshes stepped together in one persistent launch (``mm_batch_*``)."""
+
+    def __init__(self, meshes):
+        self.meshes = list(meshes)
+        arr = (C.c_void_p * len(self.meshes))(*[m._h for m in self.meshes])
+        h = C.c_void_p()
+        check(load().mm_batch_create(arr, len(self.meshes), C.byref(h)))
+        self._h = h
+
+    def close(self):
+        if getattr(self, "_h", None):
+            load().mm_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def groups(self):
+        g = np.zeros(len(self.meshes) + 1, np.int32)
+        check(load().mm_batch_groups(self._h, g.ctypes.data_as(_I32)))
+        return g
+
+    def timer_start(self):
+        check(load().mm_batch_timer_start(self._h))
+
+    def timer_stop(self) -> float:
+        ms = C.c_double()
+        check(load().mm_batch_timer_stop(self._h, C.byref(ms)))
+        return ms.value
+
+    def minimize(self, h, sps):
+        n = len(self.meshes)
+        hv = np.ascontiguousarray(np.broadcast_to(np.asarray(h, np.float64), (n,)))
+        spa = (SolverParams * n)(*sps) if isinstance(sps, (list, tuple)) else (SolverParams * n)(*([sps] * n))
+        res = (StepResult * n)()
+        check(load().mm_batch_minimize(self._h, _dp(hv), spa, res))
+        return [r.as_dict() for r in res]
+
+    def loop(self, hstart, hfinal, hstep, mstep, mfinal, sps, max_steps=0):
+        """Lockstep sweep; returns per mesh (rows [n,4], per-step dicts)."""
+        n = len(self.meshes)
+        nmax = int(abs(hfinal - hstart) / abs(hstep)) + 1
+        if max_steps > 0:
+            nmax = min(nmax, max_steps)
+        lp = LoopParams(hstart, hfinal, hstep, mstep, mfinal, max_steps)
+        spa = (SolverParams * n)(*sps) if isinstance(sps, (list, tuple)) else (SolverParams * n)(*([sps] * n))
+        rec = (Record * (n * nmax))()
+        steps = (StepResult * (n * nmax))()
+        nrec = np.zeros(n, np.int32)
+        check(load().mm_batch_loop(self._h, C.byref(lp), spa, nmax, rec, nrec.ctypes.data_as(_I32), steps))
+        out = []
+        for q in range(n):
+            k = int(nrec[q])
+            rows = np.array([[rec[q * nmax + i].counter, rec[q * nmax + i].hext, rec[q * nmax + i].mh,
+                              rec[q * nmax + i].energy] for i in range(k)]).reshape(k, 4)
+            out.append((rows, [steps[q * nmax + i].as_dict() for i in range(k)]))
+        return out
