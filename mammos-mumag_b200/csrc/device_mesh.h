@@ -18,12 +18,16 @@ struct CudaFailure : std::runtime_error {
   using std::runtime_error::runtime_error;
 };
 
+// On failure the runtime's last-error state is cleared too, so a failed (non-sticky) call
+// does not resurface in a later, unrelated cudaGetLastError().
 #define MM_CK(call)                                                                          \
   do {                                                                                       \
     cudaError_t e_ = (call);                                                                 \
-    if (e_ != cudaSuccess)                                                                   \
+    if (e_ != cudaSuccess) {                                                                 \
+      (void)cudaGetLastError();                                                              \
       throw ::mumag::CudaFailure(std::string(#call) + ": " + cudaGetErrorString(e_) + " (" + \
                                  __FILE__ + ":" + std::to_string(__LINE__) + ")");           \
+    }                                                                                        \
   } while (0)
 
 // Materials per element tag, scripts/materials.py:17-35: Js [T], K = mu0*K1,

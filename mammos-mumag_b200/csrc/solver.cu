@@ -34,6 +34,7 @@ namespace mumag {
 namespace {
 
 constexpr unsigned kSpinLimit = 1u << 23;  // bounded wait per barrier (several seconds)
+constexpr int kMaxCtaPerLane = 10;         // a reduction warp sums up to 320 CTAs
 
 // Grid barrier: one arrival counter (red.release), thread 0 of every CTA polls it with
 // acquire loads.  A grid reduction publishes the CTA's partials before arriving and reads
@@ -134,12 +135,12 @@ __device__ __noinline__ bool grid_reduce(Sync& s, double (&v)[K], unsigned maxma
     const int k = warp;
     const bool mx = (maxmask >> k) & 1;
     const double* p = set + (size_t)k * s.nblk;
-    double got[8];
+    double got[kMaxCtaPerLane];
 #pragma unroll
-    for (int t = 0; t < 8; ++t) got[t] = (lane + 32 * t < s.nblk) ? __ldcg(p + lane + 32 * t) : 0.0;
+    for (int t = 0; t < kMaxCtaPerLane; ++t) got[t] = (lane + 32 * t < s.nblk) ? __ldcg(p + lane + 32 * t) : 0.0;
     double a = got[0];
 #pragma unroll
-    for (int t = 1; t < 8; ++t) a = mx ? fmax(a, got[t]) : a + got[t];
+    for (int t = 1; t < kMaxCtaPerLane; ++t) a = mx ? fmax(a, got[t]) : a + got[t];
     a = mx ? warp_max(a) : warp_sum(a);
     if (lane == 0) res[k] = a;
   }
@@ -988,7 +989,7 @@ __device__ __forceinline__ void solve_body(const SolveArgs& args, int nblk, int 
   }
 }
 
-__global__ void __launch_bounds__(256, 1) k_solve(const __grid_constant__ SolveArgs args) {
+__global__ void __launch_bounds__(256, 2) k_solve(const __grid_constant__ SolveArgs args) {
   extern __shared__ __align__(16) unsigned char smem[];
   solve_body(args, gridDim.x, blockIdx.x, smem);
 }
@@ -996,7 +997,7 @@ __global__ void __launch_bounds__(256, 1) k_solve(const __grid_constant__ SolveA
 // Batched persistent launch: mesh q owns CTAs [group[q], group[q+1]); each group runs its
 // mesh's field step with group-local barriers and reductions (the mesh's own counter and
 // partials), independent of the other groups.
-__global__ void __launch_bounds__(256, 1) k_solve_batch(const SolveArgs* __restrict__ args, const int* __restrict__ group,
+__global__ void __launch_bounds__(256, 2) k_solve_batch(const SolveArgs* __restrict__ args, const int* __restrict__ group,
                                                         int count) {
   extern __shared__ __align__(16) unsigned char smem[];
   int lo = 0, hi = count;  // largest q with group[q] <= blockIdx.x
@@ -1046,7 +1047,7 @@ void solver_configure(DevMesh& m) {
   int grid = m.opt.grid_ctas > 0 ? m.opt.grid_ctas
                                  : (int)std::min<int64_t>(prop.multiProcessorCount,
                                                           (m.h.nslices + warps - 1) / warps);
-  grid = std::max(1, std::min(grid, 256));  // a reduction warp covers 8 x 32 CTAs
+  grid = std::max(1, std::min(grid, 32 * kMaxCtaPerLane));
   grid = (int)std::min<int64_t>(grid, m.h.nslices);
   const size_t limit = (size_t)prop.sharedMemPerBlockOptin - 16 * 1024;  // room for static smem
   const StagePlan sp = stage_plan(m, grid, limit);
@@ -1054,7 +1055,10 @@ void solver_configure(DevMesh& m) {
   m.stage_max = sp.stage_max;
   m.meta_max = sp.meta_max;
   m.smem = sp.smem;
-  if (cudaFuncSetAttribute(k_solve, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)m.smem) != cudaSuccess)
+  // The attribute is per kernel, shared by every mesh: raise it to the device limit once
+  // (occupancy follows each launch's actual request).
+  if (cudaFuncSetAttribute(k_solve, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)(prop.sharedMemPerBlockOptin - 16 * 1024)) != cudaSuccess)
     throw std::runtime_error("cannot reserve shared memory for the solver kernel");
   int occ = 0;
   if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_solve, block, m.smem) != cudaSuccess || occ < 1)
@@ -1073,8 +1077,10 @@ void batch_configure(const std::vector<DevMesh*>& ms, BatchPlan& plan) {
     if (m->device != dev) throw std::runtime_error("all meshes of a batch must live on one device");
   cudaDeviceProp prop;
   if (cudaGetDeviceProperties(&prop, dev) != cudaSuccess) throw std::runtime_error("cudaGetDeviceProperties failed");
-  const int total = prop.multiProcessorCount;  // one CTA per SM
-  if (count > total) throw std::runtime_error("a batch holds at most one mesh per SM");
+  int occ1 = 0;  // resident CTAs per SM of the batched kernel (registers bound it)
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ1, k_solve_batch, 256, 0) != cudaSuccess || occ1 < 1) occ1 = 1;
+  const int total = std::min(32 * kMaxCtaPerLane, std::min(occ1, 2) * prop.multiProcessorCount);
+  if (count > total) throw std::runtime_error("a batch holds at most " + std::to_string(total) + " meshes");
   // CTAs proportional to the mesh's slices, at least one, at most its standalone grid
   double wsum = 0;
   for (auto* m : ms) wsum += (double)m->h.nslices;
@@ -1108,7 +1114,10 @@ void batch_configure(const std::vector<DevMesh*>& ms, BatchPlan& plan) {
       grew = true;
     }
   }
-  const size_t limit = (size_t)prop.sharedMemPerBlockOptin - 16 * 1024;
+  // staging must leave room for the resident CTAs per SM the plan counts on
+  const int per_sm = std::max(1, (total + prop.multiProcessorCount - 1) / prop.multiProcessorCount);
+  const size_t limit = std::min((size_t)prop.sharedMemPerBlockOptin, (size_t)prop.sharedMemPerMultiprocessor / per_sm) -
+                       16 * 1024;
   plan.group.assign(count + 1, 0);
   plan.stage.resize(count);
   plan.stage_max.resize(count);
@@ -1124,7 +1133,8 @@ void batch_configure(const std::vector<DevMesh*>& ms, BatchPlan& plan) {
   }
   plan.grid = plan.group[count];
   plan.block = 256;
-  if (cudaFuncSetAttribute(k_solve_batch, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)plan.smem) != cudaSuccess)
+  if (cudaFuncSetAttribute(k_solve_batch, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)(prop.sharedMemPerBlockOptin - 16 * 1024)) != cudaSuccess)
     throw std::runtime_error("cannot reserve shared memory for the batched solver kernel");
   int occ = 0;
   if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_solve_batch, plan.block, plan.smem) != cudaSuccess ||
