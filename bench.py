@@ -62,6 +62,13 @@ def batch_workload(count: int = 64, seed: int = 0):
 def workload(name: str, seed: int):
     from mammos_mumag import synthetic
 
+    if name == "large":
+        X, T, tag, krn, m0 = synthetic.multigrain(n=80, L=200.0, grains=27, cone_deg=20.0, gb=2.0, seed=seed)
+        hdir = [0.0, 0.0, 1.0]
+        sweep = dict(hstart=8.0, hfinal=-8.0, hstep=-0.05, mstep=0.4, mfinal=-2.0, max_steps=20)
+        desc = ("large multigrain 200 nm, 80^3 x 6 tets (3,072,000 tets, 531,441 nodes), 27 Voronoi grains "
+                "(20 deg cone) + 2 nm grain-boundary phase, +8 T in 0.05 T steps, first 20 field steps of 321")
+        return X, T, tag, krn, m0, hdir, sweep, desc
     if name == "single":
         X, T, tag, krn, m0 = synthetic.single_grain(16, 20.0, seed=seed)
         hdir = [0.0, 0.0, 1.0]
@@ -164,6 +171,7 @@ def cpu_sample(name: str, n_field_steps: int, seed: int = 0):
     X, T, tag, krn, m0, hdir, sweep, _ = workload(name, seed)
     P = O.Problem(X, T, tag, krn)
     par = dict(hdir=hdir, tol_fun=1e-10, tol_u=1e-10, precond_iter=10, hmag_on=1, m=[0, 0, 1.0], **sweep)
+    par.pop("max_steps", None)
     t = time.perf_counter()
     rows, _ = O.run_loop(P, par, m0=m0, max_steps=n_field_steps)
     dt = time.perf_counter() - t
@@ -239,12 +247,20 @@ def run_b200(args, world, rank, local):
     sp = _native.solver_params(hdir=hdir)
     flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=f"cuda:{local}")
     mesh = _native.Mesh(X, T, tag, krn, device=local)
+    mesh.set_state(m0, None, m0)
+    mesh.autotune(sp)  # launch shape (setup, untimed)
     info = mesh.info()
     nfs_expected = int(abs(sweep["hfinal"] - sweep["hstart"]) / abs(sweep["hstep"])) + 1
+    if sweep.get("max_steps"):
+        nfs_expected = min(nfs_expected, sweep["max_steps"])
 
-    def one_sweep():
-        mesh.set_state(m0, None, m0)
-        return mesh.loop(sweep["hstart"], sweep["hfinal"], sweep["hstep"], sweep["mstep"], sweep["mfinal"], sp)
+    sw = (sweep["hstart"], sweep["hfinal"], sweep["hstep"], sweep["mstep"], sweep["mfinal"])
+    mx = sweep.get("max_steps", 0)
+
+    def one_sweep(msh=None):
+        msh = msh or mesh
+        msh.set_state(m0, None, m0)
+        return msh.loop(*sw, sp, max_steps=mx)
 
     for _ in range(args.warmup):
         one_sweep()
@@ -257,7 +273,7 @@ def run_b200(args, world, rank, local):
             torch.cuda.synchronize()
             mesh.set_state(m0, None, m0)
             mesh.timer_start()
-            rows, steps = mesh.loop(sweep["hstart"], sweep["hfinal"], sweep["hstep"], sweep["mstep"], sweep["mfinal"], sp)
+            rows, steps = mesh.loop(*sw, sp, max_steps=mx)
             total_ms += mesh.timer_stop()
             nfs += len(rows)
             steps_all += steps
@@ -279,6 +295,33 @@ def run_b200(args, world, rank, local):
     evals = sum(st["evals"] for st in steps_all)
     pcg = sum(st["pcg_iters"] for st in steps_all)
     hc, mr = hc_mr(rows)
+    variants = {"fp64": {"value": value, "pcg_iters_per_solve": pcg / evals, "hc_T": hc, "mr_T": mr}}
+    if not args.no_mixed:
+        with _native.Mesh(X, T, tag, krn, device=local, precision=_native.PREC_MIXED) as mm:
+            mm.set_state(m0, None, m0)
+            mm.autotune(sp)
+            for _ in range(max(1, args.warmup)):
+                one_sweep(mm)
+            t_mx, n_mx, st_mx, rows_mx = 0.0, 0, [], None
+            for _ in range(args.steps):
+                flush.fill_(1.0)
+                torch.cuda.synchronize()
+                mm.set_state(m0, None, m0)
+                mm.timer_start()
+                rows_mx, stp = mm.loop(*sw, sp, max_steps=mx)
+                t_mx += mm.timer_stop()
+                n_mx += len(rows_mx)
+                st_mx += stp
+        t_mx = dist_max(t_mx, world)
+        hc2, mr2 = hc_mr(rows_mx)
+        variants["mixed"] = {
+            "value": n_mx * world / (t_mx * 1e-3),
+            "pcg_iters_per_solve": sum(x["pcg_iters"] for x in st_mx) / max(1, sum(x["evals"] for x in st_mx)),
+            "hc_T": hc2, "mr_T": mr2,
+            "dHc_rel": abs(hc2 - hc) / hc if np.isfinite(hc) and np.isfinite(hc2) else None,
+            "dMr_rel": abs(mr2 - mr) / abs(mr) if np.isfinite(mr) and np.isfinite(mr2) else None,
+            "speedup_vs_fp64": (n_mx / t_mx) / (nfs / total_ms),
+        }
     # e2e: the public API from host buffers (pinned), every step: mesh build + upload,
     # state upload, sweep, result read-back
     pin = {k: torch.from_numpy(np.ascontiguousarray(v)).pin_memory() for k, v in
@@ -290,7 +333,8 @@ def run_b200(args, world, rank, local):
         t0 = time.perf_counter()
         with _native.Mesh(pin["X"].numpy(), pin["T"].numpy(), pin["tag"].numpy(), krn, device=local) as mm:
             mm.set_state(pin["m0"].numpy(), None, pin["m0"].numpy())
-            r2, _ = mm.loop(sweep["hstart"], sweep["hfinal"], sweep["hstep"], sweep["mstep"], sweep["mfinal"], sp)
+            mm.autotune(sp)  # cached for this mesh shape: no timing runs after the first
+            r2, _ = mm.loop(*sw, sp, max_steps=mx)
             mfin, _, _ = mm.get_state()
         e2e_t += time.perf_counter() - t0
         e2e_n += len(r2)
@@ -299,7 +343,7 @@ def run_b200(args, world, rank, local):
     line = None
     if rank == 0:
         cpu = None
-        if world == 1:
+        if world == 1 and args.workload != "large":
             v, dt, n = cpu_sample(args.workload, 12)
             cpu = {"value": v, "unit": UNIT, "cores": 1, "kind": "port",
                    "sample": f"first {n} field steps of the sweep ({dt:.1f} s), NumPy/SciPy oracle, single thread"}
@@ -311,6 +355,7 @@ def run_b200(args, world, rank, local):
                        "l2": "256 MB buffer written between timed sweeps (L2 flush)",
                        "grid_ctas": info["grid_ctas"], "block_threads": info["block_threads"]},
             "pcg_iters_per_solve": pcg / evals,
+            "variants": variants,
             "field_steps_per_sweep": nfs // args.steps,
             "hc_T": hc, "mr_T": mr,
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
@@ -337,7 +382,8 @@ def main():
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
-    ap.add_argument("--workload", choices=["multigrain", "single"], default="multigrain")
+    ap.add_argument("--workload", choices=["multigrain", "single", "large"], default="multigrain")
+    ap.add_argument("--no-mixed", action="store_true", help="skip the mixed-precision variant")
     args = ap.parse_args()
     world, rank, local = dist_setup()
     try:

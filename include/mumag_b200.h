@@ -196,6 +196,13 @@ mm_status mm_loop(mm_mesh* mesh, const mm_loop_params* lp, const mm_solver_param
                   mm_record* rec, int32_t* nrec, mm_step_result* steps, mm_snapshot_cb cb,
                   void* user);
 
+/* Autotune the persistent launch shape of this mesh (no counterpart in the reference): times
+ * a cold Poisson solve + energy evaluation at the current state for a few CTA counts (one
+ * per SM, two per SM, in between) and keeps the fastest; u and the full gradient are
+ * restored.  Results are cached per mesh shape and precision for the process.
+ * *grid_out (may be NULL) receives the CTA count chosen. */
+mm_status mm_autotune(mm_mesh* mesh, const mm_solver_params* sp, int32_t* grid_out);
+
 /* ---- batched persistent launch ----------------------------------------------------------
  *
  * Several independent meshes stepped together in ONE cooperative launch: mesh q runs on a

@@ -7,8 +7,12 @@
 #include <cmath>
 #include <cstdlib>
 #include <cstring>
+#include <algorithm>
+#include <map>
 #include <memory>
+#include <mutex>
 #include <new>
+#include <tuple>
 #include <stdexcept>
 #include <string>
 #include <vector>
@@ -340,7 +344,7 @@ mm_status mm_mesh_create(const double* X, int64_t N, const int32_t* T, const int
     if (p != m.ws + total) throw std::logic_error("solver workspace carve does not match its size");
     solver_configure(m);
     dalloc(m.bar, 1);
-    dalloc(m.red, (size_t)2 * kMaxRed * m.grid);
+    dalloc(m.red, (size_t)2 * kMaxRed * kMaxGrid);  // any grid the autotuner may choose
     dalloc(m.flags, 2);
     dalloc(m.resd, 2);
     dalloc(m.resi, 8);
@@ -839,6 +843,79 @@ mm_status mm_batch_timer_stop(mm_batch* batch, double* elapsed_ms) {
   float ms = 0.f;
   MM_CK(cudaEventElapsedTime(&ms, batch->ev0, batch->ev1));
   *elapsed_ms = ms;
+  return MM_OK;
+  API_END
+}
+
+namespace {
+// Launch shapes already chosen for meshes of the same shape and precision (process-wide).
+std::mutex g_tune_mu;
+std::map<std::tuple<int64_t, int64_t, int, int>, int> g_tune_cache;
+}  // namespace
+
+mm_status mm_autotune(mm_mesh* mesh, const mm_solver_params* sp, int32_t* grid_out) {
+  API_BEGIN
+  check_mesh(mesh);
+  check_params(sp);
+  DevMesh& m = mesh->dm;
+  MM_CK(cudaSetDevice(m.device));
+  cudaDeviceProp prop;
+  MM_CK(cudaGetDeviceProperties(&prop, m.device));
+  const auto key = std::make_tuple(m.h.nslices, m.h.nent, m.vals32 ? 1 : 0, m.device);
+  {
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    auto it = g_tune_cache.find(key);
+    if (it != g_tune_cache.end()) {
+      m.opt.grid_ctas = it->second;
+      solver_configure(m);
+      if (grid_out) *grid_out = m.grid;
+      return MM_OK;
+    }
+  }
+  // candidates: one CTA per SM (or one slice per warp), two per SM, and in between
+  const int64_t ns = m.h.nslices;
+  const int sms = prop.multiProcessorCount;
+  std::vector<int> cand;
+  for (int g : {(int)std::min<int64_t>(sms, (ns + 7) / 8), (int)std::min<int64_t>(2 * sms, (ns + 3) / 4),
+                (int)std::min<int64_t>(3 * sms / 2, (ns + 5) / 6)})
+    if (g >= 1 && std::find(cand.begin(), cand.end(), g) == cand.end()) cand.push_back(g);
+  // time a cold Poisson solve + energy evaluation at the current state for each shape
+  std::vector<double> u0, gf0;
+  d2h(u0, m.u, m.h.Npad, m.stream);
+  d2h(gf0, m.gf, 3 * m.h.Npad, m.stream);
+  int best = -1;
+  float best_ms = 0.f;
+  const int saved = m.opt.grid_ctas;
+  for (int g : cand) {
+    m.opt.grid_ctas = g;
+    solver_configure(m);
+    if (m.grid != g) continue;  // not resident
+    float ms = 0.f;
+    for (int rep = 0; rep < 2; ++rep) {
+      MM_CK(cudaMemsetAsync(m.u, 0, sizeof(double) * m.h.Npad, m.stream));
+      mm_status st = run(m, solver_args(m, MODE_EVAL, 0.0, *sp));
+      if (st != MM_OK && st != MM_NONFINITE) {
+        m.opt.grid_ctas = saved;
+        solver_configure(m);
+        return st;
+      }
+      ms = m.last_launch_ms;
+    }
+    if (best < 0 || ms < best_ms) {
+      best = g;
+      best_ms = ms;
+    }
+  }
+  m.opt.grid_ctas = best > 0 ? best : saved;
+  solver_configure(m);
+  MM_CK(cudaMemcpyAsync(m.u, u0.data(), sizeof(double) * m.h.Npad, cudaMemcpyHostToDevice, m.stream));
+  MM_CK(cudaMemcpyAsync(m.gf, gf0.data(), sizeof(double) * 3 * m.h.Npad, cudaMemcpyHostToDevice, m.stream));
+  MM_CK(cudaStreamSynchronize(m.stream));
+  {
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    g_tune_cache[key] = m.grid;
+  }
+  if (grid_out) *grid_out = m.grid;
   return MM_OK;
   API_END
 }

@@ -13,6 +13,7 @@ namespace mumag {
 constexpr int kSlice = 32;      // SELL slice height = one warp, lane = row
 constexpr int kMaxRed = 8;      // values per grid reduction
 constexpr int kNumPlanes = 14;  // S, Aex, K[6], D[3], G[3]
+constexpr int kMaxGrid = 320;   // CTAs a persistent launch may use (reduction coverage)
 
 // Value planes of the node-pair operators, all on one SELL-32 pattern.
 enum Plane {

@@ -1047,7 +1047,9 @@ void solver_configure(DevMesh& m) {
   int grid = m.opt.grid_ctas > 0 ? m.opt.grid_ctas
                                  : (int)std::min<int64_t>(prop.multiProcessorCount,
                                                           (m.h.nslices + warps - 1) / warps);
-  grid = std::max(1, std::min(grid, 32 * kMaxCtaPerLane));
+  // explicit requests may use every resident CTA (up to 2 per SM at 128 registers)
+  static_assert(32 * kMaxCtaPerLane >= kMaxGrid, "reductions must cover every CTA");
+  grid = std::max(1, std::min(grid, kMaxGrid));
   grid = (int)std::min<int64_t>(grid, m.h.nslices);
   const size_t limit = (size_t)prop.sharedMemPerBlockOptin - 16 * 1024;  // room for static smem
   const StagePlan sp = stage_plan(m, grid, limit);
@@ -1079,7 +1081,7 @@ void batch_configure(const std::vector<DevMesh*>& ms, BatchPlan& plan) {
   if (cudaGetDeviceProperties(&prop, dev) != cudaSuccess) throw std::runtime_error("cudaGetDeviceProperties failed");
   int occ1 = 0;  // resident CTAs per SM of the batched kernel (registers bound it)
   if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ1, k_solve_batch, 256, 0) != cudaSuccess || occ1 < 1) occ1 = 1;
-  const int total = std::min(32 * kMaxCtaPerLane, std::min(occ1, 2) * prop.multiProcessorCount);
+  const int total = std::min(kMaxGrid, std::min(occ1, 2) * prop.multiProcessorCount);
   if (count > total) throw std::runtime_error("a batch holds at most " + std::to_string(total) + " meshes");
   // CTAs proportional to the mesh's slices, at least one, at most its standalone grid
   double wsum = 0;

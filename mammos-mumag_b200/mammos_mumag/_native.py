@@ -48,6 +48,7 @@ EXPORTED = (
     "mm_loop",
     "mm_timer_start",
     "mm_timer_stop",
+    "mm_autotune",
     "mm_batch_create",
     "mm_batch_destroy",
     "mm_batch_groups",
@@ -191,6 +192,7 @@ def load():
              C.c_int32, _I32, C.c_void_p],
         ),
         "mm_profile_read": (C.c_int, [C.c_void_p, _I64, _I32]),
+        "mm_autotune": (C.c_int, [C.c_void_p, C.POINTER(SolverParams), _I32]),
         "mm_batch_create": (C.c_int, [C.POINTER(C.c_void_p), C.c_int32, C.POINTER(C.c_void_p)]),
         "mm_batch_destroy": (C.c_int, [C.c_void_p]),
         "mm_batch_groups": (C.c_int, [C.c_void_p, _I32]),
@@ -322,6 +324,12 @@ class Mesh:
 
     def __exit__(self, *exc):
         self.close()
+
+    def autotune(self, sp) -> int:
+        """Pick the persistent launch shape by timing candidates; returns the CTA count."""
+        g = C.c_int32()
+        check(load().mm_autotune(self._h, C.byref(sp), C.byref(g)))
+        return g.value
 
     def timer_start(self):
         check(load().mm_timer_start(self._h))

@@ -142,6 +142,8 @@ def run_loop(workdir, name, m0=None, device=0, grid_ctas=0, block_threads=0, ret
         sp = _native.solver_params(hdir=par["hdir"], tol_fun=par["tol_fun"], tol_u=par["tol_u"],
                                    precond_iter=par["precond_iter"], hmag_on=par["hmag_on"],
                                    mbar_mode=1 if par["mbar"] == "current" else 0)
+        if grid_ctas == 0 and X.shape[0] > 100_000:
+            mesh.autotune(sp)  # large meshes: pick the launch shape by timing
 
         def snapshot(counter, mm, uu):
             vtu.write_vtu(wd / f"{name}_{counter:04d}.vtu", X, T, tag, {"m": mm, "u": uu})
