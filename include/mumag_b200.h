@@ -245,6 +245,61 @@ mm_status mm_batch_timer_stop(mm_batch* batch, double* elapsed_ms);
 mm_status mm_profile_read(mm_mesh* mesh, long long* out, int32_t* nctas);
 mm_status mm_timer_stop(mm_mesh* mesh, double* elapsed_ms);
 
+/* ---- learned warm start of the magnetostatic Poisson solve --------------------------------
+ *
+ * No counterpart in the reference, whose PCG always starts from the previous potential
+ * (scripts/solvers.py:221-231, x0 = u).  A per-node network
+ *   16 features -> 128 -> 128 -> 128 -> 1, GELU (tanh form), BF16 weights, FP32 accumulation
+ * corrects that start: u0 = u_prev + sigma * y(features).  The features of node i over its
+ * 1-ring (its row of the Poisson pattern): m_i (3), u_i, ring mean of m (3) and u, ring max of
+ * m (3) and u, then the Jacobi-scaled initial residual z = (b - S u_prev)/diag(S) in units of
+ * sigma = rms(z): z_i and its ring mean, max and min.  The PCG then runs from u0 to the
+ * reference's tolerance, so the solution criterion is unchanged.  Training and inference
+ * run on the tensor cores (mma.sync m16n8k16 BF16 -> FP32) in this library's own kernels.
+ *
+ * A model holds FP32 master parameters (mm_model_num_params floats: W1 [128][16], b1 [128],
+ * W2 [128][128], b2, W3 [128][128], b3, w4 [128], b4 [1]; W as [out][in]) with BF16 copies
+ * for the products, per-feature normalisation (x - mean) * scale, and the output scale. */
+typedef struct mm_model mm_model;
+
+#define MM_MLP_FEATURES 16
+
+mm_status mm_model_create(int32_t device, uint64_t seed, mm_model** out);
+mm_status mm_model_destroy(mm_model* model);
+int64_t mm_model_num_params(void);
+mm_status mm_model_get_params(mm_model* model, float* params);
+/* Also resets the Adam moments. */
+mm_status mm_model_set_params(mm_model* model, const float* params);
+mm_status mm_model_set_normalization(mm_model* model, const float* fmean, const float* fscale, float out_scale);
+mm_status mm_model_get_normalization(const mm_model* model, float* fmean, float* fscale, float* out_scale);
+/* mean / (1/std) of each feature and the rms of the targets, from n samples. */
+mm_status mm_model_fit_normalization(mm_model* model, const float* feats, const float* target, int64_t n);
+/* Loss (1/n) sum (y - t/out_scale)^2 and its gradient w.r.t. the FP32 parameters (layout of
+ * mm_model_get_params), for n (a multiple of 16) samples feats [n][16], target [n]. */
+mm_status mm_model_grad(mm_model* model, const float* feats, const float* target, int32_t n, float* grads,
+                        float* loss);
+/* Adam (beta 0.9/0.999, eps 1e-8) on shuffled mini-batches of `batch` rows (a multiple of 16);
+ * *final_loss = the last epoch's mean batch loss. */
+mm_status mm_model_train(mm_model* model, const float* feats, const float* target, int64_t n, int32_t epochs,
+                         int32_t batch, float lr, uint64_t seed, float* final_loss);
+/* y [n] = out_scale * network(feats [n][16]) (the correction in units of sigma). */
+mm_status mm_model_predict(mm_model* model, const float* feats, int64_t n, float* y);
+
+/* Warm start of the mesh's Poisson solves: the reference's previous u (default), zero, or
+ * the learned correction of the previous u (model required; it must outlive its use). */
+typedef enum { MM_WARM_PREVIOUS = 0, MM_WARM_ZERO = 1, MM_WARM_LEARNED = 2 } mm_warm_mode;
+mm_status mm_mesh_set_warm_start(mm_mesh* mesh, int32_t mode, const mm_model* model);
+
+/* Training-sample recording: from now on, in every Poisson solve of the mesh (of any entry
+ * point), a hash-selected 1/stride of the nodes record their features
+ * at the warm start and, after the solve, the target (u - u0)/sigma, into a device buffer of
+ * `capacity` samples (later samples are dropped).  capacity 0 stops recording. */
+mm_status mm_mesh_record_samples(mm_mesh* mesh, int64_t capacity, int32_t stride, uint64_t seed);
+/* Copies out up to `cap` recorded samples: feats [cap][16], target [cap], node [cap] (input
+ * node ids; may be NULL); *count = the samples copied. */
+mm_status mm_mesh_read_samples(mm_mesh* mesh, float* feats, float* target, int32_t* node, int64_t cap,
+                               int64_t* count);
+
 /* ---- allocation-free Poisson solve ------------------------------------------------------
  *
  * No counterpart in the reference: an extra entry point of this library for callers that

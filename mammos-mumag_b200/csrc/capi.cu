@@ -102,6 +102,14 @@ void release(DevMesh& m) {
   dfree(m.resd);
   dfree(m.resi);
   dfree(m.prof);
+  dfree(m.feat);
+  dfree(m.du);
+  dfree(m.rs_feat);
+  dfree(m.rs_tgt);
+  dfree(m.rs_u0);
+  dfree(m.rs_node);
+  dfree(m.rs_slot);
+  dfree(m.rs_count);
   if (m.h_resd) cudaFreeHost(m.h_resd);
   if (m.h_resi) cudaFreeHost(m.h_resi);
   if (m.h_flags) cudaFreeHost(m.h_flags);
@@ -146,6 +154,9 @@ void check_params(const mm_solver_params* sp) {
   if (sp->max_pcg_iter < 0 || sp->max_ncg_iter < 1) throw std::runtime_error("iteration caps must be positive");
 }
 
+// The sample-recording hash seed of the next launch (an LCG step).
+unsigned next_seed(unsigned s) { return s * 1664525u + 1013904223u; }
+
 // Run one persistent launch and collect its status.
 mm_status run(DevMesh& m, const SolveArgs& a) {
   MM_CK(cudaSetDevice(m.device));
@@ -157,6 +168,7 @@ mm_status run(DevMesh& m, const SolveArgs& a) {
   MM_CK(cudaMemcpyAsync(m.h_flags, m.flags, 2 * sizeof(int), cudaMemcpyDeviceToHost, m.stream));
   MM_CK(cudaStreamSynchronize(m.stream));
   MM_CK(cudaEventElapsedTime(&m.last_launch_ms, m.evk0, m.evk1));
+  m.rec_seed = next_seed(m.rec_seed);
   const int st = m.h_flags[FLAG_STATUS];
   if (st == MM_TIMEOUT) return fail(MM_TIMEOUT, "a grid barrier of the persistent solver kernel timed out");
   if (st != MM_OK && st != MM_NONFINITE)
@@ -692,6 +704,7 @@ mm_status batch_run(mm_batch* b, const double* h, const mm_solver_params* sp, co
     MM_CK(cudaMemcpyAsync(m.h_flags, m.flags, 2 * sizeof(int), cudaMemcpyDeviceToHost, b->stream));
   }
   MM_CK(cudaStreamSynchronize(b->stream));
+  for (int q = 0; q < count; ++q) b->meshes[q]->dm.rec_seed = next_seed(b->meshes[q]->dm.rec_seed);
   mm_status worst = MM_OK;
   for (int q = 0; q < count; ++q) {
     const int st = b->meshes[q]->dm.h_flags[FLAG_STATUS];
@@ -916,6 +929,93 @@ mm_status mm_autotune(mm_mesh* mesh, const mm_solver_params* sp, int32_t* grid_o
     g_tune_cache[key] = m.grid;
   }
   if (grid_out) *grid_out = m.grid;
+  return MM_OK;
+  API_END
+}
+
+}  // extern "C"
+
+// ---- learned warm start and sample recording --------------------------------------------
+namespace mumag {
+MlpDev model_view(const mm_model* m);
+}
+
+extern "C" {
+
+mm_status mm_mesh_set_warm_start(mm_mesh* mesh, int32_t mode, const mm_model* model) {
+  API_BEGIN
+  check_mesh(mesh);
+  DevMesh& m = mesh->dm;
+  if (mode != MM_WARM_PREVIOUS && mode != MM_WARM_ZERO && mode != MM_WARM_LEARNED)
+    throw std::runtime_error("unknown warm-start mode");
+  if (mode == MM_WARM_LEARNED && !model) throw std::runtime_error("the learned warm start needs a model");
+  MM_CK(cudaSetDevice(m.device));
+  if (mode == MM_WARM_LEARNED) {
+    if (!m.feat) dalloc(m.feat, (size_t)m.h.Npad * kMlpIn);
+    if (!m.du) dalloc(m.du, (size_t)m.h.Npad);
+    m.mlp = model_view(model);
+  } else {
+    m.mlp = MlpDev{};
+  }
+  m.warm = mode;
+  return MM_OK;
+  API_END
+}
+
+mm_status mm_mesh_record_samples(mm_mesh* mesh, int64_t capacity, int32_t stride, uint64_t seed) {
+  API_BEGIN
+  check_mesh(mesh);
+  DevMesh& m = mesh->dm;
+  if (capacity < 0 || capacity > ((int64_t)1 << 31) - 1 || stride < 1) throw std::runtime_error("invalid recording arguments");
+  MM_CK(cudaSetDevice(m.device));
+  MM_CK(cudaStreamSynchronize(m.stream));
+  dfree(m.rs_feat);
+  dfree(m.rs_tgt);
+  dfree(m.rs_u0);
+  dfree(m.rs_node);
+  dfree(m.rs_slot);
+  dfree(m.rs_count);
+  m.rec_cap = 0;
+  if (capacity == 0) return MM_OK;
+  dalloc(m.rs_feat, (size_t)capacity * kMlpIn);
+  dalloc(m.rs_tgt, (size_t)capacity);
+  dalloc(m.rs_u0, (size_t)capacity);
+  dalloc(m.rs_node, (size_t)capacity);
+  dalloc(m.rs_slot, (size_t)m.h.Npad);
+  dalloc(m.rs_count, 1);
+  MM_CK(cudaMemsetAsync(m.rs_slot, 0xFF, sizeof(int32_t) * m.h.Npad, m.stream));
+  MM_CK(cudaMemsetAsync(m.rs_count, 0, sizeof(unsigned long long), m.stream));
+  MM_CK(cudaMemsetAsync(m.rs_tgt, 0, sizeof(float) * capacity, m.stream));
+  MM_CK(cudaStreamSynchronize(m.stream));
+  m.rec_cap = capacity;
+  m.rec_stride = stride;
+  m.rec_seed = (unsigned)(seed ^ (seed >> 32));
+  return MM_OK;
+  API_END
+}
+
+mm_status mm_mesh_read_samples(mm_mesh* mesh, float* feats, float* target, int32_t* node, int64_t cap,
+                               int64_t* count) {
+  API_BEGIN
+  check_mesh(mesh);
+  if (!feats || !target || !count || cap < 0) throw std::runtime_error("invalid arguments");
+  DevMesh& m = mesh->dm;
+  *count = 0;
+  if (m.rec_cap == 0) return MM_OK;
+  MM_CK(cudaSetDevice(m.device));
+  unsigned long long c = 0;
+  MM_CK(cudaMemcpyAsync(&c, m.rs_count, sizeof(c), cudaMemcpyDeviceToHost, m.stream));
+  MM_CK(cudaStreamSynchronize(m.stream));
+  const int64_t k = std::min<int64_t>(std::min<int64_t>((int64_t)c, m.rec_cap), cap);
+  if (k == 0) return MM_OK;
+  MM_CK(cudaMemcpyAsync(feats, m.rs_feat, sizeof(float) * k * kMlpIn, cudaMemcpyDeviceToHost, m.stream));
+  MM_CK(cudaMemcpyAsync(target, m.rs_tgt, sizeof(float) * k, cudaMemcpyDeviceToHost, m.stream));
+  std::vector<int32_t> rows(k);
+  MM_CK(cudaMemcpyAsync(rows.data(), m.rs_node, sizeof(int32_t) * k, cudaMemcpyDeviceToHost, m.stream));
+  MM_CK(cudaStreamSynchronize(m.stream));
+  if (node)
+    for (int64_t q = 0; q < k; ++q) node[q] = m.h.perm[rows[q]];
+  *count = k;
   return MM_OK;
   API_END
 }

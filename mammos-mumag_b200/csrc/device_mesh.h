@@ -9,6 +9,7 @@
 #include <string>
 #include <vector>
 
+#include "mlp.cuh"
 #include "mumag_internal.h"
 
 namespace mumag {
@@ -73,6 +74,24 @@ struct SolveArgs {
   PcgRec32* rec32[2];
   float *pp32, *e32;    // inner search direction and correction
   double* r64;          // FP64 residual of the outer refinement
+  // Poisson warm start (MM_WARM_*): previous u, zero, or previous u + the learned correction
+  int warm;
+  int32_t nreal;        // real (non-padding) rows
+  MlpDev mlp;           // learned warm start: the model
+  float* feat;          // [Npad][kMlpIn] node features of the learned start
+  float* du;            // [Npad] its predicted correction (units of sigma)
+  // training-sample recording (rec_cap > 0): at a hash-selected 1/rec_stride of the
+  // (node, solve) pairs, the node's features at the warm start and, after the solve,
+  // the target (u - u0) / sigma
+  float* rs_feat;       // [rec_cap][kMlpIn]
+  float* rs_tgt;        // [rec_cap]
+  double* rs_u0;        // [rec_cap]
+  int32_t* rs_node;     // [rec_cap] device row
+  int32_t* rs_slot;     // [Npad] sample slot of the row in the current solve, -1 = none
+  unsigned long long* rs_count;
+  long long rec_cap;
+  int rec_stride;
+  unsigned rec_seed;
   // grid synchronisation
   unsigned long long* bar;    // barrier arrival counter, zeroed before each launch
   double* red;                // [2][kMaxRed][gridDim.x] reduction partials
@@ -92,6 +111,7 @@ struct SolveArgs {
   long long* resi;  // [0] ncg iters, [1] evals, [2] pcg iters, [3] ls shrinks, [4] minv iters
 };
 
+enum { WARM_PREV = 0, WARM_ZERO = 1, WARM_LEARNED = 2 };
 enum { MODE_EVAL = 0, MODE_MINV = 1, MODE_MINIMIZE = 2, MODE_IDLE = 3 };
 enum { FLAG_ABORT = 0, FLAG_STATUS = 1 };
 
@@ -123,6 +143,17 @@ struct DevMesh {
   PcgRec32* rec32[2] = {nullptr, nullptr};
   float *pp32 = nullptr, *e32 = nullptr;
   double* r64 = nullptr;
+  // warm start and sample recording (SolveArgs)
+  int warm = 0;
+  MlpDev mlp{};
+  float *feat = nullptr, *du = nullptr;
+  float *rs_feat = nullptr, *rs_tgt = nullptr;
+  double* rs_u0 = nullptr;
+  int32_t *rs_node = nullptr, *rs_slot = nullptr;
+  unsigned long long* rs_count = nullptr;
+  long long rec_cap = 0;
+  int rec_stride = 1;
+  unsigned rec_seed = 0;
   unsigned long long* bar = nullptr;
   double* red = nullptr;
   int* flags = nullptr;

@@ -276,15 +276,197 @@ __device__ __forceinline__ CGNext cg_next(const PcgRec& q, double alpha, double 
   return o;
 }
 
-__device__ bool pcg_solve(Ctx& c, const double* x) {
+// ---------------------------------------------------------------------------------------
+// Warm starts of the Poisson solve (no counterpart in the reference, which always starts
+// from the previous u, scripts/solvers.py:221-231) and training-sample recording.
+// r0 is the solve's FP64 initial residual plane, isig = 1/sigma (mlp.cuh).
+// ---------------------------------------------------------------------------------------
+__device__ __forceinline__ void node_features(const Ctx& c, const double* x, const double* r0, double isig, int i,
+                                              int64_t loff, int w, float (&f)[kMlpIn]) {
+  const SolveArgs& a = c.a;
+  const int n = a.Npad;
+  const double m0 = x[i], m1 = x[n + i], m2 = x[2 * n + i], ui = a.u[i];
+  const double zi = r0[i] * __ldg(a.invdS + i) * isig;
+  double s0 = m0, s1 = m1, s2 = m2, su = ui, sz = zi;
+  double x0 = m0, x1 = m1, x2 = m2, xu = ui, xz = zi, nz = zi;
+  int cnt = 1;
+  for (int k = 0; k < w; ++k) {
+    const int j = c.scol[loff + 32 * (int64_t)k];
+    if (j == i) continue;  // the diagonal and the row's padding
+    const double v0 = x[j], v1 = x[n + j], v2 = x[2 * n + j], vu = a.u[j];
+    const double vz = r0[j] * __ldg(a.invdS + j) * isig;
+    s0 += v0;
+    s1 += v1;
+    s2 += v2;
+    su += vu;
+    sz += vz;
+    x0 = fmax(x0, v0);
+    x1 = fmax(x1, v1);
+    x2 = fmax(x2, v2);
+    xu = fmax(xu, vu);
+    xz = fmax(xz, vz);
+    nz = fmin(nz, vz);
+    ++cnt;
+  }
+  const double ic = 1.0 / cnt;
+  f[0] = (float)m0;
+  f[1] = (float)m1;
+  f[2] = (float)m2;
+  f[3] = (float)ui;
+  f[4] = (float)(s0 * ic);
+  f[5] = (float)(s1 * ic);
+  f[6] = (float)(s2 * ic);
+  f[7] = (float)(su * ic);
+  f[8] = (float)x0;
+  f[9] = (float)x1;
+  f[10] = (float)x2;
+  f[11] = (float)xu;
+  f[12] = (float)zi;
+  f[13] = (float)(sz * ic);
+  f[14] = (float)xz;
+  f[15] = (float)nz;
+}
+
+// The network on the 32 rows of slice s (two 16-row tensor-core tiles); du = 0 on padding rows.
+__device__ __noinline__ void mlp_slice(const MlpDev& M, const float* feat, int s, int lane, float* du, int nreal) {
+  for (int tile = 0; tile < 2; ++tile) {
+    const int r0 = s * 32 + tile * 16;
+    auto F = [&](int row, int col) { return feat[(size_t)(r0 + row) * kMlpIn + col]; };
+    float lo, hi;
+    mlp_tile_forward(M, lane, F, lo, hi);
+    if ((lane & 3) == 0) {
+      const int g = lane >> 2;
+      du[r0 + g] = r0 + g < nreal ? lo : 0.f;
+      du[r0 + g + 8] = r0 + g + 8 < nreal ? hi : 0.f;
+    }
+  }
+}
+
+// Learned start, first half: every row's features and the network's correction du (units
+// of sigma), then a barrier so that the residual update can gather du.
+__device__ __noinline__ bool learned_pass(Ctx& c, const double* x, const double* r0, double isig) {
+  const SolveArgs& a = c.a;
+  FOR_ROWS(c)
+  float f[kMlpIn];
+  node_features(c, x, r0, isig, i, loff_, w_, f);
+  float4* dst = reinterpret_cast<float4*>(a.feat + (size_t)i * kMlpIn);
+  dst[0] = make_float4(f[0], f[1], f[2], f[3]);
+  dst[1] = make_float4(f[4], f[5], f[6], f[7]);
+  dst[2] = make_float4(f[8], f[9], f[10], f[11]);
+  dst[3] = make_float4(f[12], f[13], f[14], f[15]);
+  __syncwarp();
+  mlp_slice(a.mlp, a.feat, s_, c.lane, a.du, a.nreal);
+  END_ROWS
+  return grid_barrier(c.sy);
+}
+
+// A well-mixed hash of (row, solve, launch seed) picks 1/stride of the pairs.
+__device__ __forceinline__ bool rec_pick(unsigned i, unsigned ev, unsigned seed, int stride) {
+  unsigned h = (i * 0x9E3779B1u) ^ (ev * 0x85EBCA77u + seed * 0xC2B2AE3Du);
+  h ^= h >> 15;
+  h *= 0x2C1B3C6Du;
+  h ^= h >> 12;
+  h *= 0x297A2D39u;
+  h ^= h >> 15;
+  return h % (unsigned)stride == 0u;
+}
+
+// Recording, at the warm start (before the solve changes u): features and u0 of picked rows.
+__device__ __noinline__ void record_features(Ctx& c, const double* x, const double* r0, double isig) {
+  const SolveArgs& a = c.a;
+  const unsigned ev = (unsigned)c.evals;
+  FOR_ROWS(c)
+  int slot = -1;
+  if (i < a.nreal && rec_pick((unsigned)i, ev, a.rec_seed, a.rec_stride)) {
+    const unsigned long long q = atomicAdd(a.rs_count, 1ull);
+    if (q < (unsigned long long)a.rec_cap) {
+      slot = (int)q;
+      float f[kMlpIn];
+      node_features(c, x, r0, isig, i, loff_, w_, f);
+      for (int k = 0; k < kMlpIn; ++k) a.rs_feat[(size_t)slot * kMlpIn + k] = f[k];
+      a.rs_u0[slot] = a.u[i];
+      a.rs_node[slot] = i;
+    }
+  }
+  a.rs_slot[i] = slot;
+  END_ROWS
+}
+
+// Recording, after the solve: the target (u - u0) / sigma of the rows picked for this solve.
+__device__ __noinline__ void record_targets(Ctx& c, double sig) {
+  const SolveArgs& a = c.a;
+  FOR_ROWS(c)
+  (void)w_;
+  const int slot = a.rs_slot[i];
+  if (slot >= 0) {
+    a.rs_tgt[slot] = (float)((a.u[i] - a.rs_u0[slot]) / sig);
+    a.rs_slot[i] = -1;
+  }
+  END_ROWS
+}
+
+// Learned start of the FP64 solve: u += sigma du; r = r0 - sigma S du; new gamma = r.z, rr.
+__device__ __noinline__ bool learned_start(Ctx& c, const double* x, double sig, double& gamma, double& rr) {
+  const SolveArgs& a = c.a;
+  const int n = a.Npad;
+  CHECK(learned_pass(c, x, reinterpret_cast<const double*>(a.rec[0]), 1.0 / sig));
+  double pg = 0, pr2 = 0;
+  FOR_ROWS(c)
+  double sd = 0;
+#pragma unroll 8
+  for (int k2 = 0; k2 < w_; ++k2) sd += c.sS[LENTRY(k2)] * (double)a.du[c.scol[LENTRY(k2)]];
+  const PcgRec q = rec_load(a.rec[0], i, n);
+  const double r = q.r - sig * sd;
+  a.u[i] = a.u[i] + sig * (double)a.du[i];
+  rec_store(a.rec[0], i, n, PcgRec{r, 0.0, 0.0, q.invd});
+  pg += r * (r * q.invd);
+  pr2 += r * r;
+  END_ROWS
+  double v[2] = {pg, pr2};
+  CHECK(grid_reduce<2>(c.sy, v, 0u));
+  gamma = v[0];
+  rr = v[1];
+  return true;
+}
+
+// The same for the mixed-precision solve: FP64 residual r64, FP32 inner record; new
+// rr = r.r, rin2 = rf.rf, gin = rf.zf.
+__device__ __noinline__ bool learned_start_mixed(Ctx& c, const double* x, double sig, double& rr, double& rin2,
+                                                 double& gin) {
+  const SolveArgs& a = c.a;
+  CHECK(learned_pass(c, x, a.r64, 1.0 / sig));
+  double p0 = 0, p2 = 0, p3 = 0;
+  FOR_ROWS(c)
+  double sd = 0;
+#pragma unroll 8
+  for (int k2 = 0; k2 < w_; ++k2) sd += c.sS[LENTRY(k2)] * (double)a.du[c.scol[LENTRY(k2)]];
+  const double r = a.r64[i] - sig * sd;
+  a.u[i] = a.u[i] + sig * (double)a.du[i];
+  a.r64[i] = r;
+  const float rf = (float)r, inv = (float)__ldg(a.invdS + i);
+  a.rec32[0][i] = PcgRec32{rf, 0.f, 0.f, inv};
+  p0 += r * r;
+  p2 += (double)rf * (double)rf;
+  p3 += (double)rf * (double)(rf * inv);
+  END_ROWS
+  double v[3] = {p0, p2, p3};
+  CHECK(grid_reduce<3>(c.sy, v, 0u));
+  rr = v[0];
+  rin2 = v[1];
+  gin = v[2];
+  return true;
+}
+
+__device__ __noinline__ bool pcg_solve(Ctx& c, const double* x) {
   const SolveArgs& a = c.a;
   const double* Dk = plane(a, P_D);
   const int64_t ps = a.nent;
   const int n = a.Npad;
   // phase A: b = sum_k dk x_k, r0 = b - S u; record {r0, -, s_{-1} = 0, 1/diag}
-  double gamma, rr, bb;
+  double gamma, rr, bb, zz;
+  const bool zero_start = a.warm == WARM_ZERO;
   {
-    double pg = 0, pr2 = 0, pb = 0;
+    double pg = 0, pr2 = 0, pb = 0, pz = 0;
     FOR_ROWS(c)
     double b = 0, su = 0;
 #pragma unroll 4
@@ -292,24 +474,37 @@ __device__ bool pcg_solve(Ctx& c, const double* x) {
       const int64_t e = ENTRY(k);
       const int j = c.scol[LENTRY(k)];
       b += __ldg(Dk + e) * x[j] + __ldg(Dk + ps + e) * x[n + j] + __ldg(Dk + 2 * ps + e) * x[2 * n + j];
-      su += c.sS[LENTRY(k)] * a.u[j];
+      if (!zero_start) su += c.sS[LENTRY(k)] * a.u[j];
     }
+    if (zero_start) a.u[i] = 0.0;
     const double r = b - su;
     const double invd = __ldg(a.invdS + i);
     rec_store(a.rec[0], i, n, PcgRec{r, 0.0, 0.0, invd});
     pg += r * (r * invd);
     pr2 += r * r;
     pb += b * b;
+    if (i < a.nreal) pz += (r * invd) * (r * invd);
     END_ROWS
-    double v[3] = {pg, pr2, pb};
-    CHECK(grid_reduce<3>(c.sy, v, 0u));
+    double v[4] = {pg, pr2, pb, pz};
+    CHECK(grid_reduce<4>(c.sy, v, 0u));
     gamma = v[0];
     rr = v[1];
     bb = v[2];
+    zz = v[3];
   }
   const double atol2 = fmax(a.tol_u * a.tol_u * bb, 0.0);
   int k = 0;
   if (!(rr > atol2 && k < a.max_pcg)) return true;
+  const double sig = sqrt(zz / (double)a.nreal);
+  const bool recording = a.rec_cap > 0 && sig > 0.0;
+  if (recording) record_features(c, x, reinterpret_cast<const double*>(a.rec[0]), 1.0 / sig);
+  if (a.warm == WARM_LEARNED && sig > 0.0) {
+    CHECK(learned_start(c, x, sig, gamma, rr));
+    if (!(rr > atol2)) {
+      if (recording) record_targets(c, sig);
+      return true;
+    }
+  }
   // phase B: w0 = S z0, delta0 = w0.z0; p_{-1} = 0
   double delta;
   {
@@ -368,6 +563,7 @@ __device__ bool pcg_solve(Ctx& c, const double* x) {
     gamma = v[0];
   }
   c.pcg_iters += k;
+  if (recording) record_targets(c, sig);
   return true;
 }
 
@@ -387,15 +583,16 @@ __device__ __forceinline__ CGNext32 cg_next32(const PcgRec32& q, float alpha, fl
   return o;
 }
 
-__device__ bool pcg_solve_mixed(Ctx& c, const double* x) {
+__device__ __noinline__ bool pcg_solve_mixed(Ctx& c, const double* x) {
   const SolveArgs& a = c.a;
   const double* Dk = plane(a, P_D);
   const double* S64 = plane(a, P_S);
   const int64_t ps = a.nent;
   const int n = a.Npad;
-  double rr, bb, rin2, gin;
+  double rr, bb, rin2, gin, zz;
+  const bool zero_start = a.warm == WARM_ZERO;
   {  // FP64 residual of the warm start; FP32 inner record
-    double p0 = 0, p1 = 0, p2 = 0, p3 = 0;
+    double p0 = 0, p1 = 0, p2 = 0, p3 = 0, pz = 0;
     FOR_ROWS(c)
     double b = 0, su = 0;
 #pragma unroll 4
@@ -403,26 +600,35 @@ __device__ bool pcg_solve_mixed(Ctx& c, const double* x) {
       const int64_t e = ENTRY(k);
       const int j = c.scol[LENTRY(k)];
       b += __ldg(Dk + e) * x[j] + __ldg(Dk + ps + e) * x[n + j] + __ldg(Dk + 2 * ps + e) * x[2 * n + j];
-      su += c.sS[LENTRY(k)] * a.u[j];
+      if (!zero_start) su += c.sS[LENTRY(k)] * a.u[j];
     }
+    if (zero_start) a.u[i] = 0.0;
     const double r = b - su;
-    const float rf = (float)r, inv = (float)__ldg(a.invdS + i);
+    const double invd = __ldg(a.invdS + i);
+    const float rf = (float)r, inv = (float)invd;
     a.r64[i] = r;
     a.rec32[0][i] = PcgRec32{rf, 0.f, 0.f, inv};
     p0 += r * r;
     p1 += b * b;
     p2 += (double)rf * (double)rf;
     p3 += (double)rf * (double)(rf * inv);
+    if (i < a.nreal) pz += (r * invd) * (r * invd);
     END_ROWS
-    double v[4] = {p0, p1, p2, p3};
-    CHECK(grid_reduce<4>(c.sy, v, 0u));
+    double v[5] = {p0, p1, p2, p3, pz};
+    CHECK(grid_reduce<5>(c.sy, v, 0u));
     rr = v[0];
     bb = v[1];
     rin2 = v[2];
     gin = v[3];
+    zz = v[4];
   }
   const double atol2 = fmax(a.tol_u * a.tol_u * bb, 0.0);
   int k = 0;
+  const double sig = sqrt(zz / (double)a.nreal);
+  const bool recording = rr > atol2 && a.max_pcg > 0 && a.rec_cap > 0 && sig > 0.0;
+  if (recording) record_features(c, x, a.r64, 1.0 / sig);
+  if (rr > atol2 && a.max_pcg > 0 && a.warm == WARM_LEARNED && sig > 0.0)
+    CHECK(learned_start_mixed(c, x, sig, rr, rin2, gin));
   for (int outer = 0; rr > atol2 && k < a.max_pcg && outer < 32; ++outer) {
     const double inner_tol2 = fmax(1e-10 * rin2, 0.25 * atol2);  // 1e-5 relative, or the outer target
     double gamma = gin, delta;
@@ -446,7 +652,6 @@ __device__ bool pcg_solve_mixed(Ctx& c, const double* x) {
       delta = v[0];
     }
     double alpha = gamma / delta, beta = 0.0;
-    int last = 0;
     for (int it = 0;; ++it) {
       const PcgRec32* rc = a.rec32[it & 1];
       PcgRec32* rn = a.rec32[(it & 1) ^ 1];
@@ -472,14 +677,12 @@ __device__ bool pcg_solve_mixed(Ctx& c, const double* x) {
       double v[3] = {pg, pd, pr2};
       CHECK(grid_reduce<3>(c.sy, v, 0u));
       ++k;
-      last = it;
       if (!(v[2] > inner_tol2 && k < a.max_pcg)) break;
       const double bn = v[0] / gamma;
       alpha = v[0] / (v[1] - bn * v[0] / alpha);
       beta = bn;
       gamma = v[0];
     }
-    (void)last;
     {  // u += e, r -= S e in FP64; next inner record
       double p0 = 0, p2 = 0, p3 = 0;
       FOR_ROWS(c)
@@ -503,6 +706,7 @@ __device__ bool pcg_solve_mixed(Ctx& c, const double* x) {
     }
   }
   c.pcg_iters += k;
+  if (recording) record_targets(c, sig);
   return true;
 }
 
@@ -1195,6 +1399,20 @@ SolveArgs solver_args(const DevMesh& m, int mode, double h, const mm_solver_para
   a.pp32 = m.pp32;
   a.e32 = m.e32;
   a.r64 = m.r64;
+  a.warm = m.warm;
+  a.nreal = (int32_t)m.h.N;
+  a.mlp = m.mlp;
+  a.feat = m.feat;
+  a.du = m.du;
+  a.rs_feat = m.rs_feat;
+  a.rs_tgt = m.rs_tgt;
+  a.rs_u0 = m.rs_u0;
+  a.rs_node = m.rs_node;
+  a.rs_slot = m.rs_slot;
+  a.rs_count = m.rs_count;
+  a.rec_cap = m.rec_cap;
+  a.rec_stride = m.rec_stride;
+  a.rec_seed = m.rec_seed;
   a.bar = m.bar;
   a.red = m.red;
   a.flags = m.flags;

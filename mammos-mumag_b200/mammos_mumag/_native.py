@@ -58,7 +58,23 @@ EXPORTED = (
     "mm_batch_timer_stop",
     "mm_profile_read",
     "mm_poisson_pcg_noalloc",
+    "mm_model_create",
+    "mm_model_destroy",
+    "mm_model_num_params",
+    "mm_model_get_params",
+    "mm_model_set_params",
+    "mm_model_set_normalization",
+    "mm_model_get_normalization",
+    "mm_model_fit_normalization",
+    "mm_model_grad",
+    "mm_model_train",
+    "mm_model_predict",
+    "mm_mesh_set_warm_start",
+    "mm_mesh_record_samples",
+    "mm_mesh_read_samples",
 )
+WARM_PREVIOUS, WARM_ZERO, WARM_LEARNED = 0, 1, 2
+MLP_FEATURES = 16
 
 
 class Material(C.Structure):
@@ -151,6 +167,7 @@ SNAPSHOT_CB = C.CFUNCTYPE(C.c_int, C.c_int, C.POINTER(C.c_double), C.POINTER(C.c
 _D = C.POINTER(C.c_double)
 _I32 = C.POINTER(C.c_int32)
 _I64 = C.POINTER(C.c_int64)
+_F = C.POINTER(C.c_float)
 _lib = None
 
 
@@ -211,6 +228,21 @@ def load():
             [C.c_void_p, C.POINTER(LoopParams), C.POINTER(SolverParams), C.POINTER(Record), _I32,
              C.POINTER(StepResult), SNAPSHOT_CB, C.c_void_p],
         ),
+        "mm_model_create": (C.c_int, [C.c_int32, C.c_uint64, C.POINTER(C.c_void_p)]),
+        "mm_model_destroy": (C.c_int, [C.c_void_p]),
+        "mm_model_num_params": (C.c_int64, []),
+        "mm_model_get_params": (C.c_int, [C.c_void_p, _F]),
+        "mm_model_set_params": (C.c_int, [C.c_void_p, _F]),
+        "mm_model_set_normalization": (C.c_int, [C.c_void_p, _F, _F, C.c_float]),
+        "mm_model_get_normalization": (C.c_int, [C.c_void_p, _F, _F, _F]),
+        "mm_model_fit_normalization": (C.c_int, [C.c_void_p, _F, _F, C.c_int64]),
+        "mm_model_grad": (C.c_int, [C.c_void_p, _F, _F, C.c_int32, _F, _F]),
+        "mm_model_train": (
+            C.c_int, [C.c_void_p, _F, _F, C.c_int64, C.c_int32, C.c_int32, C.c_float, C.c_uint64, _F]),
+        "mm_model_predict": (C.c_int, [C.c_void_p, _F, C.c_int64, _F]),
+        "mm_mesh_set_warm_start": (C.c_int, [C.c_void_p, C.c_int32, C.c_void_p]),
+        "mm_mesh_record_samples": (C.c_int, [C.c_void_p, C.c_int64, C.c_int32, C.c_uint64]),
+        "mm_mesh_read_samples": (C.c_int, [C.c_void_p, _F, _F, _I32, C.c_int64, _I64]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -233,6 +265,17 @@ def check(status):
 
 def _dp(a):
     return a.ctypes.data_as(_D) if a is not None else None
+
+
+def _fp(a):
+    return a.ctypes.data_as(_F) if a is not None else None
+
+
+def _f32(a, shape=None):
+    a = np.ascontiguousarray(a, dtype=np.float32)
+    if shape is not None and a.shape[1:] != shape:
+        raise ValueError(f"expected rows of shape {shape}, got {a.shape}")
+    return a
 
 
 def device_count() -> int:
@@ -324,6 +367,27 @@ class Mesh:
 
     def __exit__(self, *exc):
         self.close()
+
+    def set_warm_start(self, mode: int, model: "Model | None" = None):
+        """Warm start of the Poisson solves: WARM_PREVIOUS (the reference), WARM_ZERO or
+        WARM_LEARNED (``model`` must stay alive while the mesh uses it)."""
+        check(load().mm_mesh_set_warm_start(self._h, int(mode), model._h if model is not None else None))
+        self._warm_model = model
+
+    def record_samples(self, capacity: int, stride: int = 1, seed: int = 0):
+        """Record (features, target) pairs of 1/stride of the (node, solve) pairs from now on."""
+        check(load().mm_mesh_record_samples(self._h, int(capacity), int(stride), int(seed)))
+
+    def read_samples(self, cap: int | None = None):
+        """Recorded samples: ``(feats [k,16] float32, target [k] float32, node [k] int32)``."""
+        cap = int(cap if cap is not None else 1 << 22)
+        f = np.empty((cap, MLP_FEATURES), np.float32)
+        t = np.empty(cap, np.float32)
+        n = np.empty(cap, np.int32)
+        k = C.c_int64()
+        check(load().mm_mesh_read_samples(self._h, _fp(f), _fp(t), n.ctypes.data_as(_I32), cap, C.byref(k)))
+        k = k.value
+        return f[:k].copy(), t[:k].copy(), n[:k].copy()
 
     def autotune(self, sp) -> int:
         """Pick the persistent launch shape by timing candidates; returns the CTA count."""
@@ -503,3 +567,83 @@ class Batch:
                               rec[q * nmax + i].energy] for i in range(k)]).reshape(k, 4)
             out.append((rows, [steps[q * nmax + i].as_dict() for i in range(k)]))
         return out
+
+
+class Model:
+    """The warm-start network (an ``mm_model`` handle): 16 -> 128 -> 128 -> 128 -> 1, GELU,
+    BF16 weights with FP32 accumulation, trained and evaluated by this library's kernels."""
+
+    def __init__(self, device: int = 0, seed: int = 0):
+        h = C.c_void_p()
+        check(load().mm_model_create(int(device), int(seed), C.byref(h)))
+        self._h = h
+
+    def close(self):
+        if getattr(self, "_h", None):
+            load().mm_model_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    @staticmethod
+    def num_params() -> int:
+        return int(load().mm_model_num_params())
+
+    def get_params(self) -> np.ndarray:
+        p = np.empty(self.num_params(), np.float32)
+        check(load().mm_model_get_params(self._h, _fp(p)))
+        return p
+
+    def set_params(self, p):
+        p = np.ascontiguousarray(p, dtype=np.float32)
+        if p.shape != (self.num_params(),):
+            raise ValueError("wrong parameter count")
+        check(load().mm_model_set_params(self._h, _fp(p)))
+
+    def set_normalization(self, fmean, fscale, out_scale: float):
+        fm, fs = _f32(fmean), _f32(fscale)
+        if fm.shape != (MLP_FEATURES,) or fs.shape != (MLP_FEATURES,):
+            raise ValueError("normalisation vectors have 16 entries")
+        check(load().mm_model_set_normalization(self._h, _fp(fm), _fp(fs), float(out_scale)))
+
+    def get_normalization(self):
+        fm = np.empty(MLP_FEATURES, np.float32)
+        fs = np.empty(MLP_FEATURES, np.float32)
+        o = np.empty(1, np.float32)
+        check(load().mm_model_get_normalization(self._h, _fp(fm), _fp(fs), _fp(o)))
+        return fm, fs, float(o[0])
+
+    def fit_normalization(self, feats, target):
+        f, t = _f32(feats, (MLP_FEATURES,)), _f32(target)
+        check(load().mm_model_fit_normalization(self._h, _fp(f), _fp(t), f.shape[0]))
+
+    def grad(self, feats, target):
+        """(loss, gradient) of one batch (rows a multiple of 16)."""
+        f, t = _f32(feats, (MLP_FEATURES,)), _f32(target)
+        g = np.empty(self.num_params(), np.float32)
+        loss = np.empty(1, np.float32)
+        check(load().mm_model_grad(self._h, _fp(f), _fp(t), f.shape[0], _fp(g), _fp(loss)))
+        return float(loss[0]), g
+
+    def train(self, feats, target, epochs=30, batch=256, lr=1e-3, seed=0) -> float:
+        f, t = _f32(feats, (MLP_FEATURES,)), _f32(target)
+        loss = np.empty(1, np.float32)
+        check(load().mm_model_train(self._h, _fp(f), _fp(t), f.shape[0], int(epochs), int(batch), float(lr),
+                                    int(seed), _fp(loss)))
+        return float(loss[0])
+
+    def predict(self, feats) -> np.ndarray:
+        f = _f32(feats, (MLP_FEATURES,))
+        y = np.empty(f.shape[0], np.float32)
+        check(load().mm_model_predict(self._h, _fp(f), f.shape[0], _fp(y)))
+        return y
