@@ -57,6 +57,10 @@ typedef struct {
   int grid_ctas;       /* persistent-kernel CTAs; 0 = autotuned */
   int block_threads;   /* threads per CTA; 0 = autotuned */
   int reorder;         /* 1 = reverse Cuthill-McKee node order on the device (default), 0 = file order */
+  int pcg_variant;     /* Poisson PCG arrangement: 0 = chosen by size and mm_autotune (default),
+                          1 = one grid synchronisation per iteration (neighbour z recomputed
+                          from gathered r, w, s), 2 = two (z stored, gathered alone); both
+                          give the same iterates */
 } mm_options;
 
 /* Solver settings of one field step (scripts/tools.py:64-120, scripts/minimizers.py:140-190). */
@@ -98,6 +102,8 @@ typedef struct {
   int64_t dirichlet_nodes;
   double volume;                       /* magnetic volume V, nm^3 */
   double bandwidth_before, bandwidth_after;  /* max |i-j| over node pairs, file vs device order */
+  int32_t pcg_variant;                 /* PCG arrangement in use: 1 one-sync, 2 two-sync */
+  int32_t reserved_;
 } mm_mesh_info;
 
 /* Field-sweep parameters (the .p2 [field] section; scripts/loop.py:71-142). */
@@ -198,9 +204,10 @@ mm_status mm_loop(mm_mesh* mesh, const mm_loop_params* lp, const mm_solver_param
 
 /* Autotune the persistent launch shape of this mesh (no counterpart in the reference): times
  * a cold Poisson solve + energy evaluation at the current state for a few CTA counts (one
- * per SM, two per SM, in between) and keeps the fastest; u and the full gradient are
- * restored.  Results are cached per mesh shape and precision for the process.
- * *grid_out (may be NULL) receives the CTA count chosen. */
+ * per SM, two per SM, in between), each with both PCG arrangements unless
+ * options.pcg_variant fixes one, and keeps the fastest; u and the full gradient are
+ * restored.  Results are cached per mesh shape, precision and pcg_variant option for the
+ * process.  *grid_out (may be NULL) receives the CTA count chosen. */
 mm_status mm_autotune(mm_mesh* mesh, const mm_solver_params* sp, int32_t* grid_out);
 
 /* ---- batched persistent launch ----------------------------------------------------------

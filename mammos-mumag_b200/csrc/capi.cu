@@ -200,6 +200,7 @@ void mm_default_options(mm_options* opt) {
   opt->grid_ctas = 0;
   opt->block_threads = 0;
   opt->reorder = 1;
+  opt->pcg_variant = 0;
 }
 
 void mm_default_solver_params(mm_solver_params* sp) {
@@ -259,6 +260,7 @@ mm_status mm_mesh_create(const double* X, int64_t N, const int32_t* T, const int
   mm_default_options(&o);
   if (opt) o = *opt;
   if (!(o.size > 0)) throw std::runtime_error("options.size must be positive");
+  if (o.pcg_variant < 0 || o.pcg_variant > 2) throw std::runtime_error("options.pcg_variant must be 0, 1 or 2");
   for (int64_t i = 0; i < 3 * N; ++i)
     if (!std::isfinite(X[i])) throw std::runtime_error("non-finite node coordinate");
   int ndev = 0;
@@ -275,6 +277,8 @@ mm_status mm_mesh_create(const double* X, int64_t N, const int32_t* T, const int
   m.device = o.device;
   m.opt = o;
   preprocess(X, N, T, tag, E, nmats, o.reorder != 0, m.h);
+  // PCG arrangement: fixed by the caller, else by size until mm_autotune times both
+  m.pcg2 = o.pcg_variant == 2 ? 1 : o.pcg_variant == 1 ? 0 : (m.h.N >= kPcg2Nodes ? 1 : 0);
   HostMesh& h = m.h;
   m.ncolours = (int32_t)h.colour_off.size() - 1;
   // materials, scripts/materials.py:17-35
@@ -404,6 +408,8 @@ mm_status mm_mesh_get_info(const mm_mesh* mesh, mm_mesh_info* info) {
   info->volume = m.V;
   info->bandwidth_before = (double)m.h.bandwidth_before;
   info->bandwidth_after = (double)m.h.bandwidth_after;
+  info->pcg_variant = m.pcg2 ? 2 : 1;
+  info->reserved_ = 0;
   return MM_OK;
   API_END
 }
@@ -863,7 +869,7 @@ mm_status mm_batch_timer_stop(mm_batch* batch, double* elapsed_ms) {
 namespace {
 // Launch shapes already chosen for meshes of the same shape and precision (process-wide).
 std::mutex g_tune_mu;
-std::map<std::tuple<int64_t, int64_t, int, int>, int> g_tune_cache;
+std::map<std::tuple<int64_t, int64_t, int, int, int>, std::pair<int, int>> g_tune_cache;
 }  // namespace
 
 mm_status mm_autotune(mm_mesh* mesh, const mm_solver_params* sp, int32_t* grid_out) {
@@ -874,59 +880,74 @@ mm_status mm_autotune(mm_mesh* mesh, const mm_solver_params* sp, int32_t* grid_o
   MM_CK(cudaSetDevice(m.device));
   cudaDeviceProp prop;
   MM_CK(cudaGetDeviceProperties(&prop, m.device));
-  const auto key = std::make_tuple(m.h.nslices, m.h.nent, m.vals32 ? 1 : 0, m.device);
+  const auto key = std::make_tuple(m.h.nslices, m.h.nent, m.vals32 ? 1 : 0, m.device, m.opt.pcg_variant);
   {
     std::lock_guard<std::mutex> lk(g_tune_mu);
     auto it = g_tune_cache.find(key);
     if (it != g_tune_cache.end()) {
-      m.opt.grid_ctas = it->second;
+      m.opt.grid_ctas = it->second.first;
+      m.pcg2 = it->second.second;
       solver_configure(m);
       if (grid_out) *grid_out = m.grid;
       return MM_OK;
     }
   }
-  // candidates: one CTA per SM (or one slice per warp), two per SM, and in between
+  // candidates: one CTA per SM (or one slice per warp), two per SM, and in between; each
+  // with both PCG arrangements unless the options fix one
   const int64_t ns = m.h.nslices;
   const int sms = prop.multiProcessorCount;
   std::vector<int> cand;
   for (int g : {(int)std::min<int64_t>(sms, (ns + 7) / 8), (int)std::min<int64_t>(2 * sms, (ns + 3) / 4),
                 (int)std::min<int64_t>(3 * sms / 2, (ns + 5) / 6)})
     if (g >= 1 && std::find(cand.begin(), cand.end(), g) == cand.end()) cand.push_back(g);
+  std::vector<int> variants;
+  if (m.opt.pcg_variant == 1)
+    variants = {0};
+  else if (m.opt.pcg_variant == 2)
+    variants = {1};
+  else
+    variants = {0, 1};
   // time a cold Poisson solve + energy evaluation at the current state for each shape
   std::vector<double> u0, gf0;
   d2h(u0, m.u, m.h.Npad, m.stream);
   d2h(gf0, m.gf, 3 * m.h.Npad, m.stream);
-  int best = -1;
+  int best = -1, best_v = m.pcg2;
   float best_ms = 0.f;
-  const int saved = m.opt.grid_ctas;
+  const int saved = m.opt.grid_ctas, saved_v = m.pcg2;
   for (int g : cand) {
     m.opt.grid_ctas = g;
     solver_configure(m);
     if (m.grid != g) continue;  // not resident
-    float ms = 0.f;
-    for (int rep = 0; rep < 2; ++rep) {
-      MM_CK(cudaMemsetAsync(m.u, 0, sizeof(double) * m.h.Npad, m.stream));
-      mm_status st = run(m, solver_args(m, MODE_EVAL, 0.0, *sp));
-      if (st != MM_OK && st != MM_NONFINITE) {
-        m.opt.grid_ctas = saved;
-        solver_configure(m);
-        return st;
+    for (int v : variants) {
+      m.pcg2 = v;
+      float ms = 0.f;
+      for (int rep = 0; rep < 2; ++rep) {
+        MM_CK(cudaMemsetAsync(m.u, 0, sizeof(double) * m.h.Npad, m.stream));
+        mm_status st = run(m, solver_args(m, MODE_EVAL, 0.0, *sp));
+        if (st != MM_OK && st != MM_NONFINITE) {
+          m.opt.grid_ctas = saved;
+          m.pcg2 = saved_v;
+          solver_configure(m);
+          return st;
+        }
+        ms = m.last_launch_ms;
       }
-      ms = m.last_launch_ms;
-    }
-    if (best < 0 || ms < best_ms) {
-      best = g;
-      best_ms = ms;
+      if (best < 0 || ms < best_ms) {
+        best = g;
+        best_v = v;
+        best_ms = ms;
+      }
     }
   }
   m.opt.grid_ctas = best > 0 ? best : saved;
+  m.pcg2 = best > 0 ? best_v : saved_v;
   solver_configure(m);
   MM_CK(cudaMemcpyAsync(m.u, u0.data(), sizeof(double) * m.h.Npad, cudaMemcpyHostToDevice, m.stream));
   MM_CK(cudaMemcpyAsync(m.gf, gf0.data(), sizeof(double) * 3 * m.h.Npad, cudaMemcpyHostToDevice, m.stream));
   MM_CK(cudaStreamSynchronize(m.stream));
   {
     std::lock_guard<std::mutex> lk(g_tune_mu);
-    g_tune_cache[key] = m.grid;
+    g_tune_cache[key] = std::make_pair(m.grid, m.pcg2);
   }
   if (grid_out) *grid_out = m.grid;
   return MM_OK;

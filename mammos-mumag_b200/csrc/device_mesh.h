@@ -74,6 +74,7 @@ struct SolveArgs {
   PcgRec32* rec32[2];
   float *pp32, *e32;    // inner search direction and correction
   double* r64;          // FP64 residual of the outer refinement
+  int pcg2;             // 1: two-sync PCG iteration (z gathered alone), 0: one-sync
   // Poisson warm start (MM_WARM_*): previous u, zero, or previous u + the learned correction
   int warm;
   int32_t nreal;        // real (non-padding) rows
@@ -143,6 +144,7 @@ struct DevMesh {
   PcgRec32* rec32[2] = {nullptr, nullptr};
   float *pp32 = nullptr, *e32 = nullptr;
   double* r64 = nullptr;
+  int pcg2 = 0;  // PCG arrangement (SolveArgs::pcg2)
   // warm start and sample recording (SolveArgs)
   int warm = 0;
   MlpDev mlp{};

@@ -457,6 +457,56 @@ __device__ __noinline__ bool learned_start_mixed(Ctx& c, const double* x, double
   return true;
 }
 
+// The same Chronopoulos-Gear iteration with two grid synchronisations per iteration
+// instead of one: an update phase (own rows: s, r, p, u and z = r/diag, stored as a plane;
+// partials r.z and r.r), a barrier, and an SpMV phase w = S z gathering only z (partial
+// w.z), then the reduction.  The iterates and partial sums are the one-sync variant's, bit
+// for bit; the gathers move one value per entry instead of four, which pays on meshes
+// large enough that the extra barrier is small next to the SpMV phase.  r, w, s, 1/diag
+// stay in the planes of rec[0]; z lives in the first plane of rec[1].
+__device__ __noinline__ bool pcg_loop2(Ctx& c, double alpha, double beta, double gamma, double atol2, int& k,
+                                       double& rr) {
+  const SolveArgs& a = c.a;
+  const int n = a.Npad;
+  PcgRec* rc = a.rec[0];
+  double* z = reinterpret_cast<double*>(a.rec[1]);
+  for (;;) {
+    if (c.sy.timing && threadIdx.x == 0) c.t_phase_start = globaltimer();
+    double pg = 0, pd = 0, pr2 = 0;
+    FOR_ROWS(c)
+    (void)w_;
+    const PcgRec q = rec_load(rc, i, n);
+    const CGNext o = cg_next(q, alpha, beta);
+    const double p = q.r * q.invd + beta * a.pp[i];
+    a.pp[i] = p;
+    a.u[i] = a.u[i] + alpha * p;
+    rec_store(rc, i, n, PcgRec{o.r, q.w, o.s, q.invd});
+    z[i] = o.z;
+    pg += o.r * o.z;
+    pr2 += o.r * o.r;
+    END_ROWS
+    CHECK(grid_barrier(c.sy));
+    FOR_ROWS(c)
+    double acc = 0;
+#pragma unroll 8
+    for (int k2 = 0; k2 < w_; ++k2) acc += c.sS[LENTRY(k2)] * z[c.scol[LENTRY(k2)]];
+    rec_store_w(rc, i, n, acc);
+    pd += acc * z[i];
+    END_ROWS
+    double v[3] = {pg, pd, pr2};
+    if (c.sy.timing && threadIdx.x == 0) c.t_pcg_phase += globaltimer() - c.t_phase_start;
+    CHECK(grid_reduce<3>(c.sy, v, 0u));
+    ++k;
+    rr = v[2];
+    if (!(rr > atol2 && k < a.max_pcg)) break;
+    const double bn = v[0] / gamma;
+    alpha = v[0] / (v[1] - bn * v[0] / alpha);
+    beta = bn;
+    gamma = v[0];
+  }
+  return true;
+}
+
 __device__ __noinline__ bool pcg_solve(Ctx& c, const double* x) {
   const SolveArgs& a = c.a;
   const double* Dk = plane(a, P_D);
@@ -528,6 +578,12 @@ __device__ __noinline__ bool pcg_solve(Ctx& c, const double* x) {
     delta = v[0];
   }
   double alpha = gamma / delta, beta = 0.0;
+  if (a.pcg2) {
+    CHECK(pcg_loop2(c, alpha, beta, gamma, atol2, k, rr));
+    c.pcg_iters += k;
+    if (recording) record_targets(c, sig);
+    return true;
+  }
   for (int it = 0;; ++it) {
     if (c.sy.timing && threadIdx.x == 0) c.t_phase_start = globaltimer();
     const PcgRec* rc = a.rec[it & 1];
@@ -581,6 +637,47 @@ __device__ __forceinline__ CGNext32 cg_next32(const PcgRec32& q, float alpha, fl
   o.r = q.r - alpha * o.s;
   o.z = o.r * q.invd;
   return o;
+}
+
+// Two-sync form of the FP32 inner iteration (pcg_loop2's arrangement): records stay in
+// rec32[0], z is a float plane in rec32[1].  Returns the inner iterations in k.
+__device__ __noinline__ bool pcg_inner2(Ctx& c, double alpha, double beta, double gamma, double inner_tol2, int& k) {
+  const SolveArgs& a = c.a;
+  PcgRec32* rc = a.rec32[0];
+  float* z = reinterpret_cast<float*>(a.rec32[1]);
+  for (;;) {
+    const float af = (float)alpha, bf = (float)beta;
+    double pg = 0, pd = 0, pr2 = 0;
+    FOR_ROWS(c)
+    (void)w_;
+    const PcgRec32 q = rc[i];
+    const CGNext32 o = cg_next32(q, af, bf);
+    const float p = q.r * q.invd + bf * a.pp32[i];
+    a.pp32[i] = p;
+    a.e32[i] = a.e32[i] + af * p;
+    rc[i] = PcgRec32{o.r, q.w, o.s, q.invd};
+    z[i] = o.z;
+    pg += (double)o.r * (double)o.z;
+    pr2 += (double)o.r * (double)o.r;
+    END_ROWS
+    CHECK(grid_barrier(c.sy));
+    FOR_ROWS(c)
+    float acc = 0.f;
+#pragma unroll 8
+    for (int k2 = 0; k2 < w_; ++k2) acc += c.sS32[LENTRY(k2)] * z[c.scol[LENTRY(k2)]];
+    rc[i].w = acc;
+    pd += (double)acc * (double)z[i];
+    END_ROWS
+    double v[3] = {pg, pd, pr2};
+    CHECK(grid_reduce<3>(c.sy, v, 0u));
+    ++k;
+    if (!(v[2] > inner_tol2 && k < a.max_pcg)) break;
+    const double bn = v[0] / gamma;
+    alpha = v[0] / (v[1] - bn * v[0] / alpha);
+    beta = bn;
+    gamma = v[0];
+  }
+  return true;
 }
 
 __device__ __noinline__ bool pcg_solve_mixed(Ctx& c, const double* x) {
@@ -652,6 +749,9 @@ __device__ __noinline__ bool pcg_solve_mixed(Ctx& c, const double* x) {
       delta = v[0];
     }
     double alpha = gamma / delta, beta = 0.0;
+    if (a.pcg2) {
+      CHECK(pcg_inner2(c, alpha, beta, gamma, inner_tol2, k));
+    } else {
     for (int it = 0;; ++it) {
       const PcgRec32* rc = a.rec32[it & 1];
       PcgRec32* rn = a.rec32[(it & 1) ^ 1];
@@ -682,6 +782,7 @@ __device__ __noinline__ bool pcg_solve_mixed(Ctx& c, const double* x) {
       alpha = v[0] / (v[1] - bn * v[0] / alpha);
       beta = bn;
       gamma = v[0];
+    }
     }
     {  // u += e, r -= S e in FP64; next inner record
       double p0 = 0, p2 = 0, p3 = 0;
@@ -1399,6 +1500,7 @@ SolveArgs solver_args(const DevMesh& m, int mode, double h, const mm_solver_para
   a.pp32 = m.pp32;
   a.e32 = m.e32;
   a.r64 = m.r64;
+  a.pcg2 = m.pcg2;
   a.warm = m.warm;
   a.nreal = (int32_t)m.h.N;
   a.mlp = m.mlp;
