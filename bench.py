@@ -10,10 +10,15 @@ a 15 degree cone, a 2 nm grain-boundary phase (A=2e-12 J/m, K1=0, Js=0.5 T), fie
 tilted 1 degree toward x, +8 T -> -8 T in 0.1 T steps (161 field steps), FP64.  Inputs are
 seeded synthetic data of those shapes.
 
-``value`` is whole-job field steps/s with the mesh operators resident in HBM (device time
-from CUDA events on the library's stream), ``e2e`` the same through the public API from host
-buffers (mesh build + state upload + sweep + result read-back), ``cpu_baseline`` the CPU
-oracle on a bounded sample.  Multi-GPU runs are independent replicas (one sweep per rank,
+``value`` is whole-job field steps/s of the path the metric names -- mixed precision with
+the learned warm start (``config.path`` = learned_mixed; the plain FP64 path for the
+single-grain workload or with ``--no-learned``) -- with the mesh operators resident in HBM
+(device time from CUDA events on the library's stream); ``variants`` holds the plain FP64,
+mixed and learned+mixed sweeps of the same run with their PCG iterations per solve and
+Hc/Mr against FP64.  ``e2e`` is the headline path through the public API from host buffers
+(mesh build + state upload + sweep + result read-back), ``cpu_baseline`` the CPU oracle on
+a bounded sample.  The network of the learned warm start is trained at set-up (untimed) on
+plain loops of other seeds of the same mesh family.  Multi-GPU runs are independent replicas (one sweep per rank,
 no collective on the data path).  ``--impl reference`` times the CPU oracle alone (the
 reference's algorithm restated; its own JAX/escript stack is not installable here).
 """
@@ -99,21 +104,24 @@ def hc_mr(rows):
     return hc, mr
 
 
-def algorithmic_bytes(steps, Z: int, N: int, s: int = 8) -> float:
+def algorithmic_bytes(steps, Z: int, N: int, s: int = 8, s_pcg: int | None = None) -> float:
     """Compulsory bytes of the persistent field-step kernel, summed over its work counters.
 
-    Z = unpadded node-pair entries of the SELL pattern, N = nodes, s = value bytes.
+    Z = unpadded node-pair entries of the SELL pattern, N = nodes, s = value bytes of the
+    energy / NCG / M_inv work, s_pcg = value bytes of the Poisson PCG iterations (4 when they
+    run on FP32 planes, mixed precision; default s).
     Per Poisson PCG iteration: one S SpMV Z(s+4) + 4(N+1) + 2Ns and the fused vector
     update 9Ns.  Per energy evaluation outside the PCG: divergence + initial residual
     Z(4s+4) + 5Ns, exchange/anisotropy/gradient gathers Z(10s+4) + 14Ns, the normalised
     trial point 9Ns.  Per M_inv iteration: the C SpMV Z(7s+4) + 6Ns and ~8 three-vector
     passes 24Ns.  Per NCG iteration: ~12 three-vector passes 36Ns.
     """
+    sp = s if s_pcg is None else s_pcg
     pcg = sum(st["pcg_iters"] for st in steps)
     ev = sum(st["evals"] for st in steps)
     mi = sum(st["minv_iters"] for st in steps)
     ncg = sum(st["ncg_iters"] for st in steps)
-    b = pcg * (Z * (s + 4) + 4 * (N + 1) + 2 * N * s + 9 * N * s)
+    b = pcg * (Z * (sp + 4) + 4 * (N + 1) + 2 * N * sp + 9 * N * sp)
     b += ev * (Z * (4 * s + 4) + 5 * N * s + Z * (10 * s + 4) + 14 * N * s + 9 * N * s)
     b += mi * (Z * (7 * s + 4) + 30 * N * s)
     b += ncg * 36 * N * s
@@ -235,10 +243,21 @@ def run_reference(args, world, rank):
     return 0
 
 
+def loop_spec(name: str):
+    """The workload's mesh family and sweep as a ``learned.LoopSpec`` (training loops for the
+    learned warm start run on other seeds of the same family)."""
+    from mammos_mumag import learned
+
+    if name == "large":
+        return learned.LoopSpec(n=80, L=200.0, grains=27, cone_deg=20.0, gb=2.0, hstep=-0.05, tilt_deg=0.0,
+                                max_steps=20)
+    return learned.LoopSpec(n=32, L=80.0, grains=8, cone_deg=15.0, gb=2.0, hstep=-0.1, tilt_deg=1.0)
+
+
 def run_b200(args, world, rank, local):
     import torch
 
-    from mammos_mumag import _native
+    from mammos_mumag import _native, learned
 
     if _native.device_count() < 1:
         raise RuntimeError("no sm_100 GPU visible")
@@ -246,45 +265,98 @@ def run_b200(args, world, rank, local):
     X, T, tag, krn, m0, hdir, sweep, desc = workload(args.workload, seed=rank)
     sp = _native.solver_params(hdir=hdir)
     flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=f"cuda:{local}")
-    mesh = _native.Mesh(X, T, tag, krn, device=local)
-    mesh.set_state(m0, None, m0)
-    mesh.autotune(sp)  # launch shape (setup, untimed)
-    info = mesh.info()
     nfs_expected = int(abs(sweep["hfinal"] - sweep["hstart"]) / abs(sweep["hstep"])) + 1
     if sweep.get("max_steps"):
         nfs_expected = min(nfs_expected, sweep["max_steps"])
-
     sw = (sweep["hstart"], sweep["hfinal"], sweep["hstep"], sweep["mstep"], sweep["mfinal"])
     mx = sweep.get("max_steps", 0)
+    use_learned = args.workload != "single" and not args.no_learned
+    headline = "learned_mixed" if use_learned else "fp64"
 
-    def one_sweep(msh=None):
-        msh = msh or mesh
+    # the learned warm start's network: trained once at set-up (untimed) on plain loops of
+    # other seeds of the workload's mesh family
+    model, train_info = None, None
+    if use_learned:
+        spec = loop_spec(args.workload)
+        nseed = 2 if args.workload == "large" else 4
+        t0 = time.perf_counter()
+        feats, targets = learned.collect([1000 + 10 * rank + q for q in range(nseed)], spec, samples=50000,
+                                         device=local)
+        t1 = time.perf_counter()
+        model, loss = learned.train(feats, targets, epochs=30, device=local)
+        train_info = {"samples": int(len(targets)), "training_meshes": nseed, "collect_s": t1 - t0,
+                      "train_s": time.perf_counter() - t1, "loss_rel": loss}
+
+    def make_mesh(prec, warm):
+        msh = _native.Mesh(X, T, tag, krn, device=local, precision=prec)
+        if warm == _native.WARM_LEARNED:
+            msh.set_warm_start(warm, model)
         msh.set_state(m0, None, m0)
-        return msh.loop(*sw, sp, max_steps=mx)
+        msh.autotune(sp)  # launch shape (set-up, untimed)
+        return msh
 
-    for _ in range(args.warmup):
-        one_sweep()
-    total_ms, nfs, steps_all, rows = 0.0, 0, [], None
-    dist_barrier(world)
-    torch.cuda.synchronize()
-    with ClockSampler(local) as clk:
+    def timed(msh, clk_index=None):
+        """W untimed sweeps, then K sweeps timed with CUDA events on the library's stream,
+        the L2 flushed before each.  Returns (ms over ranks, field steps, step dicts, rows)."""
+        for _ in range(args.warmup):
+            msh.set_state(m0, None, m0)
+            msh.loop(*sw, sp, max_steps=mx)
+        total_ms, nfs, steps_all, rows = 0.0, 0, [], None
+        dist_barrier(world)
+        torch.cuda.synchronize()
         for _ in range(args.steps):
             flush.fill_(1.0)  # L2 flush between timed sweeps (256 MB > 126 MB L2)
             torch.cuda.synchronize()
-            mesh.set_state(m0, None, m0)
-            mesh.timer_start()
-            rows, steps = mesh.loop(*sw, sp, max_steps=mx)
-            total_ms += mesh.timer_stop()
+            msh.set_state(m0, None, m0)
+            msh.timer_start()
+            rows, steps = msh.loop(*sw, sp, max_steps=mx)
+            total_ms += msh.timer_stop()
             nfs += len(rows)
             steps_all += steps
-    torch.cuda.synchronize()
-    dist_barrier(world)
-    t_max = dist_max(total_ms, world)
-    value = nfs * world / (t_max * 1e-3)
-    launches = sum(1 for _ in steps_all)
+        torch.cuda.synchronize()
+        dist_barrier(world)
+        return dist_max(total_ms, world), nfs, steps_all, rows
+
+    configs = {"fp64": (_native.PREC_FP64, _native.WARM_PREVIOUS)}
+    if not args.no_mixed:
+        configs["mixed"] = (_native.PREC_MIXED, _native.WARM_PREVIOUS)
+    if use_learned:
+        configs["learned_mixed"] = (_native.PREC_MIXED, _native.WARM_LEARNED)
+    variants, raw = {}, {}
+    clk = None
+    for name, (prec, warm) in configs.items():
+        msh = make_mesh(prec, warm)
+        info = msh.info()
+        if name == headline:
+            with ClockSampler(local) as clk:
+                res = timed(msh)
+        else:
+            res = timed(msh)
+        msh.close()
+        t_ms, nfs, st, rows = res
+        evals = sum(x["evals"] for x in st)
+        hc, mr = hc_mr(rows)
+        raw[name] = (t_ms, nfs, st, rows, info)
+        variants[name] = {"value": nfs * world / (t_ms * 1e-3),
+                          "pcg_iters_per_solve": sum(x["pcg_iters"] for x in st) / max(1, evals),
+                          "hc_T": hc, "mr_T": mr, "grid_ctas": info["grid_ctas"], "pcg_variant": info["pcg_variant"]}
+    ref = variants["fp64"]
+    for name, v in variants.items():
+        if name == "fp64":
+            continue
+        v["speedup_vs_fp64"] = v["value"] / ref["value"]
+        v["pcg_per_solve_vs_fp64"] = v["pcg_iters_per_solve"] / ref["pcg_iters_per_solve"]
+        v["dHc_rel"] = (abs(v["hc_T"] - ref["hc_T"]) / ref["hc_T"]
+                        if np.isfinite(ref["hc_T"]) and np.isfinite(v["hc_T"]) else None)
+        v["dMr_rel"] = (abs(v["mr_T"] - ref["mr_T"]) / abs(ref["mr_T"])
+                        if np.isfinite(ref["mr_T"]) and np.isfinite(v["mr_T"]) else None)
+    t_max, nfs, steps_all, rows, info = raw[headline]
+    value = variants[headline]["value"]
+    launches = len(steps_all)
     kernel_ms = sum(st["device_ms"] for st in steps_all)
     Z, N = info["nnz"], info["nodes"]
-    ab = algorithmic_bytes(steps_all, Z, N)
+    s_pcg = 4 if headline != "fp64" else 8
+    ab = algorithmic_bytes(steps_all, Z, N, s_pcg=s_pcg)
     achieved = ab / (kernel_ms * 1e-3) / 1e9  # GB/s over the kernel's own launch durations
     peaks = {}
     try:
@@ -292,38 +364,9 @@ def run_b200(args, world, rank, local):
     except Exception:
         pass
     peak = float(peaks.get("hbm_gbs", 6650.0))
-    evals = sum(st["evals"] for st in steps_all)
-    pcg = sum(st["pcg_iters"] for st in steps_all)
-    hc, mr = hc_mr(rows)
-    variants = {"fp64": {"value": value, "pcg_iters_per_solve": pcg / evals, "hc_T": hc, "mr_T": mr}}
-    if not args.no_mixed:
-        with _native.Mesh(X, T, tag, krn, device=local, precision=_native.PREC_MIXED) as mm:
-            mm.set_state(m0, None, m0)
-            mm.autotune(sp)
-            for _ in range(max(1, args.warmup)):
-                one_sweep(mm)
-            t_mx, n_mx, st_mx, rows_mx = 0.0, 0, [], None
-            for _ in range(args.steps):
-                flush.fill_(1.0)
-                torch.cuda.synchronize()
-                mm.set_state(m0, None, m0)
-                mm.timer_start()
-                rows_mx, stp = mm.loop(*sw, sp, max_steps=mx)
-                t_mx += mm.timer_stop()
-                n_mx += len(rows_mx)
-                st_mx += stp
-        t_mx = dist_max(t_mx, world)
-        hc2, mr2 = hc_mr(rows_mx)
-        variants["mixed"] = {
-            "value": n_mx * world / (t_mx * 1e-3),
-            "pcg_iters_per_solve": sum(x["pcg_iters"] for x in st_mx) / max(1, sum(x["evals"] for x in st_mx)),
-            "hc_T": hc2, "mr_T": mr2,
-            "dHc_rel": abs(hc2 - hc) / hc if np.isfinite(hc) and np.isfinite(hc2) else None,
-            "dMr_rel": abs(mr2 - mr) / abs(mr) if np.isfinite(mr) and np.isfinite(mr2) else None,
-            "speedup_vs_fp64": (n_mx / t_mx) / (nfs / total_ms),
-        }
+    prec_h, warm_h = configs[headline]
     # e2e: the public API from host buffers (pinned), every step: mesh build + upload,
-    # state upload, sweep, result read-back
+    # warm-start set-up, state upload, sweep, result read-back
     pin = {k: torch.from_numpy(np.ascontiguousarray(v)).pin_memory() for k, v in
            (("X", X), ("T", np.asarray(T, np.int32)), ("tag", np.asarray(tag, np.int32)), ("m0", m0))}
     h2d = sum(t.numel() * t.element_size() for t in pin.values()) + 48 * len(krn)
@@ -331,7 +374,10 @@ def run_b200(args, world, rank, local):
     for _ in range(args.steps):
         torch.cuda.synchronize()
         t0 = time.perf_counter()
-        with _native.Mesh(pin["X"].numpy(), pin["T"].numpy(), pin["tag"].numpy(), krn, device=local) as mm:
+        with _native.Mesh(pin["X"].numpy(), pin["T"].numpy(), pin["tag"].numpy(), krn, device=local,
+                          precision=prec_h) as mm:
+            if warm_h == _native.WARM_LEARNED:
+                mm.set_warm_start(warm_h, model)
             mm.set_state(pin["m0"].numpy(), None, pin["m0"].numpy())
             mm.autotune(sp)  # cached for this mesh shape: no timing runs after the first
             r2, _ = mm.loop(*sw, sp, max_steps=mx)
@@ -340,39 +386,48 @@ def run_b200(args, world, rank, local):
         e2e_n += len(r2)
     d2h = 32 * nfs_expected + mfin.nbytes
     e2e_t = dist_max(e2e_t, world)
-    line = None
     if rank == 0:
         cpu = None
         if world == 1 and args.workload != "large":
             v, dt, n = cpu_sample(args.workload, 12)
             cpu = {"value": v, "unit": UNIT, "cores": 1, "kind": "port",
                    "sample": f"first {n} field steps of the sweep ({dt:.1f} s), NumPy/SciPy oracle, single thread"}
+        evals = sum(st["evals"] for st in steps_all)
+        pcg = sum(st["pcg_iters"] for st in steps_all)
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": t_max / args.steps, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": desc, "precision": "fp64", "parallelism": f"replicas x{world}",
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64" if headline == "fp64" else "f32+f64",
+            "data": "synthetic",
+            "config": {"workload": desc, "path": headline,
+                       "precision": "fp64" if prec_h == _native.PREC_FP64 else
+                       "mixed (FP32 operator planes and inner PCG, FP64 refinement, reductions, energies)",
+                       "warm_start": "learned" if warm_h == _native.WARM_LEARNED else "previous u (reference)",
+                       "parallelism": f"replicas x{world}",
                        "l2": "256 MB buffer written between timed sweeps (L2 flush)",
-                       "grid_ctas": info["grid_ctas"], "block_threads": info["block_threads"]},
-            "pcg_iters_per_solve": pcg / evals,
+                       "grid_ctas": info["grid_ctas"], "block_threads": info["block_threads"],
+                       "pcg_variant": info["pcg_variant"]},
+            "pcg_iters_per_solve": pcg / max(1, evals),
             "variants": variants,
+            "learned_training": train_info,
             "field_steps_per_sweep": nfs // args.steps,
-            "hc_T": hc, "mr_T": mr,
+            "hc_T": variants[headline]["hc_T"], "mr_T": variants[headline]["mr_T"],
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": None,
-                         "kernel": "k_solve (persistent field step)",
+                         "kernel": f"k_solve (persistent field step, {headline})",
                          "algorithmic_bytes_per_launch": ab / launches,
                          "avg_launch_ms": kernel_ms / launches,
-                         "peak_source": "MEASURED_PEAKS.json hbm_gbs" if peaks else "fallback"},
+                         "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)" if peaks else "fallback"},
             "sync_fraction": sum(st["sync_ns"] for st in steps_all) / max(1, sum(st["kernel_ns"] for st in steps_all)),
             "cpu_baseline": cpu,
             "e2e": {"value": e2e_n * world / e2e_t, "unit": UNIT, "h2d_bytes_per_step": int(h2d),
                     "d2h_bytes_per_step": int(d2h)},
             "gpu_launches": launches,
-            "clocks": clk.summary(),
+            "clocks": clk.summary() if clk is not None else None,
         }
         print(json.dumps(line), flush=True)
-    mesh.close()
+    if model is not None:
+        model.close()
     return 0
 
 
@@ -384,6 +439,8 @@ def main():
     ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
     ap.add_argument("--workload", choices=["multigrain", "single", "large"], default="multigrain")
     ap.add_argument("--no-mixed", action="store_true", help="skip the mixed-precision variant")
+    ap.add_argument("--no-learned", action="store_true",
+                    help="skip the learned warm start (headline = the plain FP64 path)")
     args = ap.parse_args()
     world, rank, local = dist_setup()
     try:

@@ -61,6 +61,8 @@ typedef struct {
                           1 = one grid synchronisation per iteration (neighbour z recomputed
                           from gathered r, w, s), 2 = two (z stored, gathered alone); both
                           give the same iterates */
+  int ctas_per_sm;     /* build of the persistent kernel: 0 = chosen by mm_autotune (2 until
+                          then), 2 or 3 resident CTAs per SM (128 or 80 registers per thread) */
 } mm_options;
 
 /* Solver settings of one field step (scripts/tools.py:64-120, scripts/minimizers.py:140-190). */
@@ -103,7 +105,8 @@ typedef struct {
   double volume;                       /* magnetic volume V, nm^3 */
   double bandwidth_before, bandwidth_after;  /* max |i-j| over node pairs, file vs device order */
   int32_t pcg_variant;                 /* PCG arrangement in use: 1 one-sync, 2 two-sync */
-  int32_t reserved_;
+  int32_t kernel_ctas_per_sm;          /* build of the persistent kernel in use: 2 or 3 resident
+                                          CTAs per SM (128 or 80 registers per thread) */
 } mm_mesh_info;
 
 /* Field-sweep parameters (the .p2 [field] section; scripts/loop.py:71-142). */
@@ -203,8 +206,9 @@ mm_status mm_loop(mm_mesh* mesh, const mm_loop_params* lp, const mm_solver_param
                   void* user);
 
 /* Autotune the persistent launch shape of this mesh (no counterpart in the reference): times
- * a cold Poisson solve + energy evaluation at the current state for a few CTA counts (one
- * per SM, two per SM, in between), each with both PCG arrangements unless
+ * a cold Poisson solve + energy evaluation at the current state for a few launch shapes --
+ * the kernel built for two resident CTAs per SM at one, one and a half and two CTAs per SM,
+ * the build for three at two and three per SM -- each with both PCG arrangements unless
  * options.pcg_variant fixes one, and keeps the fastest; u and the full gradient are
  * restored.  Results are cached per mesh shape, precision and pcg_variant option for the
  * process.  *grid_out (may be NULL) receives the CTA count chosen. */

@@ -201,6 +201,7 @@ void mm_default_options(mm_options* opt) {
   opt->block_threads = 0;
   opt->reorder = 1;
   opt->pcg_variant = 0;
+  opt->ctas_per_sm = 0;
 }
 
 void mm_default_solver_params(mm_solver_params* sp) {
@@ -261,6 +262,8 @@ mm_status mm_mesh_create(const double* X, int64_t N, const int32_t* T, const int
   if (opt) o = *opt;
   if (!(o.size > 0)) throw std::runtime_error("options.size must be positive");
   if (o.pcg_variant < 0 || o.pcg_variant > 2) throw std::runtime_error("options.pcg_variant must be 0, 1 or 2");
+  if (o.ctas_per_sm != 0 && o.ctas_per_sm != 2 && o.ctas_per_sm != 3)
+    throw std::runtime_error("options.ctas_per_sm must be 0, 2 or 3");
   for (int64_t i = 0; i < 3 * N; ++i)
     if (!std::isfinite(X[i])) throw std::runtime_error("non-finite node coordinate");
   int ndev = 0;
@@ -279,6 +282,7 @@ mm_status mm_mesh_create(const double* X, int64_t N, const int32_t* T, const int
   preprocess(X, N, T, tag, E, nmats, o.reorder != 0, m.h);
   // PCG arrangement: fixed by the caller, else by size until mm_autotune times both
   m.pcg2 = o.pcg_variant == 2 ? 1 : o.pcg_variant == 1 ? 0 : (m.h.N >= kPcg2Nodes ? 1 : 0);
+  m.kernel_mb = o.ctas_per_sm == 3 ? 3 : 2;
   HostMesh& h = m.h;
   m.ncolours = (int32_t)h.colour_off.size() - 1;
   // materials, scripts/materials.py:17-35
@@ -409,7 +413,7 @@ mm_status mm_mesh_get_info(const mm_mesh* mesh, mm_mesh_info* info) {
   info->bandwidth_before = (double)m.h.bandwidth_before;
   info->bandwidth_after = (double)m.h.bandwidth_after;
   info->pcg_variant = m.pcg2 ? 2 : 1;
-  info->reserved_ = 0;
+  info->kernel_ctas_per_sm = m.kernel_mb;
   return MM_OK;
   API_END
 }
@@ -869,7 +873,7 @@ mm_status mm_batch_timer_stop(mm_batch* batch, double* elapsed_ms) {
 namespace {
 // Launch shapes already chosen for meshes of the same shape and precision (process-wide).
 std::mutex g_tune_mu;
-std::map<std::tuple<int64_t, int64_t, int, int, int>, std::pair<int, int>> g_tune_cache;
+std::map<std::tuple<int64_t, int64_t, int, int, int>, std::tuple<int, int, int>> g_tune_cache;
 }  // namespace
 
 mm_status mm_autotune(mm_mesh* mesh, const mm_solver_params* sp, int32_t* grid_out) {
@@ -880,26 +884,38 @@ mm_status mm_autotune(mm_mesh* mesh, const mm_solver_params* sp, int32_t* grid_o
   MM_CK(cudaSetDevice(m.device));
   cudaDeviceProp prop;
   MM_CK(cudaGetDeviceProperties(&prop, m.device));
-  const auto key = std::make_tuple(m.h.nslices, m.h.nent, m.vals32 ? 1 : 0, m.device, m.opt.pcg_variant);
+  const auto key = std::make_tuple(m.h.nslices, m.h.nent, m.vals32 ? 1 : 0, m.device, m.opt.pcg_variant * 4 + m.opt.ctas_per_sm);
   {
     std::lock_guard<std::mutex> lk(g_tune_mu);
     auto it = g_tune_cache.find(key);
     if (it != g_tune_cache.end()) {
-      m.opt.grid_ctas = it->second.first;
-      m.pcg2 = it->second.second;
+      m.opt.grid_ctas = std::get<0>(it->second);
+      m.pcg2 = std::get<1>(it->second);
+      m.kernel_mb = std::get<2>(it->second);
       solver_configure(m);
       if (grid_out) *grid_out = m.grid;
       return MM_OK;
     }
   }
-  // candidates: one CTA per SM (or one slice per warp), two per SM, and in between; each
-  // with both PCG arrangements unless the options fix one
+  // candidates (kernel build, CTAs): the two-CTA-per-SM build with one CTA per SM (or one
+  // slice per warp), one and a half and two per SM; the three-CTA build with two and three
+  // per SM; each with both PCG arrangements unless the options fix one
   const int64_t ns = m.h.nslices;
   const int sms = prop.multiProcessorCount;
-  std::vector<int> cand;
-  for (int g : {(int)std::min<int64_t>(sms, (ns + 7) / 8), (int)std::min<int64_t>(2 * sms, (ns + 3) / 4),
-                (int)std::min<int64_t>(3 * sms / 2, (ns + 5) / 6)})
-    if (g >= 1 && std::find(cand.begin(), cand.end(), g) == cand.end()) cand.push_back(g);
+  std::vector<std::pair<int, int>> cand;
+  auto add = [&](int mb, int64_t g, int64_t per) {
+    const int gg = (int)std::min<int64_t>(g, (ns + per - 1) / per);
+    if (gg >= 1 && std::find(cand.begin(), cand.end(), std::make_pair(mb, gg)) == cand.end()) cand.emplace_back(mb, gg);
+  };
+  if (m.opt.ctas_per_sm != 3) {
+    add(2, sms, 8);
+    add(2, 3 * sms / 2, 6);
+    add(2, 2 * sms, 4);
+  }
+  if (m.opt.ctas_per_sm != 2) {
+    add(3, 2 * sms, 4);
+    add(3, 3 * sms, 3);
+  }
   std::vector<int> variants;
   if (m.opt.pcg_variant == 1)
     variants = {0};
@@ -911,11 +927,12 @@ mm_status mm_autotune(mm_mesh* mesh, const mm_solver_params* sp, int32_t* grid_o
   std::vector<double> u0, gf0;
   d2h(u0, m.u, m.h.Npad, m.stream);
   d2h(gf0, m.gf, 3 * m.h.Npad, m.stream);
-  int best = -1, best_v = m.pcg2;
+  int best = -1, best_v = m.pcg2, best_mb = m.kernel_mb;
   float best_ms = 0.f;
-  const int saved = m.opt.grid_ctas, saved_v = m.pcg2;
-  for (int g : cand) {
+  const int saved = m.opt.grid_ctas, saved_v = m.pcg2, saved_mb = m.kernel_mb;
+  for (const auto& [mb, g] : cand) {
     m.opt.grid_ctas = g;
+    m.kernel_mb = mb;
     solver_configure(m);
     if (m.grid != g) continue;  // not resident
     for (int v : variants) {
@@ -927,6 +944,7 @@ mm_status mm_autotune(mm_mesh* mesh, const mm_solver_params* sp, int32_t* grid_o
         if (st != MM_OK && st != MM_NONFINITE) {
           m.opt.grid_ctas = saved;
           m.pcg2 = saved_v;
+          m.kernel_mb = saved_mb;
           solver_configure(m);
           return st;
         }
@@ -935,19 +953,21 @@ mm_status mm_autotune(mm_mesh* mesh, const mm_solver_params* sp, int32_t* grid_o
       if (best < 0 || ms < best_ms) {
         best = g;
         best_v = v;
+        best_mb = mb;
         best_ms = ms;
       }
     }
   }
   m.opt.grid_ctas = best > 0 ? best : saved;
   m.pcg2 = best > 0 ? best_v : saved_v;
+  m.kernel_mb = best > 0 ? best_mb : saved_mb;
   solver_configure(m);
   MM_CK(cudaMemcpyAsync(m.u, u0.data(), sizeof(double) * m.h.Npad, cudaMemcpyHostToDevice, m.stream));
   MM_CK(cudaMemcpyAsync(m.gf, gf0.data(), sizeof(double) * 3 * m.h.Npad, cudaMemcpyHostToDevice, m.stream));
   MM_CK(cudaStreamSynchronize(m.stream));
   {
     std::lock_guard<std::mutex> lk(g_tune_mu);
-    g_tune_cache[key] = std::make_pair(m.grid, m.pcg2);
+    g_tune_cache[key] = std::make_tuple(m.grid, m.pcg2, m.kernel_mb);
   }
   if (grid_out) *grid_out = m.grid;
   return MM_OK;

@@ -166,8 +166,9 @@ struct DevMesh {
   double* h_resd = nullptr;
   long long* h_resi = nullptr;
   int* h_flags = nullptr;
-  // launch shape of the persistent kernel
+  // launch shape of the persistent kernel and its build (resident CTAs per SM, 2 or 3)
   int grid = 0, block = 0;
+  int kernel_mb = 2;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;    // mm_timer_*
   cudaEvent_t evk0 = nullptr, evk1 = nullptr;  // around each persistent launch
   float last_launch_ms = 0.f;

@@ -13,7 +13,7 @@ namespace mumag {
 constexpr int kSlice = 32;      // SELL slice height = one warp, lane = row
 constexpr int kMaxRed = 8;      // values per grid reduction
 constexpr int kNumPlanes = 14;  // S, Aex, K[6], D[3], G[3]
-constexpr int kMaxGrid = 320;   // CTAs a persistent launch may use (reduction coverage)
+constexpr int kMaxGrid = 480;   // CTAs a persistent launch may use (reduction coverage)
 constexpr int64_t kPcg2Nodes = 100000;  // default to the two-sync PCG from this many nodes
 
 // Value planes of the node-pair operators, all on one SELL-32 pattern.

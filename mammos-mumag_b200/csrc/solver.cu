@@ -34,7 +34,7 @@ namespace mumag {
 namespace {
 
 constexpr unsigned kSpinLimit = 1u << 23;  // bounded wait per barrier (several seconds)
-constexpr int kMaxCtaPerLane = 10;         // a reduction warp sums up to 320 CTAs
+constexpr int kMaxCtaPerLane = 15;         // a reduction warp sums up to 480 CTAs
 
 // Grid barrier: one arrival counter (red.release), thread 0 of every CTA polls it with
 // acquire loads.  A grid reduction publishes the CTA's partials before arriving and reads
@@ -1294,7 +1294,11 @@ __device__ __forceinline__ void solve_body(const SolveArgs& args, int nblk, int 
   }
 }
 
-__global__ void __launch_bounds__(256, 2) k_solve(const __grid_constant__ SolveArgs args) {
+// The persistent kernel is built for two and for three resident CTAs per SM (128 or 80
+// registers per thread); the three-CTA build hides more memory latency on large meshes, the
+// two-CTA build spills less on small ones.  mm_autotune picks one per mesh.
+template <int MB>
+__global__ void __launch_bounds__(256, MB) k_solve(const __grid_constant__ SolveArgs args) {
   extern __shared__ __align__(16) unsigned char smem[];
   solve_body(args, gridDim.x, blockIdx.x, smem);
 }
@@ -1352,7 +1356,7 @@ void solver_configure(DevMesh& m) {
   int grid = m.opt.grid_ctas > 0 ? m.opt.grid_ctas
                                  : (int)std::min<int64_t>(prop.multiProcessorCount,
                                                           (m.h.nslices + warps - 1) / warps);
-  // explicit requests may use every resident CTA (up to 2 per SM at 128 registers)
+  // explicit requests may use every resident CTA (2 or 3 per SM, by the kernel build)
   static_assert(32 * kMaxCtaPerLane >= kMaxGrid, "reductions must cover every CTA");
   grid = std::max(1, std::min(grid, kMaxGrid));
   grid = (int)std::min<int64_t>(grid, m.h.nslices);
@@ -1364,11 +1368,16 @@ void solver_configure(DevMesh& m) {
   m.smem = sp.smem;
   // The attribute is per kernel, shared by every mesh: raise it to the device limit once
   // (occupancy follows each launch's actual request).
-  if (cudaFuncSetAttribute(k_solve, cudaFuncAttributeMaxDynamicSharedMemorySize,
+  if (cudaFuncSetAttribute(k_solve<2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)(prop.sharedMemPerBlockOptin - 16 * 1024)) != cudaSuccess ||
+      cudaFuncSetAttribute(k_solve<3>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                            (int)(prop.sharedMemPerBlockOptin - 16 * 1024)) != cudaSuccess)
     throw std::runtime_error("cannot reserve shared memory for the solver kernel");
+  if (m.kernel_mb != 2 && m.kernel_mb != 3) m.kernel_mb = 2;
   int occ = 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_solve, block, m.smem) != cudaSuccess || occ < 1)
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, m.kernel_mb == 3 ? k_solve<3> : k_solve<2>, block, m.smem) !=
+          cudaSuccess ||
+      occ < 1)
     throw std::runtime_error("persistent solver kernel cannot be resident with " + std::to_string(block) +
                              " threads per CTA");
   grid = std::min(grid, occ * prop.multiProcessorCount);
@@ -1560,7 +1569,7 @@ cudaError_t solver_launch(DevMesh& m, const SolveArgs& a) {
   cfg.attrs = attr;
   cfg.numAttrs = 1;
   if (m.evk0 && (e = cudaEventRecord(m.evk0, m.stream)) != cudaSuccess) return e;
-  e = cudaLaunchKernelEx(&cfg, k_solve, a);
+  e = m.kernel_mb == 3 ? cudaLaunchKernelEx(&cfg, k_solve<3>, a) : cudaLaunchKernelEx(&cfg, k_solve<2>, a);
   if (e != cudaSuccess) return e;
   return m.evk1 ? cudaEventRecord(m.evk1, m.stream) : cudaSuccess;
 }

@@ -91,6 +91,7 @@ class Options(C.Structure):
         ("block_threads", C.c_int),
         ("reorder", C.c_int),
         ("pcg_variant", C.c_int),
+        ("ctas_per_sm", C.c_int),
     ]
 
 
@@ -143,7 +144,7 @@ class MeshInfo(C.Structure):
         ("bandwidth_before", C.c_double),
         ("bandwidth_after", C.c_double),
         ("pcg_variant", C.c_int32),
-        ("reserved_", C.c_int32),
+        ("kernel_ctas_per_sm", C.c_int32),
     ]
 
     def as_dict(self):
@@ -339,7 +340,7 @@ class Mesh:
     """Device operators of one mesh (an ``mm_mesh`` handle)."""
 
     def __init__(self, X, T, tag, materials, size=1e-9, dirichlet_rhs=0, precision=PREC_FP64, device=0,
-                 grid_ctas=0, block_threads=0, reorder=1, pcg_variant=0):
+                 grid_ctas=0, block_threads=0, reorder=1, pcg_variant=0, ctas_per_sm=0):
         lib = load()
         self.X = np.ascontiguousarray(X, dtype=np.float64)
         self.T = np.ascontiguousarray(T, dtype=np.int32)
@@ -349,7 +350,7 @@ class Mesh:
         mats = (Material * max(1, len(rows)))(*[Material(*r) for r in rows])
         opt = default_options(size=size, dirichlet_rhs=dirichlet_rhs, precision=precision, device=device,
                               grid_ctas=grid_ctas, block_threads=block_threads, reorder=reorder,
-                              pcg_variant=pcg_variant)
+                              pcg_variant=pcg_variant, ctas_per_sm=ctas_per_sm)
         h = C.c_void_p()
         check(lib.mm_mesh_create(_dp(self.X), self.N, self.T.ctypes.data_as(_I32), self.tag.ctypes.data_as(_I32),
                                  self.E, mats, len(rows), C.byref(opt), C.byref(h)))

@@ -43,10 +43,12 @@ class LoopSpec:
     mfinal: float = -2.0
     tilt_deg: float = 1.0
     precision: int = _native.PREC_FP64
+    max_steps: int = 0  # > 0: only the first max_steps field steps
 
     @property
     def steps(self) -> int:
-        return int(abs(self.hfinal - self.hstart) / abs(self.hstep)) + 1
+        n = int(abs(self.hfinal - self.hstart) / abs(self.hstep)) + 1
+        return min(n, self.max_steps) if self.max_steps > 0 else n
 
     def hdir(self):
         t = np.radians(self.tilt_deg)
@@ -62,7 +64,8 @@ class LoopSpec:
     def run(self, M, m0, max_steps: int = 0):
         sp = _native.solver_params(hdir=self.hdir())
         M.set_state(m0, np.zeros(M.N), m0)
-        return M.loop(self.hstart, self.hfinal, self.hstep, abs(self.hstep), self.mfinal, sp, max_steps=max_steps)
+        mx = max_steps if max_steps > 0 else self.max_steps
+        return M.loop(self.hstart, self.hfinal, self.hstep, abs(self.hstep), self.mfinal, sp, max_steps=mx)
 
 
 def collect(seeds, spec: LoopSpec | None = None, samples: int = 50000, device: int = 0, rng_seed: int = 0,

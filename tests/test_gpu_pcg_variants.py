@@ -13,13 +13,15 @@ pytestmark = pytest.mark.gpu
 
 
 @pytest.mark.parametrize("precision", [_native.PREC_FP64, _native.PREC_MIXED])
-def test_pcg_arrangements_agree(precision):
+@pytest.mark.parametrize("ctas_per_sm", [2, 3])
+def test_pcg_arrangements_agree(precision, ctas_per_sm):
     X, T, tag, krn, m0 = synthetic.multigrain(n=12, L=20.0, grains=3, cone_deg=20.0, gb=2.0, seed=11)
     sp = _native.solver_params(hdir=[0.0, 0.0, 1.0])
     out = {}
     for variant in (1, 2):
-        with _native.Mesh(X, T, tag, krn, precision=precision, pcg_variant=variant) as M:
-            assert M.info()["pcg_variant"] == variant
+        with _native.Mesh(X, T, tag, krn, precision=precision, pcg_variant=variant, ctas_per_sm=ctas_per_sm,
+                          grid_ctas=24) as M:
+            assert M.info()["pcg_variant"] == variant and M.info()["kernel_ctas_per_sm"] == ctas_per_sm
             M.set_state(m0, None, m0)
             E, g, it = M.energy_grad(0.5, sp)
             r1 = M.minimize(-1.0, sp)
@@ -33,9 +35,26 @@ def test_pcg_arrangements_agree(precision):
     assert a[3]["energy"] == pytest.approx(b[3]["energy"], rel=1e-12)
 
 
+def test_kernel_builds_agree():
+    """The two- and three-CTA-per-SM builds of the persistent kernel, on the same launch
+    shape, give the same field step."""
+    X, T, tag, krn, m0 = synthetic.multigrain(n=12, L=20.0, grains=3, cone_deg=20.0, gb=2.0, seed=13)
+    sp = _native.solver_params(hdir=[0.0, 0.0, 1.0])
+    res = {}
+    for mb in (2, 3):
+        with _native.Mesh(X, T, tag, krn, ctas_per_sm=mb, grid_ctas=30) as M:
+            M.set_state(m0, None, m0)
+            r = M.minimize(-1.0, sp)
+            res[mb] = (r, M.get_state()[0])
+    (ra, ma), (rb, mb_) = res[2], res[3]
+    assert ra["pcg_iters"] == rb["pcg_iters"] and ra["ncg_iters"] == rb["ncg_iters"]
+    assert ra["energy"] == pytest.approx(rb["energy"], rel=1e-12)
+    assert np.abs(ma - mb_).max() < 1e-10
+
+
 def test_autotune_reports_a_variant():
     X, T, tag, krn, m0 = synthetic.multigrain(n=10, L=15.0, grains=2, cone_deg=20.0, gb=2.0, seed=12)
     with _native.Mesh(X, T, tag, krn) as M:
         M.set_state(m0, None, m0)
         M.autotune(_native.solver_params(hdir=[0.0, 0.0, 1.0]))
-        assert M.info()["pcg_variant"] in (1, 2)
+        assert M.info()["pcg_variant"] in (1, 2) and M.info()["kernel_ctas_per_sm"] in (2, 3)
