@@ -1,7 +1,7 @@
 """Benchmark of the hysteresis hot path: field steps per second on the B200 path.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
-                    [--workload multigrain|single]
+                    [--workload multigrain|single|large|batch]
 
 A step is one full field sweep of the workload (the reference's loop, scripts/loop.py:71-142,
 run to the last field value).  The default workload is the multigrain cube: 80 nm edge,
@@ -45,6 +45,14 @@ import numpy as np  # noqa: E402
 METRIC = "field steps/s + PCG iters/solve: learned+mixed vs plain FP64 GPU at |ΔHc|<1%"
 UNIT = "field steps/s"
 L2_FLUSH_BYTES = 256 << 20
+# DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) per algorithmic byte of one
+# k_solve field-step launch of the multigrain workload, from one ncu --set full capture of
+# each path (python -m mammos_mumag.perfcase field-step ...): the FP64 launch moved
+# 124.3 MB for 5,422 MB of algorithmic bytes, the learned+mixed launch 579.2 MB for
+# 4,146 MB.  The bench scales the ratio to its own average launch (traffic grows with the
+# work counters the algorithmic bytes are computed from).
+TRAFFIC_PER_ALGORITHMIC_BYTE = {("multigrain", "fp64"): 124.3 / 5422.4,
+                                ("multigrain", "learned_mixed"): 579.2 / 4145.9}
 
 
 def batch_workload(count: int = 64, seed: int = 0):
@@ -254,6 +262,88 @@ def loop_spec(name: str):
     return learned.LoopSpec(n=32, L=80.0, grains=8, cone_deg=15.0, gb=2.0, hstep=-0.1, tilt_deg=1.0)
 
 
+def run_batch(args, world, rank, local):
+    """The batched workload: 64 independent loops on seeded meshes of uneven size, stepped in
+    lockstep field steps, all 64 meshes in ONE persistent launch per field step (mm_batch_loop).
+    Beside it, the same loops run one after another with their own autotuned launches."""
+    import torch
+
+    from mammos_mumag import _native
+
+    torch.cuda.set_device(local)
+    data = batch_workload(64, seed=rank)
+    sp = _native.solver_params(hdir=[0.0, 0.0, 1.0])
+    sw = (8.0, -8.0, -0.2, 0.4, -2.0)
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=f"cuda:{local}")
+    variants, clk = {}, None
+    for name, prec in (("fp64", _native.PREC_FP64), ("mixed", _native.PREC_MIXED)):
+        meshes = [_native.Mesh(X, T, tag, krn, device=local, precision=prec) for X, T, tag, krn, _ in data]
+        try:
+            def reset():
+                for M, d in zip(meshes, data):
+                    M.set_state(d[4], None, d[4])
+
+            with _native.Batch(meshes) as B:
+                for _ in range(args.warmup):
+                    reset()
+                    B.loop(*sw, sp)
+                t_ms, nfs, pcg, ev = 0.0, 0, 0, 0
+                dist_barrier(world)
+                with ClockSampler(local) as c:
+                    for _ in range(args.steps):
+                        flush.fill_(1.0)
+                        torch.cuda.synchronize()
+                        reset()
+                        B.timer_start()
+                        out = B.loop(*sw, sp)
+                        t_ms += B.timer_stop()
+                        for rows, st in out:
+                            nfs += len(rows)
+                            pcg += sum(x["pcg_iters"] for x in st)
+                            ev += sum(x["evals"] for x in st)
+                if name == "fp64":
+                    clk = c
+                groups = B.groups()
+            t_ms = dist_max(t_ms, world)
+            variants[name] = {"value": nfs * world / (t_ms * 1e-3), "pcg_iters_per_solve": pcg / max(1, ev),
+                              "ms_per_sweep": t_ms / args.steps, "ctas": int(groups[-1])}
+            # the same loops one after another, each with its own autotuned launch shape
+            seq_ms, seq_n = 0.0, 0
+            for M, d in zip(meshes, data):
+                M.set_state(d[4], None, d[4])
+                M.autotune(sp)
+                M.set_state(d[4], None, d[4])
+                M.loop(*sw, sp)  # warm-up
+                M.set_state(d[4], None, d[4])
+                M.timer_start()
+                rows, _ = M.loop(*sw, sp)
+                seq_ms += M.timer_stop()
+                seq_n += len(rows)
+            seq_ms = dist_max(seq_ms, world)
+            variants[name + "_sequential"] = {"value": seq_n * world / (seq_ms * 1e-3), "ms_per_sweep": seq_ms}
+        finally:
+            for M in meshes:
+                M.close()
+    if rank == 0:
+        nodes = [d[0].shape[0] for d in data]
+        line = {
+            "metric": "field steps/s (sum over the batch's loops)", "value": variants["fp64"]["value"],
+            "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": variants["fp64"]["ms_per_sweep"], "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": ("64 independent loops, seeded structured meshes of 12..40 cells per edge "
+                                    f"(h = 1.25 nm, {min(nodes)}..{max(nodes)} nodes), 1..27 Voronoi grains, cone "
+                                    "<= 30 deg, +8 -> -8 T in 0.2 T lockstep steps (81), one persistent launch per "
+                                    "lockstep field step"),
+                       "parallelism": f"replicas x{world}", "l2": "256 MB buffer written between timed sweeps"},
+            "variants": variants,
+            "gpu_launches": 81 * args.steps,
+            "clocks": clk.summary() if clk is not None else None,
+        }
+        print(json.dumps(line), flush=True)
+    return 0
+
+
 def run_b200(args, world, rank, local):
     import torch
 
@@ -364,6 +454,8 @@ def run_b200(args, world, rank, local):
     except Exception:
         pass
     peak = float(peaks.get("hbm_gbs", 6650.0))
+    ratio = TRAFFIC_PER_ALGORITHMIC_BYTE.get((args.workload, headline))
+    traffic = ratio * ab / launches if ratio is not None else None
     prec_h, warm_h = configs[headline]
     # e2e: the public API from host buffers (pinned), every step: mesh build + upload,
     # warm-start set-up, state upload, sweep, result read-back
@@ -413,7 +505,10 @@ def run_b200(args, world, rank, local):
             "field_steps_per_sweep": nfs // args.steps,
             "hc_T": variants[headline]["hc_T"], "mr_T": variants[headline]["mr_T"],
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                         "frac": achieved / peak, "traffic": None,
+                         "frac": achieved / peak, "traffic": traffic,
+                         "traffic_source": ("DRAM bytes per algorithmic byte of one ncu-captured field-step "
+                                            "launch of this path, scaled to the average launch")
+                         if traffic is not None else None,
                          "kernel": f"k_solve (persistent field step, {headline})",
                          "algorithmic_bytes_per_launch": ab / launches,
                          "avg_launch_ms": kernel_ms / launches,
@@ -437,7 +532,7 @@ def main():
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
-    ap.add_argument("--workload", choices=["multigrain", "single", "large"], default="multigrain")
+    ap.add_argument("--workload", choices=["multigrain", "single", "large", "batch"], default="multigrain")
     ap.add_argument("--no-mixed", action="store_true", help="skip the mixed-precision variant")
     ap.add_argument("--no-learned", action="store_true",
                     help="skip the learned warm start (headline = the plain FP64 path)")
@@ -446,6 +541,8 @@ def main():
     try:
         if args.impl == "reference":
             return run_reference(args, world, rank)
+        if args.workload == "batch":
+            return run_batch(args, world, rank, local)
         return run_b200(args, world, rank, local)
     finally:
         if world > 1:

@@ -311,6 +311,16 @@ mm_status mm_mesh_record_samples(mm_mesh* mesh, int64_t capacity, int32_t stride
 mm_status mm_mesh_read_samples(mm_mesh* mesh, float* feats, float* target, int32_t* node, int64_t cap,
                                int64_t* count);
 
+/* ---- failure path test hook ----------------------------------------------------------------
+ *
+ * Every wait of the persistent kernel is bounded: a grid barrier that has not seen all CTAs
+ * arrive after its spin limit (about two seconds) records MM_TIMEOUT, raises the abort flag
+ * that releases the other CTAs, and the kernel returns; the call then returns MM_TIMEOUT and
+ * the mesh stays usable.  This hook makes that happen on purpose, without a fault: with
+ * stall > 0 every barrier of the mesh's later launches waits for `stall` arrivals that never
+ * come.  stall = 0 restores normal operation.  For tests of the failure path only. */
+mm_status mm_debug_stall_barriers(mm_mesh* mesh, int32_t stall);
+
 /* ---- allocation-free Poisson solve ------------------------------------------------------
  *
  * No counterpart in the reference: an extra entry point of this library for callers that

@@ -983,6 +983,15 @@ MlpDev model_view(const mm_model* m);
 
 extern "C" {
 
+mm_status mm_debug_stall_barriers(mm_mesh* mesh, int32_t stall) {
+  API_BEGIN
+  check_mesh(mesh);
+  if (stall < 0 || stall > 1024) throw std::runtime_error("stall must be in [0, 1024]");
+  mesh->dm.bar_stall = stall;
+  return MM_OK;
+  API_END
+}
+
 mm_status mm_mesh_set_warm_start(mm_mesh* mesh, int32_t mode, const mm_model* model) {
   API_BEGIN
   check_mesh(mesh);

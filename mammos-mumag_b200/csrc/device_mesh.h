@@ -95,6 +95,7 @@ struct SolveArgs {
   unsigned rec_seed;
   // grid synchronisation
   unsigned long long* bar;    // barrier arrival counter, zeroed before each launch
+  int bar_stall;              // test hook: extra arrivals each barrier waits for (0 = normal)
   double* red;                // [2][kMaxRed][gridDim.x] reduction partials
   int* flags;                 // [0] abort, [1] status
   int stage;                  // 1: the CTA's SELL columns + Poisson values live in shared memory
@@ -145,6 +146,7 @@ struct DevMesh {
   float *pp32 = nullptr, *e32 = nullptr;
   double* r64 = nullptr;
   int pcg2 = 0;  // PCG arrangement (SolveArgs::pcg2)
+  int bar_stall = 0;  // test hook (SolveArgs::bar_stall)
   // warm start and sample recording (SolveArgs)
   int warm = 0;
   MlpDev mlp{};

@@ -47,6 +47,7 @@ struct Sync {
   int* flags;
   unsigned long long epoch;
   int nblk, blk, slot;
+  int stall;  // extra arrivals every barrier waits for (test hook: 1 = none ever come)
   unsigned long long t_sync;  // ns spent in grid synchronisation (thread 0)
   unsigned long long t_pre, t_bar, t_post;  // phase timers (thread 0): see SolveArgs::prof
   bool timing;                              // read %globaltimer only when profiling
@@ -73,7 +74,7 @@ __device__ __noinline__ bool grid_barrier(Sync& s) {
   __syncthreads();
   if (threadIdx.x == 0) {
     s.epoch += 1;
-    const unsigned long long target = s.epoch * (unsigned long long)s.nblk;
+    const unsigned long long target = s.epoch * (unsigned long long)s.nblk + (unsigned long long)s.stall;
     __threadfence();
     red_release_add_u64(s.bar, 1ull);
     int ab = 0;
@@ -1220,6 +1221,7 @@ __device__ __forceinline__ void solve_body(const SolveArgs& args, int nblk, int 
   c.sy.nblk = nblk;
   c.sy.blk = blk;
   c.sy.slot = 0;
+  c.sy.stall = args.bar_stall;
   c.sy.t_sync = 0;
   c.sy.t_pre = c.sy.t_bar = c.sy.t_post = 0;
   c.sy.timing = args.prof != nullptr;
@@ -1510,6 +1512,7 @@ SolveArgs solver_args(const DevMesh& m, int mode, double h, const mm_solver_para
   a.e32 = m.e32;
   a.r64 = m.r64;
   a.pcg2 = m.pcg2;
+  a.bar_stall = m.bar_stall;
   a.warm = m.warm;
   a.nreal = (int32_t)m.h.N;
   a.mlp = m.mlp;

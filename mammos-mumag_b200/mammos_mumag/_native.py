@@ -72,6 +72,7 @@ EXPORTED = (
     "mm_mesh_set_warm_start",
     "mm_mesh_record_samples",
     "mm_mesh_read_samples",
+    "mm_debug_stall_barriers",
 )
 WARM_PREVIOUS, WARM_ZERO, WARM_LEARNED = 0, 1, 2
 MLP_FEATURES = 16
@@ -247,6 +248,7 @@ def load():
         "mm_mesh_set_warm_start": (C.c_int, [C.c_void_p, C.c_int32, C.c_void_p]),
         "mm_mesh_record_samples": (C.c_int, [C.c_void_p, C.c_int64, C.c_int32, C.c_uint64]),
         "mm_mesh_read_samples": (C.c_int, [C.c_void_p, _F, _F, _I32, C.c_int64, _I64]),
+        "mm_debug_stall_barriers": (C.c_int, [C.c_void_p, C.c_int32]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -393,6 +395,12 @@ class Mesh:
         check(load().mm_mesh_read_samples(self._h, _fp(f), _fp(t), n.ctypes.data_as(_I32), cap, C.byref(k)))
         k = k.value
         return f[:k].copy(), t[:k].copy(), n[:k].copy()
+
+    def debug_stall_barriers(self, stall: int):
+        """Test hook of the failure path: with stall > 0 every grid barrier of later launches
+        waits for arrivals that never come, gives up after its bounded wait and the call
+        raises NativeError with status MM_TIMEOUT.  0 restores normal operation."""
+        check(load().mm_debug_stall_barriers(self._h, int(stall)))
 
     def autotune(self, sp) -> int:
         """Pick the persistent launch shape by timing candidates; returns the CTA count."""
