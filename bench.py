@@ -263,9 +263,10 @@ def loop_spec(name: str):
 
 
 def run_batch(args, world, rank, local):
-    """The batched workload: 64 independent loops on seeded meshes of uneven size, stepped in
-    lockstep field steps, all 64 meshes in ONE persistent launch per field step (mm_batch_loop).
-    Beside it, the same loops run one after another with their own autotuned launches."""
+    """The batched workload: 64 independent loops on seeded meshes of uneven size, the whole
+    sweep of all 64 meshes in ONE persistent launch (mm_batch_loop: a CTA group per mesh
+    runs that mesh's field steps on the device).  Beside it, the same loops run one after
+    another with their own autotuned launches (one launch per field step)."""
     import torch
 
     from mammos_mumag import _native
@@ -333,11 +334,11 @@ def run_batch(args, world, rank, local):
             "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "config": {"workload": ("64 independent loops, seeded structured meshes of 12..40 cells per edge "
                                     f"(h = 1.25 nm, {min(nodes)}..{max(nodes)} nodes), 1..27 Voronoi grains, cone "
-                                    "<= 30 deg, +8 -> -8 T in 0.2 T lockstep steps (81), one persistent launch per "
-                                    "lockstep field step"),
+                                    "<= 30 deg, +8 -> -8 T in 0.2 T steps (81), all sweeps in one persistent "
+                                    "launch"),
                        "parallelism": f"replicas x{world}", "l2": "256 MB buffer written between timed sweeps"},
             "variants": variants,
-            "gpu_launches": 81 * args.steps,
+            "gpu_launches": args.steps,
             "clocks": clk.summary() if clk is not None else None,
         }
         print(json.dumps(line), flush=True)

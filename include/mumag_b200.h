@@ -233,10 +233,12 @@ mm_status mm_batch_groups(const mm_batch* batch, int32_t* group);
 /* One field step of every mesh: h[q], sp[q], res[q] (count each). */
 mm_status mm_batch_minimize(mm_batch* batch, const double* h, const mm_solver_params* sp, mm_step_result* res);
 
-/* The field sweep of every mesh in lockstep (all share lp; sp[q] per mesh): rec holds
+/* The field sweep of every mesh (all share lp; sp[q] per mesh), each mesh's whole sweep
+ * inside ONE launch: its CTA group runs the reference's loop (scripts/loop.py:71-124: field
+ * steps, cumulative field update, mfinal stop, snapshot counter) on the device, independent
+ * of the other groups, so a mesh never waits for another mesh's field step.  rec holds
  * count x max_steps rows (mesh-major), nrec[q] the rows written for mesh q, steps (may be
- * NULL) count x max_steps results.  A mesh whose mh falls below mfinal stops (idles in
- * the later launches); the sweep ends when all have stopped or the field range is done.
+ * NULL) count x max_steps results (device_ms 0; kernel_ns is the step's device time).
  * No snapshot callback. */
 mm_status mm_batch_loop(mm_batch* batch, const mm_loop_params* lp, const mm_solver_params* sp, int32_t max_steps,
                         mm_record* rec, int32_t* nrec, mm_step_result* steps);

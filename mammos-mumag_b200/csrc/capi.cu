@@ -803,45 +803,93 @@ mm_status mm_batch_loop(mm_batch* batch, const mm_loop_params* lp, const mm_solv
                         mm_record* rec, int32_t* nrec, mm_step_result* steps) {
   API_BEGIN
   if (!batch || !lp || !sp || !rec || !nrec || max_steps < 1) throw std::runtime_error("invalid batch loop arguments");
-  if (!(lp->hstep != 0.0)) throw std::runtime_error("invalid field sweep");
+  if (!(lp->hstep != 0.0) || !std::isfinite(lp->hstart) || !std::isfinite(lp->hfinal))
+    throw std::runtime_error("invalid field sweep");
   const int count = (int)batch->meshes.size();
   for (int q = 0; q < count; ++q) check_params(&sp[q]);
   int64_t nmax = (int64_t)(std::fabs(lp->hfinal - lp->hstart) / std::fabs(lp->hstep)) + 1;
   if (lp->max_steps > 0) nmax = std::min<int64_t>(nmax, lp->max_steps);
   nmax = std::min<int64_t>(nmax, max_steps);
-  std::vector<double> mh(count, 1.7976931348623157e308), last(count, 1.7976931348623157e308), hv(count);
-  std::vector<int> counter(count, 0);
-  std::vector<char> active(count, 1);
   for (int q = 0; q < count; ++q) nrec[q] = 0;
-  double hext = lp->hstart;
-  for (int64_t idx = 0; idx < nmax; ++idx) {
-    bool any = false;
+  MM_CK(cudaSetDevice(batch->device));
+  // per mesh: rows [nmax][4] doubles, counters [nmax][8] int64, one row count
+  const size_t per = (size_t)nmax * (4 * sizeof(double) + 8 * sizeof(long long)) + 256;
+  char* buf = nullptr;
+  MM_CK(cudaMalloc(reinterpret_cast<void**>(&buf), per * count));
+  std::vector<char> host(per * count);
+  try {
+    MM_CK(cudaMemsetAsync(buf, 0, per * count, batch->stream));
     for (int q = 0; q < count; ++q) {
-      active[q] = active[q] && mh[q] > lp->mfinal;
-      any = any || active[q];
-      hv[q] = hext;
-    }
-    if (!any) break;
-    mm_status st = batch_run(batch, hv.data(), sp, active);
-    if (st != MM_OK) return st == MM_NONFINITE ? fail(st, "energy is not finite at field " + std::to_string(hext)) : st;
-    for (int q = 0; q < count; ++q) {
-      if (!active[q]) continue;
       DevMesh& m = batch->meshes[q]->dm;
-      mh[q] = m.h_resd[1];
-      if ((last[q] - mh[q]) > lp->mstep) {
-        counter[q] += 1;
-        last[q] = mh[q];
-      }
-      mm_record& r = rec[(size_t)q * max_steps + idx];
-      r.counter = counter[q];
-      r.hext = hext;
-      r.mh = mh[q];
-      r.energy = m.h_resd[0];
-      if (steps) fill_result(m, MM_OK, steps[(size_t)q * max_steps + idx]);
-      nrec[q] = (int32_t)(idx + 1);
+      SolveArgs a = solver_args(m, MODE_SWEEP, lp->hstart, sp[q]);
+      char* b = buf + per * q;
+      a.sw_rec = reinterpret_cast<double*>(b);
+      a.sw_stat = reinterpret_cast<long long*>(b + (size_t)nmax * 4 * sizeof(double));
+      a.sw_nrec = reinterpret_cast<int*>(b + (size_t)nmax * (4 * sizeof(double) + 8 * sizeof(long long)));
+      a.sw_hstep = lp->hstep;
+      a.sw_mstep = lp->mstep;
+      a.sw_mfinal = lp->mfinal;
+      a.sw_nmax = (int)nmax;
+      a.stage = batch->plan.stage[q];
+      a.stage_max = batch->plan.stage_max[q];
+      a.meta_max = batch->plan.meta_max[q];
+      a.prof = nullptr;
+      batch->h_args[q] = a;
+      MM_CK(launch_prep(m, batch->stream));
     }
-    hext = hext + lp->hstep;
+    MM_CK(cudaMemcpyAsync(batch->d_args, batch->h_args.data(), sizeof(SolveArgs) * count, cudaMemcpyHostToDevice,
+                          batch->stream));
+    MM_CK(batch_launch(batch->plan, batch->d_args, batch->d_group, count, batch->stream));
+    MM_CK(cudaMemcpyAsync(host.data(), buf, per * count, cudaMemcpyDeviceToHost, batch->stream));
+    for (int q = 0; q < count; ++q) {
+      DevMesh& m = batch->meshes[q]->dm;
+      MM_CK(cudaMemcpyAsync(m.h_flags, m.flags, 2 * sizeof(int), cudaMemcpyDeviceToHost, batch->stream));
+    }
+    MM_CK(cudaStreamSynchronize(batch->stream));
+  } catch (...) {
+    cudaFree(buf);
+    throw;
   }
+  cudaFree(buf);
+  for (int q = 0; q < count; ++q) batch->meshes[q]->dm.rec_seed = next_seed(batch->meshes[q]->dm.rec_seed);
+  mm_status worst = MM_OK;
+  for (int q = 0; q < count; ++q) {
+    const int st = batch->meshes[q]->dm.h_flags[FLAG_STATUS];
+    if (st == MM_TIMEOUT) return fail(MM_TIMEOUT, "a grid barrier of the batched solver kernel timed out");
+    if (st != MM_OK && st != MM_NONFINITE)
+      return fail(MM_CUDA_ERROR, "the batched solver kernel left an invalid status word");
+    if (st == MM_NONFINITE) worst = MM_NONFINITE;
+    const char* b = host.data() + per * q;
+    const double* rows = reinterpret_cast<const double*>(b);
+    const long long* stat = reinterpret_cast<const long long*>(b + (size_t)nmax * 4 * sizeof(double));
+    const int k = *reinterpret_cast<const int*>(b + (size_t)nmax * (4 * sizeof(double) + 8 * sizeof(long long)));
+    if (k < 0 || k > nmax) return fail(MM_CUDA_ERROR, "the batched solver kernel left an invalid row count");
+    for (int i = 0; i < k; ++i) {
+      mm_record& r = rec[(size_t)q * max_steps + i];
+      r.counter = rows[4 * i + 0];
+      r.hext = rows[4 * i + 1];
+      r.mh = rows[4 * i + 2];
+      r.energy = rows[4 * i + 3];
+      if (steps) {
+        mm_step_result& t = steps[(size_t)q * max_steps + i];
+        t = mm_step_result{};
+        t.energy = r.energy;
+        t.mh = r.mh;
+        t.ncg_iters = stat[8 * i + 0];
+        t.evals = stat[8 * i + 1];
+        t.pcg_iters = stat[8 * i + 2];
+        t.ls_shrinks = stat[8 * i + 3];
+        t.minv_iters = stat[8 * i + 4];
+        t.kernel_ns = stat[8 * i + 5];
+        t.sync_ns = stat[8 * i + 6];
+        t.barriers = stat[8 * i + 7];
+        t.device_ms = 0.0;
+        t.status = MM_OK;
+      }
+    }
+    nrec[q] = k;
+  }
+  if (worst == MM_NONFINITE) return fail(MM_NONFINITE, "energy is not finite in a batched sweep");
   return MM_OK;
   API_END
 }

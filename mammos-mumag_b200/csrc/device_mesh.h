@@ -102,9 +102,15 @@ struct SolveArgs {
   int64_t stage_max;          // entries of the largest CTA (shared-memory layout)
   int64_t meta_max;           // slices of the largest CTA (shared-memory slice metadata)
   // control
-  int mode;  // 0 energy+gradient, 1 M_inv, 2 minimise (one field step)
+  int mode;  // 0 energy+gradient, 1 M_inv, 2 minimise (one field step), 3 idle, 4 field sweep
   double h, hdir[3], tol_fun, sqrt_tol, cbrt_tol, tol_u;
   int precond_iter, hmag_on, mbar_current, max_pcg, max_ncg;
+  // field sweep inside one launch (MODE_SWEEP): from h by sw_hstep, scripts/loop.py:71-124
+  double sw_hstep, sw_mstep, sw_mfinal;
+  int sw_nmax;
+  double* sw_rec;       // [sw_nmax][4] counter, hext, mh, energy
+  long long* sw_stat;   // [sw_nmax][8] ncg, evals, pcg, shrinks, minv, ns, sync ns, barriers
+  int* sw_nrec;         // rows written
   // optional per-CTA timing [gridDim.x][4] ns (null = off): PCG row phases, reduction
   // before the barrier, barrier wait, partial read after the barrier
   long long* prof;
@@ -114,7 +120,7 @@ struct SolveArgs {
 };
 
 enum { WARM_PREV = 0, WARM_ZERO = 1, WARM_LEARNED = 2 };
-enum { MODE_EVAL = 0, MODE_MINV = 1, MODE_MINIMIZE = 2, MODE_IDLE = 3 };
+enum { MODE_EVAL = 0, MODE_MINV = 1, MODE_MINIMIZE = 2, MODE_IDLE = 3, MODE_SWEEP = 4 };
 enum { FLAG_ABORT = 0, FLAG_STATUS = 1 };
 
 struct DevMesh {

@@ -182,7 +182,8 @@ struct Ctx {
   int64_t cbase;
   long long evals = 0, pcg_iters = 0, minv_iters = 0, shrinks = 0;
   unsigned long long t_phase_start = 0, t_pcg_phase = 0;
-  __device__ Ctx(const SolveArgs& args) : a(args) {}
+  double h;  // applied field of the current field step (mu0 H, T)
+  __device__ Ctx(const SolveArgs& args) : a(args), h(args.h) {}
 };
 
 // Rows of this CTA: warp w takes slices s0+w, s0+w+nwarps, ...; lane = row in slice.
@@ -828,9 +829,9 @@ __device__ bool eval(Ctx& c, const double* x, const double* xref, const double* 
   const int n = a.Npad;
   const double* G = plane(a, P_G);
   const int64_t ps = a.nent;
-  const double cz0 = (-a.h * a.hdir[0]) / a.V;
-  const double cz1 = (-a.h * a.hdir[1]) / a.V;
-  const double cz2 = (-a.h * a.hdir[2]) / a.V;
+  const double cz0 = (-c.h * a.hdir[0]) / a.V;
+  const double cz1 = (-c.h * a.hdir[1]) / a.V;
+  const double cz2 = (-c.h * a.hdir[2]) / a.V;
   double pE = 0, pgd = 0, pdx = 0, px = 0, pgi = 0;
   FOR_ROWS(c)
   double gc[3];
@@ -1032,7 +1033,7 @@ __device__ bool minv(Ctx& c, const double* g, const double* mb, double* zout) {
 // ---------------------------------------------------------------------------------------
 // hestenes_stiefel_ncg + line_search, scripts/minimizers.py:16-190
 // ---------------------------------------------------------------------------------------
-__device__ bool minimize(Ctx& c) {
+__device__ __noinline__ bool minimize(Ctx& c, double& f_out, double& mh_out, long long& k_out) {
   const SolveArgs& a = c.a;
   const int n = a.Npad;
   const double sqrt_eps = 1.4901161193847656e-08;  // sqrt(2^-52)
@@ -1200,11 +1201,57 @@ __device__ bool minimize(Ctx& c) {
   END_ROWS
   double v[1] = {pm};
   CHECK(grid_reduce<1>(c.sy, v, 0u));
+  f_out = f;
+  mh_out = v[0] / a.V;
+  k_out = k;
   if (c.sy.blk == 0 && threadIdx.x == 0) {
     a.resd[0] = f;
     a.resd[1] = v[0] / a.V;
     a.resi[0] = k;
     if (!(f - f == 0.0)) atomicCAS(&a.flags[FLAG_STATUS], 0, (int)MM_NONFINITE);
+  }
+  return true;
+}
+
+// The field sweep of scripts/loop.py:71-124 inside one launch (MODE_SWEEP, the batched
+// loop): field steps from a.h by a.sw_hstep while mh > a.sw_mfinal and fewer than
+// a.sw_nmax steps, the cumulative field update and the snapshot counter of the reference
+// (no snapshots are written).  Rows [counter, hext, mh, E] and per-step counters
+// [ncg, evals, pcg, shrinks, minv, ns, sync ns, barriers] go to a.sw_rec / a.sw_stat.
+__device__ bool sweep(Ctx& c) {
+  const SolveArgs& a = c.a;
+  double mh = DBL_MAX, last_saved = DBL_MAX, counter = 0.0, hext = a.h;
+  const bool lead = c.sy.blk == 0 && threadIdx.x == 0;
+  for (int idx = 0; idx < a.sw_nmax && mh > a.sw_mfinal; ++idx) {
+    const long long e0 = c.evals, p0 = c.pcg_iters, s0 = c.shrinks, m0 = c.minv_iters;
+    const unsigned long long t0 = lead ? globaltimer() : 0ull, y0 = c.sy.t_sync, b0 = c.sy.epoch;
+    c.h = hext;
+    double f;
+    long long k;
+    CHECK(minimize(c, f, mh, k));
+    if (!(f - f == 0.0)) return true;  // non-finite energy: status set, the sweep stops
+    if ((last_saved - mh) > a.sw_mstep) {
+      counter += 1.0;
+      last_saved = mh;
+    }
+    if (lead) {
+      double* r = a.sw_rec + 4 * (size_t)idx;
+      r[0] = counter;
+      r[1] = hext;
+      r[2] = mh;
+      r[3] = f;
+      long long* st = a.sw_stat + 8 * (size_t)idx;
+      st[0] = k;
+      st[1] = c.evals - e0;
+      st[2] = c.pcg_iters - p0;
+      st[3] = c.shrinks - s0;
+      st[4] = c.minv_iters - m0;
+      st[5] = (long long)(globaltimer() - t0);
+      st[6] = (long long)(c.sy.t_sync - y0);
+      st[7] = (long long)(c.sy.epoch - b0);
+      *a.sw_nrec = idx + 1;
+    }
+    hext = hext + a.sw_hstep;
   }
   return true;
 }
@@ -1275,8 +1322,12 @@ __device__ __forceinline__ void solve_body(const SolveArgs& args, int nblk, int 
     }
   } else if (args.mode == MODE_MINV) {
     ok = minv(c, args.g, args.mbar_current ? args.x : args.mbar, args.zp);
+  } else if (args.mode == MODE_SWEEP) {
+    ok = sweep(c);
   } else {
-    ok = minimize(c);
+    double f, mh;
+    long long k;
+    ok = minimize(c, f, mh, k);
   }
   if (ok && blk == 0 && threadIdx.x == 0) {
     args.resi[1] = c.evals;

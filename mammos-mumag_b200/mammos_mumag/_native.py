@@ -562,7 +562,7 @@ class Batch:
         return [r.as_dict() for r in res]
 
     def loop(self, hstart, hfinal, hstep, mstep, mfinal, sps, max_steps=0):
-        """Lockstep sweep; returns per mesh (rows [n,4], per-step dicts)."""
+        """Every mesh's whole sweep in one launch; returns per mesh (rows [n,4], per-step dicts)."""
         n = len(self.meshes)
         nmax = int(abs(hfinal - hstart) / abs(hstep)) + 1
         if max_steps > 0:
