@@ -261,18 +261,192 @@ __global__ void k_publish(const float* p, __nv_bfloat16* W1, __nv_bfloat16* W2, 
   }
 }
 
-__global__ void k_predict(MlpDev M, const float* __restrict__ feat, int n, float* du) {
-  const int lane = threadIdx.x & 31;
-  const int tile = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  if (tile * 16 >= n) return;
-  const int r0 = tile * 16, g = lane >> 2, t = lane & 3;
-  auto F = [&](int row, int col) { return r0 + row < n ? feat[(size_t)(r0 + row) * kMlpIn + col] : 0.f; };
-  float lo, hi;
-  mlp_tile_forward(M, lane, F, lo, hi);
-  if (t == 0) {
-    if (r0 + g < n) du[r0 + g] = lo;
-    if (r0 + g + 8 < n) du[r0 + g + 8] = hi;
+// ---- inference on the 5th-generation tensor cores (tcgen05, accumulators in TMEM) ----------
+//
+// One CTA of 128 threads takes 128-row tiles (M = 128): thread r owns row r.  The three
+// hidden layers are tcgen05.mma kind::f16 products, M = 128, N = 128, BF16 operands from
+// shared memory, FP32 accumulation in 128 TMEM columns; one elected thread issues them and
+// commits to an mbarrier.  Between layers every thread reads its row's 128 accumulators
+// (tcgen05.ld 32x32b), adds the bias, applies GELU, rounds to BF16 and writes the row into
+// the next layer's operand buffer.  The 128 -> 1 head is a per-thread dot product.  The
+// weights are copied into shared memory once per CTA.
+//
+// Operand layout (K-major, no swizzle): 8-row x 16-byte core matrices, 128 contiguous bytes
+// each; the K/8 core matrices of an 8-row group are adjacent (leading byte offset 128), the
+// groups K/8 * 128 bytes apart (stride byte offset).  One MMA consumes K = 16, i.e. two
+// core matrices: the descriptors of step ks start 256 * ks bytes in.
+constexpr int kTcThreads = 128;
+constexpr uint32_t kSmW1 = 0;                                            // [128][16]  bf16
+constexpr uint32_t kSmW2 = kSmW1 + kMlpHidden * kMlpInPad * 2;           // [128][128]
+constexpr uint32_t kSmW3 = kSmW2 + kMlpHidden * kMlpHidden * 2;
+constexpr uint32_t kSmA0 = kSmW3 + kMlpHidden * kMlpHidden * 2;          // [128][16] layer-1 input
+constexpr uint32_t kSmA = kSmA0 + kTcThreads * kMlpInPad * 2;            // [128][128] hidden rows
+constexpr uint32_t kSmBar = kSmA + kTcThreads * kMlpHidden * 2;          // mbarrier, TMEM address
+constexpr uint32_t kSmTc = kSmBar + 16;
+constexpr uint32_t kTmemCols = 128;
+constexpr unsigned kTcWaitLimit = 1u << 22;
+
+// byte offset of element (r, k) of a K-major [rows][kdim] BF16 operand
+__device__ __forceinline__ uint32_t umma_off(int r, int k, int kdim) {
+  return (uint32_t)(((r >> 3) * (kdim >> 3) + (k >> 3)) * 128 + (r & 7) * 16 + (k & 7) * 2);
+}
+// shared-memory matrix descriptor: start, leading and stride byte offsets (>> 4), the
+// Blackwell descriptor version 1 (bit 46), no swizzle
+__device__ __forceinline__ uint64_t umma_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
+  return (uint64_t)((saddr >> 4) & 0x3FFFu) | ((uint64_t)((lbo >> 4) & 0x3FFFu) << 16) |
+         ((uint64_t)((sbo >> 4) & 0x3FFFu) << 32) | (1ull << 46);
+}
+// instruction descriptor: FP32 accumulator, BF16 A and B, both K-major, N = 128, M = 128
+constexpr uint32_t kTcIdesc = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(128 >> 3) << 17) |
+                              ((uint32_t)(128 >> 4) << 24);
+
+__device__ __forceinline__ void tc_mma(uint32_t tmem, uint64_t a, uint64_t b, uint32_t accumulate) {
+  const uint32_t z = 0;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n" ::"r"(tmem),
+      "l"(a), "l"(b), "r"(kTcIdesc), "r"(accumulate), "r"(z), "r"(z), "r"(z), "r"(z));
+}
+__device__ __forceinline__ void tc_commit(uint32_t bar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar) : "memory");
+}
+// bounded wait for the mbarrier phase; false after the limit
+__device__ __forceinline__ bool tc_wait(uint32_t bar, uint32_t phase) {
+  for (unsigned it = 0; it < kTcWaitLimit; ++it) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred P1;\n\tmbarrier.try_wait.parity.shared::cta.b64 P1, [%1], %2;\n\t"
+        "selp.b32 %0, 1, 0, P1;\n\t}\n"
+        : "=r"(ok)
+        : "r"(bar), "r"(phase)
+        : "memory");
+    if (ok) return true;
+    if (it > 64) __nanosleep(64);
   }
+  return false;
+}
+__device__ __forceinline__ void tc_ld16(uint32_t taddr, float (&v)[16]) {
+  uint32_t r[16];
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+        "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+      : "r"(taddr));
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+  for (int q = 0; q < 16; ++q) v[q] = __uint_as_float(r[q]);
+}
+
+// Copy a [128][kdim] BF16 weight matrix (row-major [out][in]) into the operand layout.
+__device__ __forceinline__ void tc_stage_weights(unsigned char* sm, uint32_t off, const __nv_bfloat16* W, int kdim) {
+  const int chunks = kMlpHidden * kdim / 8;
+  for (int c = threadIdx.x; c < chunks; c += blockDim.x) {
+    const int r = c / (kdim / 8), k = (c % (kdim / 8)) * 8;
+    *reinterpret_cast<uint4*>(sm + off + umma_off(r, k, kdim)) =
+        __ldg(reinterpret_cast<const uint4*>(W + (size_t)r * kdim + k));
+  }
+}
+
+__global__ void __launch_bounds__(kTcThreads, 1) k_mlp_tc(MlpDev M, const float* __restrict__ feat, int n,
+                                                          float* __restrict__ y, int* err) {
+  extern __shared__ __align__(1024) unsigned char sm[];
+  const int tid = threadIdx.x, warp = tid >> 5;
+  const uint32_t sbase = (uint32_t)__cvta_generic_to_shared(sm);
+  const uint32_t bar = sbase + kSmBar;
+  uint32_t* tslot = reinterpret_cast<uint32_t*>(sm + kSmBar + 8);
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(bar + 8),
+                 "r"(kTmemCols));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+  }
+  if (tid == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(1));
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  tc_stage_weights(sm, kSmW1, M.W1, kMlpInPad);
+  tc_stage_weights(sm, kSmW2, M.W2, kMlpHidden);
+  tc_stage_weights(sm, kSmW3, M.W3, kMlpHidden);
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  const uint32_t tmem = *tslot;
+  const uint32_t trow = tmem + ((uint32_t)(32 * warp) << 16);  // this warp's 32 TMEM lanes
+  uint32_t phase = 0;
+  bool ok = true;
+  const int ntiles = (n + kTcThreads - 1) / kTcThreads;
+  for (int tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x) {
+    const int row = tile * kTcThreads + tid;
+    {  // layer-1 operand: the row's normalised features, BF16
+      float f[kMlpIn];
+#pragma unroll
+      for (int q = 0; q < kMlpIn; ++q)
+        f[q] = row < n ? (feat[(size_t)row * kMlpIn + q] - __ldg(M.fmean + q)) * __ldg(M.fscale + q) : 0.f;
+#pragma unroll
+      for (int c = 0; c < kMlpIn / 8; ++c) {
+        uint4 v;
+        v.x = pack_bf16(f[8 * c + 0], f[8 * c + 1]);
+        v.y = pack_bf16(f[8 * c + 2], f[8 * c + 3]);
+        v.z = pack_bf16(f[8 * c + 4], f[8 * c + 5]);
+        v.w = pack_bf16(f[8 * c + 6], f[8 * c + 7]);
+        *reinterpret_cast<uint4*>(sm + kSmA0 + umma_off(tid, 8 * c, kMlpInPad)) = v;
+      }
+    }
+    float yacc = 0.f;
+    for (int layer = 0; layer < 3 && ok; ++layer) {
+      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+      asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+      __syncthreads();
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+      if (tid == 0) {
+        const uint32_t aoff = layer == 0 ? kSmA0 : kSmA;
+        const uint32_t woff = layer == 0 ? kSmW1 : layer == 1 ? kSmW2 : kSmW3;
+        const int kdim = layer == 0 ? kMlpInPad : kMlpHidden;
+        const uint32_t sbo = (uint32_t)(kdim / 8) * 128;
+        for (int ks = 0; ks < kdim / 16; ++ks)
+          tc_mma(tmem, umma_desc(sbase + aoff + 256 * ks, 128, sbo), umma_desc(sbase + woff + 256 * ks, 128, sbo),
+                 ks > 0 ? 1u : 0u);
+        tc_commit(bar);
+      }
+      const bool got = tc_wait(bar, phase);
+      if (__syncthreads_or(!got)) {  // every thread leaves together
+        ok = false;
+        if (tid == 0) atomicExch(err, 1);
+        break;
+      }
+      phase ^= 1u;
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+      const float* bias = layer == 0 ? M.b1 : layer == 1 ? M.b2 : M.b3;
+#pragma unroll 1
+      for (int j = 0; j < kMlpHidden / 16; ++j) {
+        float v[16];
+        tc_ld16(trow + 16 * j, v);
+#pragma unroll
+        for (int q = 0; q < 16; ++q) v[q] = gelu_f(v[q] + __ldg(bias + 16 * j + q));
+        if (layer < 2) {
+#pragma unroll
+          for (int c = 0; c < 2; ++c) {
+            uint4 w;
+            w.x = pack_bf16(v[8 * c + 0], v[8 * c + 1]);
+            w.y = pack_bf16(v[8 * c + 2], v[8 * c + 3]);
+            w.z = pack_bf16(v[8 * c + 4], v[8 * c + 5]);
+            w.w = pack_bf16(v[8 * c + 6], v[8 * c + 7]);
+            *reinterpret_cast<uint4*>(sm + kSmA + umma_off(tid, 16 * j + 8 * c, kMlpHidden)) = w;
+          }
+        } else {  // head: the BF16-rounded activations against w4
+#pragma unroll
+          for (int q = 0; q < 16; ++q)
+            yacc += __bfloat162float(__float2bfloat16(v[q])) * __ldg(M.w4 + 16 * j + q);
+        }
+      }
+    }
+    if (ok && row < n) y[row] = (yacc + __ldg(M.b4)) * M.out_scale;
+  }
+  if (!ok) tc_wait(bar, phase);  // bounded: let an outstanding product finish before freeing TMEM
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  if (warp == 0)
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTmemCols));
 }
 
 }  // namespace
@@ -657,12 +831,25 @@ mm_status mm_model_predict(mm_model* mo, const float* feats, int64_t n, float* y
   Model& md = mo->md;
   MM_CK(cudaSetDevice(md.device));
   DevBuf<float> df((size_t)n * kMlpIn), dd(n);
+  DevBuf<int> derr(1);
+  MM_CK(cudaMemsetAsync(derr.p, 0, sizeof(int), md.stream));
   MM_CK(cudaMemcpyAsync(df.p, feats, sizeof(float) * n * kMlpIn, cudaMemcpyHostToDevice, md.stream));
-  const int64_t warps = (n + 15) / 16;
-  k_predict<<<(unsigned)((warps * 32 + 127) / 128), 128, 0, md.stream>>>(md.view(), df.p, (int)n, dd.p);
+  static bool attr_set[64] = {};
+  if (md.device < 64 && !attr_set[md.device]) {
+    MM_CK(cudaFuncSetAttribute(k_mlp_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmTc));
+    attr_set[md.device] = true;
+  }
+  cudaDeviceProp prop;
+  MM_CK(cudaGetDeviceProperties(&prop, md.device));
+  const int64_t tiles = (n + kTcThreads - 1) / kTcThreads;
+  const int grid = (int)std::min<int64_t>(tiles, 2 * (int64_t)prop.multiProcessorCount);
+  k_mlp_tc<<<grid, kTcThreads, kSmTc, md.stream>>>(md.view(), df.p, (int)n, dd.p, derr.p);
   MM_CK(cudaGetLastError());
+  int herr = 0;
   MM_CK(cudaMemcpyAsync(y, dd.p, sizeof(float) * n, cudaMemcpyDeviceToHost, md.stream));
+  MM_CK(cudaMemcpyAsync(&herr, derr.p, sizeof(int), cudaMemcpyDeviceToHost, md.stream));
   MM_CK(cudaStreamSynchronize(md.stream));
+  if (herr) return mfail(MM_TIMEOUT, "the tensor-core inference kernel timed out waiting for its products");
   return MM_OK;
   MAPI_END
 }

@@ -27,8 +27,10 @@ def _model_and_data(seed=0, n=256):
     return model, feats, target
 
 
-def test_predict_matches_oracle():
-    model, feats, _ = _model_and_data(1, 512)
+@pytest.mark.parametrize("rows", [512, 1000, 20000])
+def test_predict_matches_oracle(rows):
+    """mm_model_predict runs the tcgen05 kernel: 128-row tiles, the last one partial."""
+    model, feats, _ = _model_and_data(1, rows)
     p = model.get_params()
     fm, fs, osc = model.get_normalization()
     y = model.predict(feats)
