@@ -263,25 +263,29 @@ __global__ void k_publish(const float* p, __nv_bfloat16* W1, __nv_bfloat16* W2, 
 
 // ---- inference on the 5th-generation tensor cores (tcgen05, accumulators in TMEM) ----------
 //
-// One CTA of 128 threads takes 128-row tiles (M = 128): thread r owns row r.  The three
-// hidden layers are tcgen05.mma kind::f16 products, M = 128, N = 128, BF16 operands from
-// shared memory, FP32 accumulation in 128 TMEM columns; one elected thread issues them and
-// commits to an mbarrier.  Between layers every thread reads its row's 128 accumulators
-// (tcgen05.ld 32x32b), adds the bias, applies GELU, rounds to BF16 and writes the row into
-// the next layer's operand buffer.  The 128 -> 1 head is a per-thread dot product.  The
-// weights are copied into shared memory once per CTA.
+// One CTA of 256 threads takes 128-row tiles (M = 128).  The three hidden layers are
+// tcgen05.mma kind::f16 products, M = 128, N = 128, BF16 operands from shared memory, FP32
+// accumulation in 128 TMEM columns; one thread issues them and commits to an mbarrier.
+// Between layers warp w reads TMEM lanes 32 (w % 4) .. +31 (its rows) and columns
+// 64 (w / 4) .. +63 (tcgen05.ld 32x32b), adds the bias, applies GELU, rounds to BF16 and
+// writes them into the next layer's operand buffer; two warps per lane quarter split the
+// CUDA-core epilogue.  The 128 -> 1 head is a per-thread dot product over its 64 columns,
+// the two halves summed through shared memory.  The weights are copied into shared memory
+// once per CTA.
 //
 // Operand layout (K-major, no swizzle): 8-row x 16-byte core matrices, 128 contiguous bytes
 // each; the K/8 core matrices of an 8-row group are adjacent (leading byte offset 128), the
 // groups K/8 * 128 bytes apart (stride byte offset).  One MMA consumes K = 16, i.e. two
 // core matrices: the descriptors of step ks start 256 * ks bytes in.
-constexpr int kTcThreads = 128;
+constexpr int kTcRows = 128;     // rows per tile (M)
+constexpr int kTcThreads = 256;  // two warps per TMEM lane quarter
 constexpr uint32_t kSmW1 = 0;                                            // [128][16]  bf16
 constexpr uint32_t kSmW2 = kSmW1 + kMlpHidden * kMlpInPad * 2;           // [128][128]
 constexpr uint32_t kSmW3 = kSmW2 + kMlpHidden * kMlpHidden * 2;
 constexpr uint32_t kSmA0 = kSmW3 + kMlpHidden * kMlpHidden * 2;          // [128][16] layer-1 input
-constexpr uint32_t kSmA = kSmA0 + kTcThreads * kMlpInPad * 2;            // [128][128] hidden rows
-constexpr uint32_t kSmBar = kSmA + kTcThreads * kMlpHidden * 2;          // mbarrier, TMEM address
+constexpr uint32_t kSmA = kSmA0 + kTcRows * kMlpInPad * 2;               // [128][128] hidden rows
+constexpr uint32_t kSmHead = kSmA + kTcRows * kMlpHidden * 2;            // [128] head partials
+constexpr uint32_t kSmBar = kSmHead + kTcRows * 4;                       // mbarrier, TMEM address
 constexpr uint32_t kSmTc = kSmBar + 16;
 constexpr uint32_t kTmemCols = 128;
 constexpr unsigned kTcWaitLimit = 1u << 22;
@@ -350,10 +354,13 @@ __device__ __forceinline__ void tc_stage_weights(unsigned char* sm, uint32_t off
 __global__ void __launch_bounds__(kTcThreads, 1) k_mlp_tc(MlpDev M, const float* __restrict__ feat, int n,
                                                           float* __restrict__ y, int* err) {
   extern __shared__ __align__(1024) unsigned char sm[];
-  const int tid = threadIdx.x, warp = tid >> 5;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int rloc = 32 * (warp & 3) + lane;  // this thread's row in the tile (its TMEM lane)
+  const int cbase = 64 * (warp >> 2);       // its 64 columns
   const uint32_t sbase = (uint32_t)__cvta_generic_to_shared(sm);
   const uint32_t bar = sbase + kSmBar;
   uint32_t* tslot = reinterpret_cast<uint32_t*>(sm + kSmBar + 8);
+  float* head = reinterpret_cast<float*>(sm + kSmHead);
   if (warp == 0) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(bar + 8),
                  "r"(kTmemCols));
@@ -371,26 +378,26 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_mlp_tc(MlpDev M, const float*
   __syncthreads();
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
   const uint32_t tmem = *tslot;
-  const uint32_t trow = tmem + ((uint32_t)(32 * warp) << 16);  // this warp's 32 TMEM lanes
+  const uint32_t trow = tmem + ((uint32_t)(32 * (warp & 3)) << 16) + (uint32_t)cbase;
   uint32_t phase = 0;
   bool ok = true;
-  const int ntiles = (n + kTcThreads - 1) / kTcThreads;
+  const int ntiles = (n + kTcRows - 1) / kTcRows;
   for (int tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x) {
-    const int row = tile * kTcThreads + tid;
-    {  // layer-1 operand: the row's normalised features, BF16
-      float f[kMlpIn];
+    const int row = tile * kTcRows + rloc;
+    {  // layer-1 operand: the row's normalised features, BF16 (8 per thread)
+      const int c = warp >> 2;
+      float f[8];
 #pragma unroll
-      for (int q = 0; q < kMlpIn; ++q)
-        f[q] = row < n ? (feat[(size_t)row * kMlpIn + q] - __ldg(M.fmean + q)) * __ldg(M.fscale + q) : 0.f;
-#pragma unroll
-      for (int c = 0; c < kMlpIn / 8; ++c) {
-        uint4 v;
-        v.x = pack_bf16(f[8 * c + 0], f[8 * c + 1]);
-        v.y = pack_bf16(f[8 * c + 2], f[8 * c + 3]);
-        v.z = pack_bf16(f[8 * c + 4], f[8 * c + 5]);
-        v.w = pack_bf16(f[8 * c + 6], f[8 * c + 7]);
-        *reinterpret_cast<uint4*>(sm + kSmA0 + umma_off(tid, 8 * c, kMlpInPad)) = v;
-      }
+      for (int q = 0; q < 8; ++q)
+        f[q] = row < n ? (feat[(size_t)row * kMlpIn + 8 * c + q] - __ldg(M.fmean + 8 * c + q)) *
+                             __ldg(M.fscale + 8 * c + q)
+                       : 0.f;
+      uint4 v;
+      v.x = pack_bf16(f[0], f[1]);
+      v.y = pack_bf16(f[2], f[3]);
+      v.z = pack_bf16(f[4], f[5]);
+      v.w = pack_bf16(f[6], f[7]);
+      *reinterpret_cast<uint4*>(sm + kSmA0 + umma_off(rloc, 8 * c, kMlpInPad)) = v;
     }
     float yacc = 0.f;
     for (int layer = 0; layer < 3 && ok; ++layer) {
@@ -416,9 +423,9 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_mlp_tc(MlpDev M, const float*
       }
       phase ^= 1u;
       asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-      const float* bias = layer == 0 ? M.b1 : layer == 1 ? M.b2 : M.b3;
+      const float* bias = (layer == 0 ? M.b1 : layer == 1 ? M.b2 : M.b3) + cbase;
 #pragma unroll 1
-      for (int j = 0; j < kMlpHidden / 16; ++j) {
+      for (int j = 0; j < 4; ++j) {
         float v[16];
         tc_ld16(trow + 16 * j, v);
 #pragma unroll
@@ -431,16 +438,20 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_mlp_tc(MlpDev M, const float*
             w.y = pack_bf16(v[8 * c + 2], v[8 * c + 3]);
             w.z = pack_bf16(v[8 * c + 4], v[8 * c + 5]);
             w.w = pack_bf16(v[8 * c + 6], v[8 * c + 7]);
-            *reinterpret_cast<uint4*>(sm + kSmA + umma_off(tid, 16 * j + 8 * c, kMlpHidden)) = w;
+            *reinterpret_cast<uint4*>(sm + kSmA + umma_off(rloc, cbase + 16 * j + 8 * c, kMlpHidden)) = w;
           }
         } else {  // head: the BF16-rounded activations against w4
 #pragma unroll
           for (int q = 0; q < 16; ++q)
-            yacc += __bfloat162float(__float2bfloat16(v[q])) * __ldg(M.w4 + 16 * j + q);
+            yacc += __bfloat162float(__float2bfloat16(v[q])) * __ldg(M.w4 + cbase + 16 * j + q);
         }
       }
     }
-    if (ok && row < n) y[row] = (yacc + __ldg(M.b4)) * M.out_scale;
+    if (ok) {  // the two column halves of each row's head
+      if (warp >= 4) head[rloc] = yacc;
+      __syncthreads();
+      if (warp < 4 && row < n) y[row] = (yacc + head[rloc] + __ldg(M.b4)) * M.out_scale;
+    }
   }
   if (!ok) tc_wait(bar, phase);  // bounded: let an outstanding product finish before freeing TMEM
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
@@ -841,7 +852,7 @@ mm_status mm_model_predict(mm_model* mo, const float* feats, int64_t n, float* y
   }
   cudaDeviceProp prop;
   MM_CK(cudaGetDeviceProperties(&prop, md.device));
-  const int64_t tiles = (n + kTcThreads - 1) / kTcThreads;
+  const int64_t tiles = (n + kTcRows - 1) / kTcRows;
   const int grid = (int)std::min<int64_t>(tiles, 2 * (int64_t)prop.multiProcessorCount);
   k_mlp_tc<<<grid, kTcThreads, kSmTc, md.stream>>>(md.view(), df.p, (int)n, dd.p, derr.p);
   MM_CK(cudaGetLastError());
