@@ -459,6 +459,43 @@ __device__ __noinline__ bool learned_start_mixed(Ctx& c, const double* x, double
   return true;
 }
 
+// One row of an SpMV over the staged pattern, sum_k val[k] z[col[k]] in entry order, with
+// the next 8 entries' columns and values loaded while the current 8 gather z: two
+// dependent memory round trips (column, then z) overlap across chunks.  w is the slice's
+// width, the same for the warp's 32 lanes, so the guards do not diverge.
+template <class VT, class ZT, class AT>
+__device__ __forceinline__ AT gather_row(const Ctx& c, const VT* sval, int64_t loff, int w, const ZT* z) {
+  AT acc = 0;
+  int jc[8];
+  VT vc[8];
+#pragma unroll
+  for (int q = 0; q < 8; ++q) {
+    const bool in = q < w;
+    jc[q] = in ? c.scol[loff + 32 * (int64_t)q] : 0;
+    vc[q] = in ? sval[loff + 32 * (int64_t)q] : VT(0);
+  }
+  for (int k0 = 0; k0 < w; k0 += 8) {
+    int jn[8];
+    VT vn[8];
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+      const int k = k0 + 8 + q;
+      const bool in = k < w;
+      jn[q] = in ? c.scol[loff + 32 * (int64_t)k] : 0;
+      vn[q] = in ? sval[loff + 32 * (int64_t)k] : VT(0);
+    }
+#pragma unroll
+    for (int q = 0; q < 8; ++q)
+      if (k0 + q < w) acc += vc[q] * (AT)z[jc[q]];
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+      jc[q] = jn[q];
+      vc[q] = vn[q];
+    }
+  }
+  return acc;
+}
+
 // The same Chronopoulos-Gear iteration with two grid synchronisations per iteration
 // instead of one: an update phase (own rows: s, r, p, u and z = r/diag, stored as a plane;
 // partials r.z and r.r), a barrier, and an SpMV phase w = S z gathering only z (partial
@@ -482,16 +519,16 @@ __device__ __noinline__ bool pcg_loop2(Ctx& c, double alpha, double beta, double
     const double p = q.r * q.invd + beta * a.pp[i];
     a.pp[i] = p;
     a.u[i] = a.u[i] + alpha * p;
-    rec_store(rc, i, n, PcgRec{o.r, q.w, o.s, q.invd});
+    double* pl = reinterpret_cast<double*>(rc);
+    pl[i] = o.r;          // r plane
+    pl[2 * n + i] = o.s;  // s plane (w and 1/diag unchanged)
     z[i] = o.z;
     pg += o.r * o.z;
     pr2 += o.r * o.r;
     END_ROWS
     CHECK(grid_barrier(c.sy));
     FOR_ROWS(c)
-    double acc = 0;
-#pragma unroll 8
-    for (int k2 = 0; k2 < w_; ++k2) acc += c.sS[LENTRY(k2)] * z[c.scol[LENTRY(k2)]];
+    const double acc = gather_row<double, double, double>(c, c.sS, loff_, w_, z);
     rec_store_w(rc, i, n, acc);
     pd += acc * z[i];
     END_ROWS
@@ -664,9 +701,7 @@ __device__ __noinline__ bool pcg_inner2(Ctx& c, double alpha, double beta, doubl
     END_ROWS
     CHECK(grid_barrier(c.sy));
     FOR_ROWS(c)
-    float acc = 0.f;
-#pragma unroll 8
-    for (int k2 = 0; k2 < w_; ++k2) acc += c.sS32[LENTRY(k2)] * z[c.scol[LENTRY(k2)]];
+    const float acc = gather_row<float, float, float>(c, c.sS32, loff_, w_, z);
     rc[i].w = acc;
     pd += (double)acc * (double)z[i];
     END_ROWS
