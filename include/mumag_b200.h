@@ -263,7 +263,9 @@ mm_status mm_timer_stop(mm_mesh* mesh, double* elapsed_ms);
  * No counterpart in the reference, whose PCG always starts from the previous potential
  * (scripts/solvers.py:221-231, x0 = u).  A per-node network
  *   16 features -> 128 -> 128 -> 128 -> 1, GELU (tanh form), BF16 weights, FP32 accumulation
- * corrects that start: u0 = u_prev + sigma * y(features).  The features of node i over its
+ * corrects that start: u0 = u_prev + alpha * y(features), with the step alpha = y.r0 / y.S y
+ * that minimises the S-norm of the error along the prediction (a one-dimensional Galerkin
+ * projection: the start is never worse than u_prev in that norm).  The features of node i over its
  * 1-ring (its row of the Poisson pattern): m_i (3), u_i, ring mean of m (3) and u, ring max of
  * m (3) and u, then the Jacobi-scaled initial residual z = (b - S u_prev)/diag(S) in units of
  * sigma = rms(z): z_i and its ring mean, max and min.  The PCG then runs from u0 to the

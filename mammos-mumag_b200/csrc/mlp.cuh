@@ -14,8 +14,10 @@
 // The first input layer is one k16 step of the tensor-core product, so the four residual
 // features ride in what would otherwise be zero padding of the twelve.  Inputs are
 // normalised with the model's per-feature mean/scale; the output y gives the correction
-// du_i = sigma * out_scale * y added to u_i (the solve's equation is linear in the
-// residual, so the correction is predicted in units of sigma).
+// du_i = out_scale * y in units of sigma (the solve's equation is linear in the residual).
+// The solve adds alpha du to u with the step alpha = du.r0 / du.S du that minimises the
+// S-norm of the error along du, so a poor prediction cannot make the start worse than
+// the previous potential in that norm.
 #pragma once
 
 #include <cuda_bf16.h>

@@ -407,19 +407,45 @@ __device__ __noinline__ void record_targets(Ctx& c, double sig) {
   END_ROWS
 }
 
-// Learned start of the FP64 solve: u += sigma du; r = r0 - sigma S du; new gamma = r.z, rr.
-__device__ __noinline__ bool learned_start(Ctx& c, const double* x, double sig, double& gamma, double& rr) {
+// Learned start, second half: the network's correction du taken with the step that
+// minimises the S-norm of the error along it (a one-dimensional Galerkin projection):
+// alpha = du.r0 / du.S du, so the start is never worse than u_prev in that norm, whatever
+// the network predicts.  S du goes to a scratch plane (M_inv's, free during evaluations);
+// then u += alpha du and r = r0 - alpha S du on the CTA's own rows.  r0 is the plane
+// `rplane` (FP64); returns the new partial sums through `own`, which the two solves differ in.
+__device__ __forceinline__ bool learned_alpha(Ctx& c, const double* r0, double& alpha) {
   const SolveArgs& a = c.a;
-  const int n = a.Npad;
-  CHECK(learned_pass(c, x, reinterpret_cast<const double*>(a.rec[0]), 1.0 / sig));
-  double pg = 0, pr2 = 0;
+  double* sdu = a.tBd;
+  double p0 = 0, p1 = 0;
   FOR_ROWS(c)
   double sd = 0;
 #pragma unroll 8
   for (int k2 = 0; k2 < w_; ++k2) sd += c.sS[LENTRY(k2)] * (double)a.du[c.scol[LENTRY(k2)]];
+  sdu[i] = sd;
+  const double d = (double)a.du[i];
+  p0 += d * r0[i];
+  p1 += d * sd;
+  END_ROWS
+  double v[2] = {p0, p1};
+  CHECK(grid_reduce<2>(c.sy, v, 0u));
+  alpha = v[1] > 0.0 ? v[0] / v[1] : 0.0;
+  return true;
+}
+
+// Learned start of the FP64 solve: new gamma = r.z, rr.
+__device__ __noinline__ bool learned_start(Ctx& c, const double* x, double sig, double& gamma, double& rr) {
+  const SolveArgs& a = c.a;
+  const int n = a.Npad;
+  const double* r0 = reinterpret_cast<const double*>(a.rec[0]);
+  CHECK(learned_pass(c, x, r0, 1.0 / sig));
+  double alpha;
+  CHECK(learned_alpha(c, r0, alpha));
+  double pg = 0, pr2 = 0;
+  FOR_ROWS(c)
+  (void)w_;
   const PcgRec q = rec_load(a.rec[0], i, n);
-  const double r = q.r - sig * sd;
-  a.u[i] = a.u[i] + sig * (double)a.du[i];
+  const double r = q.r - alpha * a.tBd[i];
+  a.u[i] = a.u[i] + alpha * (double)a.du[i];
   rec_store(a.rec[0], i, n, PcgRec{r, 0.0, 0.0, q.invd});
   pg += r * (r * q.invd);
   pr2 += r * r;
@@ -437,13 +463,13 @@ __device__ __noinline__ bool learned_start_mixed(Ctx& c, const double* x, double
                                                  double& gin) {
   const SolveArgs& a = c.a;
   CHECK(learned_pass(c, x, a.r64, 1.0 / sig));
+  double alpha;
+  CHECK(learned_alpha(c, a.r64, alpha));
   double p0 = 0, p2 = 0, p3 = 0;
   FOR_ROWS(c)
-  double sd = 0;
-#pragma unroll 8
-  for (int k2 = 0; k2 < w_; ++k2) sd += c.sS[LENTRY(k2)] * (double)a.du[c.scol[LENTRY(k2)]];
-  const double r = a.r64[i] - sig * sd;
-  a.u[i] = a.u[i] + sig * (double)a.du[i];
+  (void)w_;
+  const double r = a.r64[i] - alpha * a.tBd[i];
+  a.u[i] = a.u[i] + alpha * (double)a.du[i];
   a.r64[i] = r;
   const float rf = (float)r, inv = (float)__ldg(a.invdS + i);
   a.rec32[0][i] = PcgRec32{rf, 0.f, 0.f, inv};
