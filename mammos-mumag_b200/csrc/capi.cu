@@ -702,6 +702,7 @@ mm_status batch_run(mm_batch* b, const double* h, const mm_solver_params* sp, co
     a.stage_max = b->plan.stage_max[q];
     a.meta_max = b->plan.meta_max[q];
     a.prof = nullptr;
+    a.tc_off = -1;  // batched launches run the network on mma.sync
     b->h_args[q] = a;
     MM_CK(launch_prep(m, b->stream));
   }
@@ -834,6 +835,7 @@ mm_status mm_batch_loop(mm_batch* batch, const mm_loop_params* lp, const mm_solv
       a.stage_max = batch->plan.stage_max[q];
       a.meta_max = batch->plan.meta_max[q];
       a.prof = nullptr;
+      a.tc_off = -1;  // batched launches run the network on mma.sync
       batch->h_args[q] = a;
       MM_CK(launch_prep(m, batch->stream));
     }
@@ -932,7 +934,8 @@ mm_status mm_autotune(mm_mesh* mesh, const mm_solver_params* sp, int32_t* grid_o
   MM_CK(cudaSetDevice(m.device));
   cudaDeviceProp prop;
   MM_CK(cudaGetDeviceProperties(&prop, m.device));
-  const auto key = std::make_tuple(m.h.nslices, m.h.nent, m.vals32 ? 1 : 0, m.device, m.opt.pcg_variant * 4 + m.opt.ctas_per_sm);
+  const auto key = std::make_tuple(m.h.nslices, m.h.nent, (m.vals32 ? 1 : 0) + (m.warm == WARM_LEARNED ? 2 : 0),
+                                   m.device, m.opt.pcg_variant * 4 + m.opt.ctas_per_sm);
   {
     std::lock_guard<std::mutex> lk(g_tune_mu);
     auto it = g_tune_cache.find(key);
@@ -1056,6 +1059,7 @@ mm_status mm_mesh_set_warm_start(mm_mesh* mesh, int32_t mode, const mm_model* mo
     m.mlp = MlpDev{};
   }
   m.warm = mode;
+  solver_configure(m);  // the learned start's network region changes the shared-memory plan
   return MM_OK;
   API_END
 }

@@ -81,6 +81,8 @@ struct SolveArgs {
   MlpDev mlp;           // learned warm start: the model
   float* feat;          // [Npad][kMlpIn] node features of the learned start
   float* du;            // [Npad] its predicted correction (units of sigma)
+  int tc_off;           // >= 0: dynamic shared-memory offset of the tensor-core network's
+                        // region (learned start on tcgen05); -1: the network runs on mma.sync
   // training-sample recording (rec_cap > 0): at a hash-selected 1/rec_stride of the
   // (node, solve) pairs, the node's features at the warm start and, after the solve,
   // the target (u - u0) / sigma
@@ -183,6 +185,7 @@ struct DevMesh {
   int stage = 0;
   int64_t stage_max = 0, meta_max = 0;
   size_t smem = 0;
+  int tc_off = -1;  // SolveArgs::tc_off
 };
 
 // A batched persistent launch over several meshes: mesh q runs on CTAs

@@ -81,17 +81,19 @@ __device__ __forceinline__ void load_b_frag(const __nv_bfloat16* W, int ldk, int
 
 // One hidden layer on a 16-row tile: out = act(A . W^T + b), A as k16 fragments
 // ain[ks][4] (K = 16 * nks), output as k16 fragments aout[8][4] of the 128 outputs.
-// If zout != nullptr the pre-activations are returned in C layout (zout[16][4]).
+// If zout != nullptr the pre-activations are returned in C layout (zout[16][4]).  The 16
+// n-tiles are done four at a time (16 accumulator registers live), which keeps the layer
+// within the register budget of the persistent solver kernel.
 template <int NKS>
 __device__ __forceinline__ void mlp_layer(const uint32_t (&ain)[NKS][4], const __nv_bfloat16* W, const float* b,
                                           int lane, uint32_t (&aout)[8][4], float (*zout)[4] = nullptr) {
   const int t = lane & 3;
 #pragma unroll
-  for (int half = 0; half < 2; ++half) {
-    float acc[8][4];
+  for (int quarter = 0; quarter < 4; ++quarter) {
+    float acc[4][4];
 #pragma unroll
-    for (int j = 0; j < 8; ++j) {
-      const int nt = half * 8 + j;
+    for (int j = 0; j < 4; ++j) {
+      const int nt = quarter * 4 + j;
       const float bl = __ldg(b + nt * 8 + 2 * t), bh = __ldg(b + nt * 8 + 2 * t + 1);
       acc[j][0] = bl;
       acc[j][1] = bh;
@@ -105,18 +107,18 @@ __device__ __forceinline__ void mlp_layer(const uint32_t (&ain)[NKS][4], const _
       }
     }
 #pragma unroll
-    for (int j = 0; j < 8; ++j) {
+    for (int j = 0; j < 4; ++j) {
       if (zout) {
 #pragma unroll
-        for (int q = 0; q < 4; ++q) zout[half * 8 + j][q] = acc[j][q];
+        for (int q = 0; q < 4; ++q) zout[quarter * 4 + j][q] = acc[j][q];
       }
 #pragma unroll
       for (int q = 0; q < 4; ++q) acc[j][q] = gelu_f(acc[j][q]);
     }
-    // n-tiles (2p, 2p+1) of this half form k-step (half*4 + p) of the next layer
+    // n-tiles (2p, 2p+1) of this quarter form k-step (quarter*2 + p) of the next layer
 #pragma unroll
-    for (int p = 0; p < 4; ++p) {
-      const int ks = half * 4 + p;
+    for (int p = 0; p < 2; ++p) {
+      const int ks = quarter * 2 + p;
       aout[ks][0] = pack_bf16(acc[2 * p][0], acc[2 * p][1]);
       aout[ks][1] = pack_bf16(acc[2 * p][2], acc[2 * p][3]);
       aout[ks][2] = pack_bf16(acc[2 * p + 1][0], acc[2 * p + 1][1]);

@@ -28,6 +28,7 @@
 #include <string>
 
 #include "device_mesh.h"
+#include "umma.cuh"
 
 namespace mumag {
 
@@ -183,6 +184,11 @@ struct Ctx {
   long long evals = 0, pcg_iters = 0, minv_iters = 0, shrinks = 0;
   unsigned long long t_phase_start = 0, t_pcg_phase = 0;
   double h;  // applied field of the current field step (mu0 H, T)
+  // the tensor-core network of the learned start (tcsm = its shared-memory region, null when
+  // the network runs on mma.sync), its TMEM columns and mbarrier phase
+  unsigned char* tcsm = nullptr;
+  uint32_t tctm = 0, tcph = 0;
+  bool tcbad = false;
   __device__ Ctx(const SolveArgs& args) : a(args), h(args.h) {}
 };
 
@@ -292,23 +298,42 @@ __device__ __forceinline__ void node_features(const Ctx& c, const double* x, con
   double s0 = m0, s1 = m1, s2 = m2, su = ui, sz = zi;
   double x0 = m0, x1 = m1, x2 = m2, xu = ui, xz = zi, nz = zi;
   int cnt = 1;
-  for (int k = 0; k < w; ++k) {
-    const int j = c.scol[loff + 32 * (int64_t)k];
-    if (j == i) continue;  // the diagonal and the row's padding
-    const double v0 = x[j], v1 = x[n + j], v2 = x[2 * n + j], vu = a.u[j];
-    const double vz = r0[j] * __ldg(a.invdS + j) * isig;
-    s0 += v0;
-    s1 += v1;
-    s2 += v2;
-    su += vu;
-    sz += vz;
-    x0 = fmax(x0, v0);
-    x1 = fmax(x1, v1);
-    x2 = fmax(x2, v2);
-    xu = fmax(xu, vu);
-    xz = fmax(xz, vz);
-    nz = fmin(nz, vz);
-    ++cnt;
+  // four entries at a time: all their gathers are issued before any is used
+  for (int k0 = 0; k0 < w; k0 += 4) {
+    int jj[4];
+    bool use[4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const int k = k0 + q;
+      jj[q] = k < w ? c.scol[loff + 32 * (int64_t)k] : i;
+      use[q] = jj[q] != i;  // the diagonal and the row's padding are the node itself
+    }
+    double v0[4], v1[4], v2[4], vu[4], vz[4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const int j = jj[q];
+      v0[q] = x[j];
+      v1[q] = x[n + j];
+      v2[q] = x[2 * n + j];
+      vu[q] = a.u[j];
+      vz[q] = r0[j] * __ldg(a.invdS + j) * isig;
+    }
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      if (!use[q]) continue;
+      s0 += v0[q];
+      s1 += v1[q];
+      s2 += v2[q];
+      su += vu[q];
+      sz += vz[q];
+      x0 = fmax(x0, v0[q]);
+      x1 = fmax(x1, v1[q]);
+      x2 = fmax(x2, v2[q]);
+      xu = fmax(xu, vu[q]);
+      xz = fmax(xz, vz[q]);
+      nz = fmin(nz, vz[q]);
+      ++cnt;
+    }
   }
   const double ic = 1.0 / cnt;
   f[0] = (float)m0;
@@ -346,6 +371,7 @@ __device__ __noinline__ void mlp_slice(const MlpDev& M, const float* feat, int s
 
 // Learned start, first half: every row's features and the network's correction du (units
 // of sigma), then a barrier so that the residual update can gather du.
+template <bool TC>
 __device__ __noinline__ bool learned_pass(Ctx& c, const double* x, const double* r0, double isig) {
   const SolveArgs& a = c.a;
   FOR_ROWS(c)
@@ -356,9 +382,34 @@ __device__ __noinline__ bool learned_pass(Ctx& c, const double* x, const double*
   dst[1] = make_float4(f[4], f[5], f[6], f[7]);
   dst[2] = make_float4(f[8], f[9], f[10], f[11]);
   dst[3] = make_float4(f[12], f[13], f[14], f[15]);
-  __syncwarp();
-  mlp_slice(a.mlp, a.feat, s_, c.lane, a.du, a.nreal);
+  if (!c.tcsm) {
+    __syncwarp();
+    mlp_slice(a.mlp, a.feat, s_, c.lane, a.du, a.nreal);
+  }
   END_ROWS
+  if constexpr (TC) {
+    if (!c.tcsm) return grid_barrier(c.sy);
+    // the CTA's rows [32 s0, 32 s1) in 128-row tiles on tcgen05
+    __syncthreads();
+    const int rb = 32 * c.s0, re = 32 * c.s1;
+    for (int t0 = rb; t0 < re; t0 += kTcRows) {
+      const bool ok = tc_net_tile(
+          c.tcsm, c.tctm, c.tcph, a.mlp,
+          [&](int r, int col) { return t0 + r < re ? a.feat[(size_t)(t0 + r) * kMlpIn + col] : 0.f; },
+          [&](int r, float v) {
+            const int i = t0 + r;
+            if (i < re) a.du[i] = i < a.nreal ? v : 0.f;
+          });
+      if (!ok) {
+        c.tcbad = true;
+        if (threadIdx.x == 0) {
+          atomicCAS(&a.flags[FLAG_STATUS], 0, (int)MM_TIMEOUT);
+          atomicExch(&a.flags[FLAG_ABORT], 1);
+        }
+        return false;
+      }
+    }
+  }
   return grid_barrier(c.sy);
 }
 
@@ -433,11 +484,12 @@ __device__ __forceinline__ bool learned_alpha(Ctx& c, const double* r0, double& 
 }
 
 // Learned start of the FP64 solve: new gamma = r.z, rr.
+template <bool TC>
 __device__ __noinline__ bool learned_start(Ctx& c, const double* x, double sig, double& gamma, double& rr) {
   const SolveArgs& a = c.a;
   const int n = a.Npad;
   const double* r0 = reinterpret_cast<const double*>(a.rec[0]);
-  CHECK(learned_pass(c, x, r0, 1.0 / sig));
+  CHECK(learned_pass<TC>(c, x, r0, 1.0 / sig));
   double alpha;
   CHECK(learned_alpha(c, r0, alpha));
   double pg = 0, pr2 = 0;
@@ -459,10 +511,11 @@ __device__ __noinline__ bool learned_start(Ctx& c, const double* x, double sig, 
 
 // The same for the mixed-precision solve: FP64 residual r64, FP32 inner record; new
 // rr = r.r, rin2 = rf.rf, gin = rf.zf.
+template <bool TC>
 __device__ __noinline__ bool learned_start_mixed(Ctx& c, const double* x, double sig, double& rr, double& rin2,
                                                  double& gin) {
   const SolveArgs& a = c.a;
-  CHECK(learned_pass(c, x, a.r64, 1.0 / sig));
+  CHECK(learned_pass<TC>(c, x, a.r64, 1.0 / sig));
   double alpha;
   CHECK(learned_alpha(c, a.r64, alpha));
   double p0 = 0, p2 = 0, p3 = 0;
@@ -572,6 +625,7 @@ __device__ __noinline__ bool pcg_loop2(Ctx& c, double alpha, double beta, double
   return true;
 }
 
+template <bool TC>
 __device__ __noinline__ bool pcg_solve(Ctx& c, const double* x) {
   const SolveArgs& a = c.a;
   const double* Dk = plane(a, P_D);
@@ -614,7 +668,7 @@ __device__ __noinline__ bool pcg_solve(Ctx& c, const double* x) {
   const bool recording = a.rec_cap > 0 && sig > 0.0;
   if (recording) record_features(c, x, reinterpret_cast<const double*>(a.rec[0]), 1.0 / sig);
   if (a.warm == WARM_LEARNED && sig > 0.0) {
-    CHECK(learned_start(c, x, sig, gamma, rr));
+    CHECK(learned_start<TC>(c, x, sig, gamma, rr));
     if (!(rr > atol2)) {
       if (recording) record_targets(c, sig);
       return true;
@@ -743,6 +797,7 @@ __device__ __noinline__ bool pcg_inner2(Ctx& c, double alpha, double beta, doubl
   return true;
 }
 
+template <bool TC>
 __device__ __noinline__ bool pcg_solve_mixed(Ctx& c, const double* x) {
   const SolveArgs& a = c.a;
   const double* Dk = plane(a, P_D);
@@ -788,7 +843,7 @@ __device__ __noinline__ bool pcg_solve_mixed(Ctx& c, const double* x) {
   const bool recording = rr > atol2 && a.max_pcg > 0 && a.rec_cap > 0 && sig > 0.0;
   if (recording) record_features(c, x, a.r64, 1.0 / sig);
   if (rr > atol2 && a.max_pcg > 0 && a.warm == WARM_LEARNED && sig > 0.0)
-    CHECK(learned_start_mixed(c, x, sig, rr, rin2, gin));
+    CHECK(learned_start_mixed<TC>(c, x, sig, rr, rin2, gin));
   for (int outer = 0; rr > atol2 && k < a.max_pcg && outer < 32; ++outer) {
     const double inner_tol2 = fmax(1e-10 * rin2, 0.25 * atol2);  // 1e-5 relative, or the outer target
     double gamma = gin, delta;
@@ -884,9 +939,10 @@ struct EvalOut {
 // Energy and gradient at x (all CTAs' x complete).  Writes gout = projected gradient and
 // gf = full gradient; u is the PCG solution (warm-started from the previous u).  Extras:
 // gd = gout.d (d may be null), dxinf = max|x - xref|, xinf = max|x|, ginf = max|gout|.
+template <bool TC>
 __device__ bool eval(Ctx& c, const double* x, const double* xref, const double* d, double* gout, EvalOut& o) {
   const SolveArgs& a = c.a;
-  if (a.hmag_on > 0) CHECK(a.mixed ? pcg_solve_mixed(c, x) : pcg_solve(c, x));
+  if (a.hmag_on > 0) CHECK(a.mixed ? pcg_solve_mixed<TC>(c, x) : pcg_solve<TC>(c, x));
   const int n = a.Npad;
   const double* G = plane(a, P_G);
   const int64_t ps = a.nent;
@@ -1094,6 +1150,7 @@ __device__ bool minv(Ctx& c, const double* g, const double* mb, double* zout) {
 // ---------------------------------------------------------------------------------------
 // hestenes_stiefel_ncg + line_search, scripts/minimizers.py:16-190
 // ---------------------------------------------------------------------------------------
+template <bool TC>
 __device__ __noinline__ bool minimize(Ctx& c, double& f_out, double& mh_out, long long& k_out) {
   const SolveArgs& a = c.a;
   const int n = a.Npad;
@@ -1106,7 +1163,7 @@ __device__ __noinline__ bool minimize(Ctx& c, double& f_out, double& mh_out, lon
   const double tol = a.tol_fun;
   double f0 = DBL_MAX;
   EvalOut o;
-  CHECK(eval(c, x, x, nullptr, g, o));
+  CHECK(eval<TC>(c, x, x, nullptr, g, o));
   double f = o.E, dxinf = 0.0, xinf = o.xinf, ginf = o.ginf;
   CHECK(minv(c, g, a.mbar_current ? x : a.mbar, a.zp));
   FOR_ROWS(c)
@@ -1160,7 +1217,7 @@ __device__ __noinline__ bool minimize(Ctx& c, double& f_out, double& mh_out, lon
     const double t2 = sqrt_eps / dinf;
     const double hh = t1 < t2 ? t1 : t2;
     CHECK(step_normalize(c, x1, x, hh, d));
-    CHECK(eval(c, x1, x, d, g1, o));
+    CHECK(eval<TC>(c, x1, x, d, g1, o));
     double alpha;
     {  // alpha_init, scripts/minimizers.py:34-57
       double a1 = -hh * (gd / (o.gd - gd));
@@ -1170,7 +1227,7 @@ __device__ __noinline__ bool minimize(Ctx& c, double& f_out, double& mh_out, lon
       alpha = (a1 < 0.99 * a2) ? a1 : a2;
     }
     CHECK(step_normalize(c, x1, x, alpha, d));
-    CHECK(eval(c, x1, x, d, g1, o));
+    CHECK(eval<TC>(c, x1, x, d, g1, o));
     const double eps_k = 1e-6 * fabs(f);
     for (int ls = 0;; ++ls) {
       const bool wolfe = ((2.0 * 0.1 - 1.0) * gd >= o.gd) && (o.E <= f + eps_k);
@@ -1178,7 +1235,7 @@ __device__ __noinline__ bool minimize(Ctx& c, double& f_out, double& mh_out, lon
       alpha *= 0.5;
       c.shrinks += 1;
       CHECK(step_normalize(c, x1, x, alpha, d));
-      CHECK(eval(c, x1, x, d, g1, o));
+      CHECK(eval<TC>(c, x1, x, d, g1, o));
     }
     // direction update
     CHECK(minv(c, g1, a.mbar_current ? x : a.mbar, a.zp));
@@ -1279,6 +1336,7 @@ __device__ __noinline__ bool minimize(Ctx& c, double& f_out, double& mh_out, lon
 // a.sw_nmax steps, the cumulative field update and the snapshot counter of the reference
 // (no snapshots are written).  Rows [counter, hext, mh, E] and per-step counters
 // [ncg, evals, pcg, shrinks, minv, ns, sync ns, barriers] go to a.sw_rec / a.sw_stat.
+template <bool TC>
 __device__ bool sweep(Ctx& c) {
   const SolveArgs& a = c.a;
   double mh = DBL_MAX, last_saved = DBL_MAX, counter = 0.0, hext = a.h;
@@ -1289,7 +1347,7 @@ __device__ bool sweep(Ctx& c) {
     c.h = hext;
     double f;
     long long k;
-    CHECK(minimize(c, f, mh, k));
+    CHECK(minimize<TC>(c, f, mh, k));
     if (!(f - f == 0.0)) return true;  // non-finite energy: status set, the sweep stops
     if ((last_saved - mh) > a.sw_mstep) {
       counter += 1.0;
@@ -1319,6 +1377,7 @@ __device__ bool sweep(Ctx& c) {
 
 // One field step (or one evaluation / M_inv application) of one mesh, run by a group of
 // nblk CTAs of which this is number blk.
+template <bool TC>
 __device__ __forceinline__ void solve_body(const SolveArgs& args, int nblk, int blk, unsigned char* smem) {
   if (args.mode == MODE_IDLE) return;
   Ctx c(args);
@@ -1373,10 +1432,17 @@ __device__ __forceinline__ void solve_body(const SolveArgs& args, int nblk, int 
     c.scol = args.col;
     c.cbase = 0;
   }
+  if constexpr (TC) {
+    if (args.warm == WARM_LEARNED && args.tc_off >= 0 && blockDim.x == kTcThreads &&
+        (args.mode == MODE_EVAL || args.mode == MODE_MINIMIZE || args.mode == MODE_SWEEP)) {
+      c.tcsm = smem + args.tc_off;
+      c.tctm = tc_net_setup(c.tcsm, args.mlp);
+    }
+  }
   bool ok = true;
   if (args.mode == MODE_EVAL) {
     EvalOut o;
-    ok = eval(c, args.x, args.x, nullptr, args.g, o);
+    ok = eval<TC>(c, args.x, args.x, nullptr, args.g, o);
     if (ok && blk == 0 && threadIdx.x == 0) {
       args.resd[0] = o.E;
       if (!(o.E - o.E == 0.0)) atomicCAS(&args.flags[FLAG_STATUS], 0, (int)MM_NONFINITE);
@@ -1384,11 +1450,11 @@ __device__ __forceinline__ void solve_body(const SolveArgs& args, int nblk, int 
   } else if (args.mode == MODE_MINV) {
     ok = minv(c, args.g, args.mbar_current ? args.x : args.mbar, args.zp);
   } else if (args.mode == MODE_SWEEP) {
-    ok = sweep(c);
+    ok = sweep<TC>(c);
   } else {
     double f, mh;
     long long k;
-    ok = minimize(c, f, mh, k);
+    ok = minimize<TC>(c, f, mh, k);
   }
   if (ok && blk == 0 && threadIdx.x == 0) {
     args.resi[1] = c.evals;
@@ -1398,6 +1464,9 @@ __device__ __forceinline__ void solve_body(const SolveArgs& args, int nblk, int 
     args.resi[5] = (long long)(globaltimer() - t_start);  // kernel ns (CTA 0)
     args.resi[6] = (long long)c.sy.t_sync;                // of which in grid barriers
     args.resi[7] = (long long)c.sy.epoch;                 // grid barriers executed
+  }
+  if constexpr (TC) {
+    if (c.tcsm) tc_net_teardown(c.tcsm, c.tctm, c.tcbad, c.tcph);
   }
   if (args.prof && threadIdx.x == 0) {
     long long* p = args.prof + 4 * blk;
@@ -1411,10 +1480,10 @@ __device__ __forceinline__ void solve_body(const SolveArgs& args, int nblk, int 
 // The persistent kernel is built for two and for three resident CTAs per SM (128 or 80
 // registers per thread); the three-CTA build hides more memory latency on large meshes, the
 // two-CTA build spills less on small ones.  mm_autotune picks one per mesh.
-template <int MB>
+template <int MB, bool TC>
 __global__ void __launch_bounds__(256, MB) k_solve(const __grid_constant__ SolveArgs args) {
   extern __shared__ __align__(16) unsigned char smem[];
-  solve_body(args, gridDim.x, blockIdx.x, smem);
+  solve_body<TC>(args, gridDim.x, blockIdx.x, smem);
 }
 
 // Batched persistent launch: mesh q owns CTAs [group[q], group[q+1]); each group runs its
@@ -1428,7 +1497,7 @@ __global__ void __launch_bounds__(256, 2) k_solve_batch(const SolveArgs* __restr
     const int mid = (lo + hi) / 2;
     if (group[mid] <= (int)blockIdx.x) lo = mid; else hi = mid;
   }
-  solve_body(args[lo], group[lo + 1] - group[lo], (int)blockIdx.x - group[lo], smem);
+  solve_body<false>(args[lo], group[lo + 1] - group[lo], (int)blockIdx.x - group[lo], smem);
 }
 
 }  // namespace
@@ -1440,8 +1509,9 @@ struct StagePlan {
   int stage;
   int64_t stage_max, meta_max;
   size_t smem;
+  int extra_off;  // offset of the extra region, -1 = none
 };
-StagePlan stage_plan(const DevMesh& m, int grid, size_t limit) {
+StagePlan stage_plan(const DevMesh& m, int grid, size_t limit, size_t extra = 0) {
   int64_t emax = 0, smax = 0;
   for (int b = 0; b < grid; ++b) {
     const int64_t s0 = (m.h.nslices * b) / grid, s1 = (m.h.nslices * (b + 1)) / grid;
@@ -1451,13 +1521,27 @@ StagePlan stage_plan(const DevMesh& m, int grid, size_t limit) {
   const size_t meta = (size_t)smax * (sizeof(int64_t) + sizeof(int32_t));
   const size_t need = (size_t)emax * (sizeof(double) + sizeof(int32_t) + (m.vals32 ? sizeof(float) : 0));
   StagePlan p;
-  p.stage = (need + meta + 16 <= limit) ? 1 : 0;
+  p.stage = (need + meta + 16 + (extra ? extra + 1024 : 0) <= limit) ? 1 : 0;
   p.stage_max = emax;
   p.meta_max = smax;
   p.smem = (p.stage ? ((need + 15) & ~(size_t)15) : 0) + meta;
+  p.extra_off = -1;
+  if (extra) {  // the tensor-core network's region, 1024-byte aligned, after the metadata
+    p.extra_off = (int)((p.smem + 1023) & ~(size_t)1023);
+    p.smem = (size_t)p.extra_off + extra;
+  }
   return p;
 }
 }  // namespace
+
+// The persistent kernel a mesh's launches use: the build for its resident CTAs per SM, or,
+// when the learned start's network has a shared-memory region, the build with the tcgen05
+// network (a kernel that allocates tensor memory is resident once per SM).
+using SolveKernel = void (*)(SolveArgs);
+SolveKernel solve_kernel(const DevMesh& m) {
+  if (m.tc_off >= 0) return k_solve<2, true>;
+  return m.kernel_mb == 3 ? k_solve<3, false> : k_solve<2, false>;
+}
 
 void solver_configure(DevMesh& m) {
   int dev = m.device;
@@ -1475,23 +1559,27 @@ void solver_configure(DevMesh& m) {
   grid = std::max(1, std::min(grid, kMaxGrid));
   grid = (int)std::min<int64_t>(grid, m.h.nslices);
   const size_t limit = (size_t)prop.sharedMemPerBlockOptin - 16 * 1024;  // room for static smem
-  const StagePlan sp = stage_plan(m, grid, limit);
+  // The learned start's network runs on tcgen05 from its own shared-memory region (256-thread
+  // CTAs) when the launch has at most one CTA per SM anyway; larger launches, whose CTAs
+  // share SMs, would lose residency to the region and keep the network on mma.sync.
+  const size_t extra =
+      (m.warm == WARM_LEARNED && block == kTcThreads && grid <= prop.multiProcessorCount) ? (size_t)kSmTc : 0;
+  const StagePlan sp = stage_plan(m, grid, limit, extra);
   m.stage = sp.stage;
   m.stage_max = sp.stage_max;
   m.meta_max = sp.meta_max;
   m.smem = sp.smem;
+  m.tc_off = sp.extra_off;
   // The attribute is per kernel, shared by every mesh: raise it to the device limit once
   // (occupancy follows each launch's actual request).
-  if (cudaFuncSetAttribute(k_solve<2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                           (int)(prop.sharedMemPerBlockOptin - 16 * 1024)) != cudaSuccess ||
-      cudaFuncSetAttribute(k_solve<3>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                           (int)(prop.sharedMemPerBlockOptin - 16 * 1024)) != cudaSuccess)
+  const int dsm = (int)(prop.sharedMemPerBlockOptin - 16 * 1024);
+  if (cudaFuncSetAttribute(k_solve<2, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, dsm) != cudaSuccess ||
+      cudaFuncSetAttribute(k_solve<3, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, dsm) != cudaSuccess ||
+      cudaFuncSetAttribute(k_solve<2, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, dsm) != cudaSuccess)
     throw std::runtime_error("cannot reserve shared memory for the solver kernel");
   if (m.kernel_mb != 2 && m.kernel_mb != 3) m.kernel_mb = 2;
   int occ = 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, m.kernel_mb == 3 ? k_solve<3> : k_solve<2>, block, m.smem) !=
-          cudaSuccess ||
-      occ < 1)
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, solve_kernel(m), block, m.smem) != cudaSuccess || occ < 1)
     throw std::runtime_error("persistent solver kernel cannot be resident with " + std::to_string(block) +
                              " threads per CTA");
   grid = std::min(grid, occ * prop.multiProcessorCount);
@@ -1624,6 +1712,7 @@ SolveArgs solver_args(const DevMesh& m, int mode, double h, const mm_solver_para
   a.e32 = m.e32;
   a.r64 = m.r64;
   a.pcg2 = m.pcg2;
+  a.tc_off = m.tc_off;
   a.bar_stall = m.bar_stall;
   a.warm = m.warm;
   a.nreal = (int32_t)m.h.N;
@@ -1684,7 +1773,7 @@ cudaError_t solver_launch(DevMesh& m, const SolveArgs& a) {
   cfg.attrs = attr;
   cfg.numAttrs = 1;
   if (m.evk0 && (e = cudaEventRecord(m.evk0, m.stream)) != cudaSuccess) return e;
-  e = m.kernel_mb == 3 ? cudaLaunchKernelEx(&cfg, k_solve<3>, a) : cudaLaunchKernelEx(&cfg, k_solve<2>, a);
+  e = cudaLaunchKernelEx(&cfg, solve_kernel(m), a);
   if (e != cudaSuccess) return e;
   return m.evk1 ? cudaEventRecord(m.evk1, m.stream) : cudaSuccess;
 }

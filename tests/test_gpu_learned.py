@@ -121,3 +121,31 @@ def test_learned_start_fewer_pcg_iterations(small_experiment):
     print(f"PCG iterations per solve: previous-u {prev:.2f}, zero {zero:.2f}, learned {lrn:.2f}")
     assert prev < zero
     assert lrn < prev
+
+
+def test_learned_start_tensor_core_path_matches_mma_sync_path():
+    """The learned start runs its network on tcgen05 when the launch has at most one CTA per
+    SM (100 CTAs here) and on mma.sync otherwise (200 CTAs of the three-CTA-per-SM build):
+    same solve, the warm start differing only by the network's rounding."""
+    X, T, tag, krn, m0 = synthetic.multigrain(n=20, L=25.0, grains=3, cone_deg=20.0, gb=2.0, seed=9)
+    rng = np.random.default_rng(3)
+    feats = rng.standard_normal((4096, 16)).astype(np.float32)
+    model, _ = learned.train(feats, (0.1 * feats[:, 12]).astype(np.float32), epochs=2)
+    sp = _native.solver_params(hdir=[0.0, 0.0, 1.0])
+    m1 = m0.reshape(-1, 3) + 0.05 * rng.standard_normal((len(m0) // 3, 3))
+    m1 = (m1 / np.linalg.norm(m1, axis=1, keepdims=True)).ravel()
+    out = {}
+    for grid, mb in ((100, 2), (200, 3)):
+        with _native.Mesh(X, T, tag, krn, grid_ctas=grid, ctas_per_sm=mb) as M:
+            assert M.info()["grid_ctas"] == grid
+            M.set_warm_start(_native.WARM_LEARNED, model)
+            M.set_state(m0, None, m0)
+            M.energy_grad(0.3, sp)
+            M.set_state(m1, M.get_state()[1], m0)
+            E, g, it = M.energy_grad(0.3, sp)
+            out[grid] = (E, M.get_state()[1], it)
+    (Ea, ua, ia), (Eb, ub, ib) = out[100], out[200]
+    assert abs(ia - ib) <= 2
+    assert np.abs(ua - ub).max() <= 1e-8 * np.abs(ua).max()
+    assert Ea == pytest.approx(Eb, rel=1e-10)
+    model.close()
