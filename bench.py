@@ -48,11 +48,11 @@ L2_FLUSH_BYTES = 256 << 20
 # DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) per algorithmic byte of one
 # k_solve field-step launch of the multigrain workload, from one ncu --set full capture of
 # each path (python -m mammos_mumag.perfcase field-step ...): the FP64 launch moved
-# 124.3 MB for 5,422 MB of algorithmic bytes, the learned+mixed launch 579.2 MB for
-# 4,146 MB.  The bench scales the ratio to its own average launch (traffic grows with the
-# work counters the algorithmic bytes are computed from).
+# 124.3 MB for 5,422 MB of algorithmic bytes, the learned+mixed launch (network on
+# tcgen05) 394.1 MB for 4,123 MB.  The bench scales the ratio to its own average launch
+# (traffic grows with the work counters the algorithmic bytes are computed from).
 TRAFFIC_PER_ALGORITHMIC_BYTE = {("multigrain", "fp64"): 124.3 / 5422.4,
-                                ("multigrain", "learned_mixed"): 579.2 / 4145.9}
+                                ("multigrain", "learned_mixed"): 394.1 / 4122.6}
 
 
 def batch_workload(count: int = 64, seed: int = 0):
