@@ -452,14 +452,14 @@ def run_b200(args, world, rank, local):
         dist_barrier(world)
         return dist_max(total_ms, world), nfs, steps_all, rows
 
-    configs = {"fp64": (_native.PREC_FP64, _native.WARM_PREVIOUS)}
+    paths = {"fp64": (_native.PREC_FP64, _native.WARM_PREVIOUS)}
     if not args.no_mixed:
-        configs["mixed"] = (_native.PREC_MIXED, _native.WARM_PREVIOUS)
+        paths["mixed"] = (_native.PREC_MIXED, _native.WARM_PREVIOUS)
     if use_learned:
-        configs["learned_mixed"] = (_native.PREC_MIXED, _native.WARM_LEARNED)
+        paths["learned_mixed"] = (_native.PREC_MIXED, _native.WARM_LEARNED)
     variants, raw = {}, {}
     clk = None
-    for name, (prec, warm) in configs.items():
+    for name, (prec, warm) in paths.items():
         msh = make_mesh(prec, warm)
         info = msh.info()
         if name == headline:
@@ -501,7 +501,7 @@ def run_b200(args, world, rank, local):
     peak = float(peaks.get("hbm_gbs", 6650.0))
     ratio = TRAFFIC_PER_ALGORITHMIC_BYTE.get((args.workload, headline))
     traffic = ratio * ab / launches if ratio is not None else None
-    prec_h, warm_h = configs[headline]
+    prec_h, warm_h = paths[headline]
     # e2e: the public API from host buffers (pinned), every step: mesh build + upload,
     # warm-start set-up, state upload, sweep, result read-back
     pin = {k: torch.from_numpy(np.ascontiguousarray(v)).pin_memory() for k, v in
