@@ -539,35 +539,37 @@ __device__ __noinline__ bool learned_start_mixed(Ctx& c, const double* x, double
 }
 
 // One row of an SpMV over the staged pattern, sum_k val[k] z[col[k]] in entry order, with
-// the next 8 entries' columns and values loaded while the current 8 gather z: two
+// the next CH entries' columns and values loaded while the current CH gather z: two
 // dependent memory round trips (column, then z) overlap across chunks.  w is the slice's
 // width, the same for the warp's 32 lanes, so the guards do not diverge.
-template <class VT, class ZT, class AT>
+constexpr int kChunk32 = 8;  // FP32 gather chunk (16 measured slower: fewer resident warps)
+
+template <class VT, class ZT, class AT, int CH>
 __device__ __forceinline__ AT gather_row(const Ctx& c, const VT* sval, int64_t loff, int w, const ZT* z) {
   AT acc = 0;
-  int jc[8];
-  VT vc[8];
+  int jc[CH];
+  VT vc[CH];
 #pragma unroll
-  for (int q = 0; q < 8; ++q) {
+  for (int q = 0; q < CH; ++q) {
     const bool in = q < w;
     jc[q] = in ? c.scol[loff + 32 * (int64_t)q] : 0;
     vc[q] = in ? sval[loff + 32 * (int64_t)q] : VT(0);
   }
-  for (int k0 = 0; k0 < w; k0 += 8) {
-    int jn[8];
-    VT vn[8];
+  for (int k0 = 0; k0 < w; k0 += CH) {
+    int jn[CH];
+    VT vn[CH];
 #pragma unroll
-    for (int q = 0; q < 8; ++q) {
-      const int k = k0 + 8 + q;
+    for (int q = 0; q < CH; ++q) {
+      const int k = k0 + CH + q;
       const bool in = k < w;
       jn[q] = in ? c.scol[loff + 32 * (int64_t)k] : 0;
       vn[q] = in ? sval[loff + 32 * (int64_t)k] : VT(0);
     }
 #pragma unroll
-    for (int q = 0; q < 8; ++q)
+    for (int q = 0; q < CH; ++q)
       if (k0 + q < w) acc += vc[q] * (AT)z[jc[q]];
 #pragma unroll
-    for (int q = 0; q < 8; ++q) {
+    for (int q = 0; q < CH; ++q) {
       jc[q] = jn[q];
       vc[q] = vn[q];
     }
@@ -607,7 +609,7 @@ __device__ __noinline__ bool pcg_loop2(Ctx& c, double alpha, double beta, double
     END_ROWS
     CHECK(grid_barrier(c.sy));
     FOR_ROWS(c)
-    const double acc = gather_row<double, double, double>(c, c.sS, loff_, w_, z);
+    const double acc = gather_row<double, double, double, 8>(c, c.sS, loff_, w_, z);
     rec_store_w(rc, i, n, acc);
     pd += acc * z[i];
     END_ROWS
@@ -781,7 +783,7 @@ __device__ __noinline__ bool pcg_inner2(Ctx& c, double alpha, double beta, doubl
     END_ROWS
     CHECK(grid_barrier(c.sy));
     FOR_ROWS(c)
-    const float acc = gather_row<float, float, float>(c, c.sS32, loff_, w_, z);
+    const float acc = gather_row<float, float, float, kChunk32>(c, c.sS32, loff_, w_, z);
     rc[i].w = acc;
     pd += (double)acc * (double)z[i];
     END_ROWS
