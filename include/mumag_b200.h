@@ -210,8 +210,9 @@ mm_status mm_loop(mm_mesh* mesh, const mm_loop_params* lp, const mm_solver_param
  * the kernel built for two resident CTAs per SM at one, one and a half and two CTAs per SM,
  * the build for three at two and three per SM -- each with both PCG arrangements unless
  * options.pcg_variant fixes one, and keeps the fastest; u and the full gradient are
- * restored.  Results are cached per mesh shape, precision and pcg_variant option for the
- * process.  *grid_out (may be NULL) receives the CTA count chosen. */
+ * restored.  Results are cached per mesh shape, precision, warm-start kind and the
+ * pcg_variant / ctas_per_sm options for the process.  *grid_out (may be NULL) receives the
+ * CTA count chosen. */
 mm_status mm_autotune(mm_mesh* mesh, const mm_solver_params* sp, int32_t* grid_out);
 
 /* ---- batched persistent launch ----------------------------------------------------------
@@ -301,7 +302,10 @@ mm_status mm_model_train(mm_model* model, const float* feats, const float* targe
 mm_status mm_model_predict(mm_model* model, const float* feats, int64_t n, float* y);
 
 /* Warm start of the mesh's Poisson solves: the reference's previous u (default), zero, or
- * the learned correction of the previous u (model required; it must outlive its use). */
+ * the learned correction of the previous u (model required; it must outlive its use).
+ * With the learned start and a launch of at most one CTA per SM the network runs on
+ * tcgen05 from its own shared-memory region (the launch shape is re-planned here; run
+ * mm_autotune after this call to tune for it); larger launches run it on mma.sync. */
 typedef enum { MM_WARM_PREVIOUS = 0, MM_WARM_ZERO = 1, MM_WARM_LEARNED = 2 } mm_warm_mode;
 mm_status mm_mesh_set_warm_start(mm_mesh* mesh, int32_t mode, const mm_model* model);
 
