@@ -13,9 +13,16 @@
 // CTA sums in the same fixed order, so every CTA sees bit-identical scalars and takes the
 // same branches: the control flow of the reference runs redundantly in all CTAs.
 //
-// Two algebraic rewrites save one grid barrier per inner iteration; both are exact in
-// exact arithmetic: the PCG keeps q = S p up to date as q <- S z + beta q, and the
-// truncated CG keeps B d as B d <- -B z + beta B d.
+// Algebraic rewrites, exact in exact arithmetic, cut grid barriers per inner iteration:
+// the Poisson PCG runs in the Chronopoulos-Gear form (s = S p kept as s <- w + beta s, both
+// inner products from one reduction) with either one barrier per iteration (neighbours' z
+// recomputed from their gathered r, w, s) or two (z stored, gathered alone; large meshes);
+// the truncated CG keeps B d as B d <- -B z + beta B d.
+//
+// Modes: one energy evaluation, one M_inv application, one field step, or (MODE_SWEEP, the
+// batched loop) a whole field sweep.  The learned warm start of the Poisson solve runs a
+// small network over the nodes before the PCG, on tcgen05 in the kernel instantiation that
+// has a shared-memory region for it, on mma.sync otherwise.
 //
 // Every wait on another CTA is bounded; on timeout the kernel records MM_TIMEOUT, raises
 // the abort flag and all CTAs return.
