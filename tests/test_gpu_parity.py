@@ -200,3 +200,33 @@ def test_synthetic_multigrain_loop_matches_oracle():
     # loop tolerance from the NCG stopping rule (see test_field_step_matches_oracle)
     np.testing.assert_allclose(rows[:, 2], rows_o[:, 2], rtol=2e-5)
     np.testing.assert_allclose(rows[:, 3], rows_o[:, 3], rtol=1e-8)
+
+
+def test_diagnostic_energies_match_reference_kats(cube_mesh, golden, energies):
+    """The reference's diagnostic known-answer energies (tests/data/hmag, exani, external of
+    the reference, E_gradient columns) reproduced by the GPU path on the 20 nm cube in its
+    shell: magnetostatic (uniform +z), exchange + anisotropy (vortex and uniform), Zeeman.
+    Terms are isolated by switching the magnetostatic term and the field off."""
+    X, T, tag = cube_mesh
+    krn = O.read_krn_rows((golden / "loop_cube.krn").read_text())
+    P = O.Problem(X, T, tag, krn)
+    par = O.read_params(energies["p2"]["external"])
+    mu = O.initial_m_uniform(P, [0.0, 0.0, 1.0])
+    mv, _ = O.vortex_m(P)
+    on, off = _native.solver_params(hmag_on=1), _native.solver_params(hmag_on=0)
+    with _native.Mesh(X, T, tag, krn) as M:
+        def energy(m, h, sp):
+            M.set_state(m, None, m)
+            return M.energy_grad(h, sp)[0] / O.MU0_OUT
+
+        e_hmag = energy(mu, 0.0, on) - energy(mu, 0.0, off)
+        e_vortex = energy(mv, 0.0, off)
+        e_uniform = energy(mu, 0.0, off)
+        mz = O.initial_m_uniform(P, par["m"])
+        h = par["hstart"] - par["hstep"]  # scripts/external.py:105
+        sp_h = _native.solver_params(hdir=par["hdir"], hmag_on=0)
+        e_zeeman = energy(mz, h, sp_h) - energy(mz, 0.0, sp_h)
+    assert e_hmag == pytest.approx(energies["hmag"]["E_gradient"], rel=1e-9)
+    assert e_vortex == pytest.approx(energies["exani_vortex"]["E_gradient"], rel=1e-11)
+    assert e_uniform == pytest.approx(energies["exani_uniform"]["E_gradient"], rel=1e-11)
+    assert e_zeeman == pytest.approx(energies["external"]["E_gradient"], rel=1e-9)
