@@ -63,6 +63,9 @@ typedef struct {
                           give the same iterates */
   int ctas_per_sm;     /* build of the persistent kernel: 0 = chosen by mm_autotune (2 until
                           then), 2 or 3 resident CTAs per SM (128 or 80 registers per thread) */
+  int stage_operators; /* 1 (default): each CTA keeps its SELL columns and Poisson values in
+                          shared memory when they fit; 0: always read them from HBM (the
+                          large-mesh path, selectable on any mesh; results are identical) */
 } mm_options;
 
 /* Solver settings of one field step (scripts/tools.py:64-120, scripts/minimizers.py:140-190). */
@@ -107,6 +110,7 @@ typedef struct {
   int32_t pcg_variant;                 /* PCG arrangement in use: 1 one-sync, 2 two-sync */
   int32_t kernel_ctas_per_sm;          /* build of the persistent kernel in use: 2 or 3 resident
                                           CTAs per SM (128 or 80 registers per thread) */
+  int32_t staged;                      /* 1: SELL columns + Poisson values in shared memory */
 } mm_mesh_info;
 
 /* Field-sweep parameters (the .p2 [field] section; scripts/loop.py:71-142). */

@@ -202,6 +202,7 @@ void mm_default_options(mm_options* opt) {
   opt->reorder = 1;
   opt->pcg_variant = 0;
   opt->ctas_per_sm = 0;
+  opt->stage_operators = 1;
 }
 
 void mm_default_solver_params(mm_solver_params* sp) {
@@ -264,6 +265,8 @@ mm_status mm_mesh_create(const double* X, int64_t N, const int32_t* T, const int
   if (o.pcg_variant < 0 || o.pcg_variant > 2) throw std::runtime_error("options.pcg_variant must be 0, 1 or 2");
   if (o.ctas_per_sm != 0 && o.ctas_per_sm != 2 && o.ctas_per_sm != 3)
     throw std::runtime_error("options.ctas_per_sm must be 0, 2 or 3");
+  if (o.stage_operators != 0 && o.stage_operators != 1)
+    throw std::runtime_error("options.stage_operators must be 0 or 1");
   for (int64_t i = 0; i < 3 * N; ++i)
     if (!std::isfinite(X[i])) throw std::runtime_error("non-finite node coordinate");
   int ndev = 0;
@@ -414,6 +417,7 @@ mm_status mm_mesh_get_info(const mm_mesh* mesh, mm_mesh_info* info) {
   info->bandwidth_after = (double)m.h.bandwidth_after;
   info->pcg_variant = m.pcg2 ? 2 : 1;
   info->kernel_ctas_per_sm = m.kernel_mb;
+  info->staged = m.stage;
   return MM_OK;
   API_END
 }
@@ -935,7 +939,7 @@ mm_status mm_autotune(mm_mesh* mesh, const mm_solver_params* sp, int32_t* grid_o
   cudaDeviceProp prop;
   MM_CK(cudaGetDeviceProperties(&prop, m.device));
   const auto key = std::make_tuple(m.h.nslices, m.h.nent, (m.vals32 ? 1 : 0) + (m.warm == WARM_LEARNED ? 2 : 0),
-                                   m.device, m.opt.pcg_variant * 4 + m.opt.ctas_per_sm);
+                                   m.device, (m.opt.pcg_variant * 4 + m.opt.ctas_per_sm) * 2 + m.opt.stage_operators);
   {
     std::lock_guard<std::mutex> lk(g_tune_mu);
     auto it = g_tune_cache.find(key);

@@ -1520,7 +1520,7 @@ struct StagePlan {
   size_t smem;
   int extra_off;  // offset of the extra region, -1 = none
 };
-StagePlan stage_plan(const DevMesh& m, int grid, size_t limit, size_t extra = 0) {
+StagePlan stage_plan(const DevMesh& m, int grid, size_t limit, size_t extra = 0, bool allow_stage = true) {
   int64_t emax = 0, smax = 0;
   for (int b = 0; b < grid; ++b) {
     const int64_t s0 = (m.h.nslices * b) / grid, s1 = (m.h.nslices * (b + 1)) / grid;
@@ -1530,7 +1530,7 @@ StagePlan stage_plan(const DevMesh& m, int grid, size_t limit, size_t extra = 0)
   const size_t meta = (size_t)smax * (sizeof(int64_t) + sizeof(int32_t));
   const size_t need = (size_t)emax * (sizeof(double) + sizeof(int32_t) + (m.vals32 ? sizeof(float) : 0));
   StagePlan p;
-  p.stage = (need + meta + 16 + (extra ? extra + 1024 : 0) <= limit) ? 1 : 0;
+  p.stage = (allow_stage && need + meta + 16 + (extra ? extra + 1024 : 0) <= limit) ? 1 : 0;
   p.stage_max = emax;
   p.meta_max = smax;
   p.smem = (p.stage ? ((need + 15) & ~(size_t)15) : 0) + meta;
@@ -1573,7 +1573,7 @@ void solver_configure(DevMesh& m) {
   // share SMs, would lose residency to the region and keep the network on mma.sync.
   const size_t extra =
       (m.warm == WARM_LEARNED && block == kTcThreads && grid <= prop.multiProcessorCount) ? (size_t)kSmTc : 0;
-  const StagePlan sp = stage_plan(m, grid, limit, extra);
+  const StagePlan sp = stage_plan(m, grid, limit, extra, m.opt.stage_operators != 0);
   m.stage = sp.stage;
   m.stage_max = sp.stage_max;
   m.meta_max = sp.meta_max;
@@ -1652,7 +1652,7 @@ void batch_configure(const std::vector<DevMesh*>& ms, BatchPlan& plan) {
   plan.smem = 0;
   for (int q = 0; q < count; ++q) {
     plan.group[q + 1] = plan.group[q] + g[q];
-    const StagePlan sp = stage_plan(*ms[q], g[q], limit);
+    const StagePlan sp = stage_plan(*ms[q], g[q], limit, 0, ms[q]->opt.stage_operators != 0);
     plan.stage[q] = sp.stage;
     plan.stage_max[q] = sp.stage_max;
     plan.meta_max[q] = sp.meta_max;

@@ -93,6 +93,7 @@ class Options(C.Structure):
         ("reorder", C.c_int),
         ("pcg_variant", C.c_int),
         ("ctas_per_sm", C.c_int),
+        ("stage_operators", C.c_int),
     ]
 
 
@@ -146,6 +147,7 @@ class MeshInfo(C.Structure):
         ("bandwidth_after", C.c_double),
         ("pcg_variant", C.c_int32),
         ("kernel_ctas_per_sm", C.c_int32),
+        ("staged", C.c_int32),
     ]
 
     def as_dict(self):
@@ -342,7 +344,7 @@ class Mesh:
     """Device operators of one mesh (an ``mm_mesh`` handle)."""
 
     def __init__(self, X, T, tag, materials, size=1e-9, dirichlet_rhs=0, precision=PREC_FP64, device=0,
-                 grid_ctas=0, block_threads=0, reorder=1, pcg_variant=0, ctas_per_sm=0):
+                 grid_ctas=0, block_threads=0, reorder=1, pcg_variant=0, ctas_per_sm=0, stage_operators=1):
         lib = load()
         self.X = np.ascontiguousarray(X, dtype=np.float64)
         self.T = np.ascontiguousarray(T, dtype=np.int32)
@@ -352,7 +354,8 @@ class Mesh:
         mats = (Material * max(1, len(rows)))(*[Material(*r) for r in rows])
         opt = default_options(size=size, dirichlet_rhs=dirichlet_rhs, precision=precision, device=device,
                               grid_ctas=grid_ctas, block_threads=block_threads, reorder=reorder,
-                              pcg_variant=pcg_variant, ctas_per_sm=ctas_per_sm)
+                              pcg_variant=pcg_variant, ctas_per_sm=ctas_per_sm,
+                              stage_operators=stage_operators)
         h = C.c_void_p()
         check(lib.mm_mesh_create(_dp(self.X), self.N, self.T.ctypes.data_as(_I32), self.tag.ctypes.data_as(_I32),
                                  self.E, mats, len(rows), C.byref(opt), C.byref(h)))

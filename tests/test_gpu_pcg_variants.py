@@ -58,3 +58,30 @@ def test_autotune_reports_a_variant():
         M.set_state(m0, None, m0)
         M.autotune(_native.solver_params(hdir=[0.0, 0.0, 1.0]))
         assert M.info()["pcg_variant"] in (1, 2) and M.info()["kernel_ctas_per_sm"] in (2, 3)
+
+
+@pytest.mark.parametrize("precision", [_native.PREC_FP64, _native.PREC_MIXED])
+@pytest.mark.parametrize("variant", [1, 2])
+def test_streamed_operators_match_staged(precision, variant):
+    """Operators read from HBM (the path of meshes too large for shared memory) give the
+    field step of operators staged in shared memory: same data, same arithmetic order, so
+    the same numbers.  Four CTAs, so that every warp walks several slices."""
+    X, T, tag, krn, m0 = synthetic.multigrain(n=12, L=20.0, grains=3, cone_deg=20.0, gb=2.0, seed=14)
+    sp = _native.solver_params(hdir=[0.0, 0.0, 1.0])
+    res = {}
+    for stage in (1, 0):
+        with _native.Mesh(X, T, tag, krn, precision=precision, pcg_variant=variant, ctas_per_sm=3, grid_ctas=4,
+                          stage_operators=stage) as M:
+            assert M.info()["staged"] == stage
+            M.set_state(m0, None, m0)
+            E, g, it = M.energy_grad(0.5, sp)
+            r = M.minimize(-1.0, sp)
+            m, u, _ = M.get_state()
+            res[stage] = (E, g, it, r, m, u)
+    a, b = res[1], res[0]
+    assert a[2] == b[2] and a[3]["pcg_iters"] == b[3]["pcg_iters"] and a[3]["evals"] == b[3]["evals"]
+    assert a[0] == pytest.approx(b[0], rel=1e-14)
+    assert np.abs(a[1] - b[1]).max() <= 1e-13 * np.abs(a[1]).max()
+    assert a[3]["energy"] == pytest.approx(b[3]["energy"], rel=1e-14)
+    assert np.abs(a[4] - b[4]).max() <= 1e-13
+    assert np.abs(a[5] - b[5]).max() <= 1e-13 * np.abs(a[5]).max()
