@@ -560,7 +560,6 @@ def run_b200(args, world, rank, local):
                          "algorithmic_bytes_per_launch": ab / launches,
                          "avg_launch_ms": kernel_ms / launches,
                          "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)" if peaks else "fallback"},
-            "sync_fraction": sum(st["sync_ns"] for st in steps_all) / max(1, sum(st["kernel_ns"] for st in steps_all)),
             "cpu_baseline": cpu,
             "e2e": {"value": e2e_n * world / e2e_t, "unit": UNIT, "h2d_bytes_per_step": int(h2d),
                     "d2h_bytes_per_step": int(d2h)},
