@@ -48,12 +48,12 @@ L2_FLUSH_BYTES = 256 << 20
 # DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) per algorithmic byte of one
 # k_solve field-step launch, from one ncu capture of each workload and path
 # (python -m mammos_mumag.perfcase field-step ...): the multigrain FP64 launch moved
-# 124.3 MB for 5,422 MB of algorithmic bytes, the multigrain learned+mixed launch (network
-# on tcgen05) 394.1 MB for 4,123 MB, the large mesh's FP64 launch 178.3 GB for 162.8 GB.
+# 133.8 MB for 5,422 MB of algorithmic bytes, the multigrain learned+mixed launch (network
+# on tcgen05) 406.5 MB for 4,128 MB, the large mesh's FP64 launch 178.3 GB for 162.8 GB.
 # The bench scales the ratio to its own average launch (traffic grows with the work
 # counters the algorithmic bytes are computed from).
-TRAFFIC_PER_ALGORITHMIC_BYTE = {("multigrain", "fp64"): 124.3 / 5422.4,
-                                ("multigrain", "learned_mixed"): 394.1 / 4122.6,
+TRAFFIC_PER_ALGORITHMIC_BYTE = {("multigrain", "fp64"): 133.8 / 5422.4,
+                                ("multigrain", "learned_mixed"): 406.5 / 4128.4,
                                 ("large", "fp64"): 178.3 / 162.8}
 
 

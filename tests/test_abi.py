@@ -61,3 +61,13 @@ def test_no_device_is_reported_without_gpu():
     with pytest.raises(_native.NativeError) as ei:
         _native.Mesh(X, T, np.ones(len(T), np.int32), [[0, 0, 1e6, 0, 1.0, 1e-11]])
     assert ei.value.status == _native.MM_NO_DEVICE
+
+
+@pytest.mark.parametrize("opt", [dict(stage_operators=2), dict(ctas_per_sm=4), dict(pcg_variant=3)])
+def test_bad_options_are_rejected(opt):
+    """Option values outside their range are refused before any device work (so also here)."""
+    X, T = synthetic.cube_grid(2, 4.0)
+    with pytest.raises(_native.NativeError) as ei:
+        _native.Mesh(X, T, np.ones(len(T), np.int32), [[0, 0, 1e6, 0, 1.0, 1e-11]], **opt)
+    assert ei.value.status == _native.MM_BAD_INPUT
+    assert next(iter(opt)) in str(ei.value)
