@@ -18,32 +18,52 @@ namespace mumag {
 
 namespace {
 
-// Undirected node graph (no self loops), CSR with sorted unique neighbours.
 struct Graph {
   std::vector<int64_t> off;
   std::vector<int32_t> adj;
 };
 
+// Undirected node graph, CSR with sorted unique neighbours.  A node is its own neighbour
+// only if an element lists it twice.  Built from the node -> element incidence with a
+// per-node marker, so every node's list is gathered once and only its ~14 distinct
+// neighbours are sorted.
 Graph node_graph(int64_t N, const int32_t* T, int64_t E) {
+  std::vector<int64_t> eoff(N + 1, 0);
+  for (int64_t k = 0; k < 4 * E; ++k) eoff[T[k] + 1]++;
+  for (int64_t i = 0; i < N; ++i) eoff[i + 1] += eoff[i];
+  std::vector<int64_t> inc(4 * E);
+  {
+    std::vector<int64_t> pos(eoff.begin(), eoff.end() - 1);
+    for (int64_t e = 0; e < E; ++e)
+      for (int a = 0; a < 4; ++a) inc[pos[T[4 * e + a]]++] = e;
+  }
   Graph g;
-  std::vector<int64_t> cnt(N + 1, 0);
-  for (int64_t e = 0; e < E; ++e)
-    for (int a = 0; a < 4; ++a) cnt[T[4 * e + a] + 1] += 3;
-  for (int64_t i = 0; i < N; ++i) cnt[i + 1] += cnt[i];
-  std::vector<int32_t> tmp(cnt[N]);
-  std::vector<int64_t> pos(cnt.begin(), cnt.end() - 1);
-  for (int64_t e = 0; e < E; ++e)
-    for (int a = 0; a < 4; ++a)
-      for (int b = 0; b < 4; ++b)
-        if (a != b) tmp[pos[T[4 * e + a]]++] = T[4 * e + b];
   g.off.assign(N + 1, 0);
-  g.adj.reserve(tmp.size() / 3);
+  g.adj.reserve(static_cast<size_t>(eoff[N]) / 2);
+  std::vector<int64_t> mark(N, -1);
+  std::vector<int32_t> nb;
   for (int64_t i = 0; i < N; ++i) {
-    auto* b = tmp.data() + cnt[i];
-    auto* en = tmp.data() + cnt[i + 1];
-    std::sort(b, en);
-    auto* u = std::unique(b, en);
-    g.adj.insert(g.adj.end(), b, u);
+    nb.clear();
+    mark[i] = i;  // the node itself, unless an element repeats it
+    for (int64_t k = eoff[i]; k < eoff[i + 1]; ++k) {
+      const int32_t* t = T + 4 * inc[k];
+      int self = 0;
+      for (int a = 0; a < 4; ++a) {
+        const int32_t j = t[a];
+        if (j == i) {
+          ++self;
+        } else if (mark[j] != i) {
+          mark[j] = i;
+          nb.push_back(j);
+        }
+      }
+      if (self > 1 && mark[i] == i) {
+        mark[i] = -2;  // listed twice: a self loop, once
+        nb.push_back(static_cast<int32_t>(i));
+      }
+    }
+    std::sort(nb.begin(), nb.end());
+    g.adj.insert(g.adj.end(), nb.begin(), nb.end());
     g.off[i + 1] = static_cast<int64_t>(g.adj.size());
   }
   return g;
@@ -83,11 +103,8 @@ int bfs_levels(const Graph& g, int32_t r, std::vector<int32_t>& level, std::vect
   return depth;
 }
 
-}  // namespace
-
-std::vector<int32_t> rcm_order(int64_t N, const int32_t* T, int64_t E) {
-  validate(N, T, E);
-  Graph g = node_graph(N, T, E);
+// Reverse Cuthill-McKee order of graph g: order[new] = old.
+std::vector<int32_t> rcm_of_graph(const Graph& g, int64_t N) {
   std::vector<int32_t> deg(N);
   for (int64_t i = 0; i < N; ++i) deg[i] = static_cast<int32_t>(g.off[i + 1] - g.off[i]);
   std::vector<char> seen(N, 0);
@@ -132,6 +149,13 @@ std::vector<int32_t> rcm_order(int64_t N, const int32_t* T, int64_t E) {
   return order;  // order[new] = old
 }
 
+}  // namespace
+
+std::vector<int32_t> rcm_order(int64_t N, const int32_t* T, int64_t E) {
+  validate(N, T, E);
+  return rcm_of_graph(node_graph(N, T, E), N);
+}
+
 int32_t greedy_colour(int64_t N, const int32_t* T, int64_t E, const int64_t* order, int32_t* colour) {
   constexpr int kWords = 8;  // up to 512 colours
   std::vector<uint64_t> used(static_cast<size_t>(N) * kWords, 0);
@@ -158,42 +182,50 @@ void preprocess(const double* X, int64_t N, const int32_t* T, const int32_t* tag
   h.N = N;
   h.E = E;
   // ---- element tags -> material rows (scripts/materials.py:22-25)
-  h.tags.assign(tag, tag + E);
-  std::sort(h.tags.begin(), h.tags.end());
-  h.tags.erase(std::unique(h.tags.begin(), h.tags.end()), h.tags.end());
+  // sorted unique tags: a mesh has few, so a sorted insert beats sorting all E of them
+  h.tags.clear();
+  for (int64_t e = 0; e < E; ++e) {
+    if (e > 0 && tag[e] == tag[e - 1]) continue;
+    auto it = std::lower_bound(h.tags.begin(), h.tags.end(), tag[e]);
+    if (it == h.tags.end() || *it != tag[e]) h.tags.insert(it, tag[e]);
+  }
   if (static_cast<int32_t>(h.tags.size()) > nmats)
     throw std::runtime_error("materials file has " + std::to_string(nmats) + " rows for " +
                              std::to_string(h.tags.size()) + " element tags");
   // ---- node order
+  const Graph g = node_graph(N, T, E);
   if (reorder) {
-    h.perm = rcm_order(N, T, E);
+    h.perm = rcm_of_graph(g, N);
   } else {
     h.perm.resize(N);
     std::iota(h.perm.begin(), h.perm.end(), 0);
   }
   h.iperm.assign(N, 0);
   for (int64_t i = 0; i < N; ++i) h.iperm[h.perm[i]] = static_cast<int32_t>(i);
-  // ---- node-pair pattern in device order
-  Graph g = node_graph(N, T, E);
+  // ---- node-pair pattern in device order: row inew = itself and its neighbours, sorted
   h.nslices = (N + kSlice - 1) / kSlice;
   h.Npad = h.nslices * kSlice;
   h.rowlen.assign(h.Npad, 0);
-  std::vector<std::vector<int32_t>> rows(N);
-  h.nnz = 0;
+  std::vector<int64_t> roff(N + 1, 0);
   for (int64_t inew = 0; inew < N; ++inew) {
-    int32_t iold = h.perm[inew];
-    auto& r = rows[inew];
-    r.reserve(g.off[iold + 1] - g.off[iold] + 1);
-    r.push_back(static_cast<int32_t>(inew));
+    const int32_t iold = h.perm[inew];
+    roff[inew + 1] = roff[inew] + (g.off[iold + 1] - g.off[iold]) + 1;
+  }
+  std::vector<int32_t> rows(roff[N]);
+  h.nnz = roff[N];
+  for (int64_t inew = 0; inew < N; ++inew) {
+    const int32_t iold = h.perm[inew];
+    int32_t* r = rows.data() + roff[inew];
+    int32_t* w = r;
+    *w++ = static_cast<int32_t>(inew);
     for (int64_t k = g.off[iold]; k < g.off[iold + 1]; ++k) {
-      int32_t jnew = h.iperm[g.adj[k]];
-      r.push_back(jnew);
+      const int32_t jnew = h.iperm[g.adj[k]];
+      *w++ = jnew;
       h.bandwidth_before = std::max<int64_t>(h.bandwidth_before, std::llabs(int64_t(g.adj[k]) - iold));
       h.bandwidth_after = std::max<int64_t>(h.bandwidth_after, std::llabs(int64_t(jnew) - inew));
     }
-    std::sort(r.begin(), r.end());
-    h.rowlen[inew] = static_cast<int32_t>(r.size());
-    h.nnz += static_cast<int64_t>(r.size());
+    std::sort(r, w);
+    h.rowlen[inew] = static_cast<int32_t>(w - r);
   }
   h.sl_off.assign(h.nslices + 1, 0);
   h.sl_w.assign(h.nslices, 0);
@@ -210,21 +242,26 @@ void preprocess(const double* X, int64_t N, const int32_t* T, const int32_t* tag
       int64_t i = s * kSlice + l;
       for (int32_t k = 0; k < h.sl_w[s]; ++k) {
         int32_t c = static_cast<int32_t>(i);  // padding entries point at the row itself
-        if (i < N && k < h.rowlen[i]) c = rows[i][k];
+        if (i < N && k < h.rowlen[i]) c = rows[roff[i] + k];
         h.col[h.sl_off[s] + static_cast<int64_t>(k) * kSlice + l] = c;
       }
     }
-  rows.clear();
-  rows.shrink_to_fit();
+  rows = std::vector<int32_t>();
   // ---- elements: device node ids, colour classes sorted by first node (locality)
   std::vector<int32_t> cn(4 * E);
   for (int64_t k = 0; k < 4 * E; ++k) cn[k] = h.iperm[T[k]];
+  // elements by their smallest device node id, ties in input order (a stable counting sort)
   std::vector<int64_t> eorder(E);
-  std::iota(eorder.begin(), eorder.end(), 0);
-  std::vector<int32_t> emin(E);
-  for (int64_t e = 0; e < E; ++e)
-    emin[e] = std::min(std::min(cn[4 * e], cn[4 * e + 1]), std::min(cn[4 * e + 2], cn[4 * e + 3]));
-  std::stable_sort(eorder.begin(), eorder.end(), [&](int64_t a, int64_t b) { return emin[a] < emin[b]; });
+  {
+    std::vector<int32_t> emin(E);
+    std::vector<int64_t> cnt(N + 1, 0);
+    for (int64_t e = 0; e < E; ++e) {
+      emin[e] = std::min(std::min(cn[4 * e], cn[4 * e + 1]), std::min(cn[4 * e + 2], cn[4 * e + 3]));
+      cnt[emin[e] + 1]++;
+    }
+    for (int64_t i = 0; i < N; ++i) cnt[i + 1] += cnt[i];
+    for (int64_t e = 0; e < E; ++e) eorder[cnt[emin[e]]++] = e;
+  }
   std::vector<int32_t> colour(E);
   int32_t ncol = greedy_colour(N, cn.data(), E, eorder.data(), colour.data());
   std::vector<int64_t> byc(E);
@@ -241,10 +278,17 @@ void preprocess(const double* X, int64_t N, const int32_t* T, const int32_t* tag
   }
   h.econn.resize(4 * E);
   h.etag.resize(E);
-  for (int64_t q = 0; q < E; ++q) {
-    int64_t e = byc[q];
-    for (int a = 0; a < 4; ++a) h.econn[4 * q + a] = cn[4 * e + a];
-    h.etag[q] = static_cast<int32_t>(std::lower_bound(h.tags.begin(), h.tags.end(), tag[e]) - h.tags.begin());
+  {
+    std::vector<int32_t> tix(E);  // tag index of every element, in input order
+    for (int64_t e = 0; e < E; ++e)
+      tix[e] = (e > 0 && tag[e] == tag[e - 1])
+                   ? tix[e - 1]
+                   : static_cast<int32_t>(std::lower_bound(h.tags.begin(), h.tags.end(), tag[e]) - h.tags.begin());
+    for (int64_t q = 0; q < E; ++q) {
+      const int64_t e = byc[q];
+      for (int a = 0; a < 4; ++a) h.econn[4 * q + a] = cn[4 * e + a];
+      h.etag[q] = tix[e];
+    }
   }
   // ---- coordinates in device order
   h.Xd.assign(3 * h.Npad, 0.0);
