@@ -5,7 +5,9 @@
 ``<name>_stats.txt`` and ``info.json`` there -- but runs the loop in process on the GPU
 (``mammos_mumag.runner``) instead of ``run-escript scripts/loop.py <name>``.  Failures raise
 ``RuntimeError("Simulation has failed. ...")`` as the reference's subprocess wrapper does
-(``simulation.py:437-458``).
+(``simulation.py:437-458``).  ``run_exani``, ``run_external`` and ``run_hmag`` run the
+reference's energy known-answer scripts the same way (``mammos_mumag.diagnostics``); the
+other escript-only scripts raise ``NotImplementedError``.
 """
 
 from __future__ import annotations
@@ -15,7 +17,7 @@ import json
 import pathlib
 
 import mammos_mumag
-from mammos_mumag import fly, runner
+from mammos_mumag import diagnostics, fly, runner
 from mammos_mumag.materials import Materials
 from mammos_mumag.parameters import Parameters
 from mammos_mumag.tools import check_dir
@@ -70,8 +72,15 @@ class Simulation:
         outdir = check_dir(outdir)
         b200 = {k: v for k, v in (("precision", precision), ("dirichlet_rhs", dirichlet_rhs), ("mbar", mbar)) if v}
         self._write_inputs(outdir, name, b200)
+        self._run(runner.run_loop, outdir, name, m0=m0, device=device)
+
+    @staticmethod
+    def _run(fn, outdir, name, **kw):
+        """Run one script replacement in ``outdir``; failures raise as the reference's
+        subprocess wrapper does (``simulation.py:437-458``), and ``info.json`` is written as
+        its ``run_script`` writes it (``simulation.py:114-140``)."""
         try:
-            runner.run_loop(outdir, name, m0=m0, device=device)
+            fn(outdir, name, **kw)
         except Exception as e:
             raise RuntimeError(f"Simulation has failed. Exit with error: \n{e}") from e
         with open(outdir / "info.json", "w") as f:
@@ -80,19 +89,38 @@ class Simulation:
                 "mammos_mumag_version": mammos_mumag.__version__,
             }, f)
 
+    def _write_mesh_krn(self, outdir, name):
+        self.check_attribute("mesh_filepath", "materials")
+        fly.copy_as_fly(self.mesh_filepath, outdir / f"{name}.fly")
+        self.materials.write_krn(outdir / f"{name}.krn")
+
     def _out_of_scope(self, what):
         raise NotImplementedError(
             f"run_{what} is an escript diagnostic of the reference and is not part of the B200 hysteresis path"
         )
 
-    def run_exani(self, outdir="exani", name="out"):
-        self._out_of_scope("exani")
+    def run_exani(self, outdir="exani", name="out", device=0):
+        """Exchange energy density of the test vortex and anisotropy energy density of the
+        uniform state (the reference's ``exani`` script, on the GPU path): writes
+        ``<name>.fly``, ``<name>.krn``, ``<name>_vortex.csv`` and ``<name>_uniform.csv``."""
+        outdir = check_dir(outdir)
+        self._write_mesh_krn(outdir, name)
+        self._run(diagnostics.run_exani, outdir, name, device=device)
 
-    def run_external(self, outdir="external", name="out"):
-        self._out_of_scope("external")
+    def run_external(self, outdir="external", name="out", device=0):
+        """Zeeman energy density (the reference's ``external`` script, on the GPU path):
+        writes ``<name>.fly``, ``<name>.krn``, ``<name>.p2`` and ``<name>.csv``."""
+        outdir = check_dir(outdir)
+        self._write_inputs(outdir, name)
+        self._run(diagnostics.run_external, outdir, name, device=device)
 
-    def run_hmag(self, outdir="hmag", name="out"):
-        self._out_of_scope("hmag")
+    def run_hmag(self, outdir="hmag", name="out", device=0):
+        """Magnetostatic energy density and field of the uniform +z state (the reference's
+        ``hmag`` script, on the GPU path): writes ``<name>.fly``, ``<name>.krn``,
+        ``<name>.csv`` and ``<name>_hmag.vtu``."""
+        outdir = check_dir(outdir)
+        self._write_mesh_krn(outdir, name)
+        self._run(diagnostics.run_hmag, outdir, name, device=device)
 
     def run_magnetization(self, outdir="magnetization", name="out"):
         self._out_of_scope("magnetization")

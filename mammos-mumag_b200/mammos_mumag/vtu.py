@@ -17,7 +17,9 @@ def _fmt(a: np.ndarray, ncomp: int) -> str:
     return "\n".join(fmt % tuple(r) for r in a.tolist()) + "\n"
 
 
-def write_vtu(path, X, T, tag, point_data: dict, time=0.0, cycle=0) -> None:
+def write_vtu(path, X, T, tag, point_data: dict, time=0.0, cycle=0, cell_data: dict | None = None) -> None:
+    """Point data arrays of N x ncomp values; cell data ``tags`` and, optionally, further
+    arrays of E x ncomp values (``cell_data``)."""
     X = np.asarray(X)
     T = np.asarray(T)
     n, e = X.shape[0], T.shape[0]
@@ -47,13 +49,21 @@ def write_vtu(path, X, T, tag, point_data: dict, time=0.0, cycle=0) -> None:
         out.append("</DataArray>\n")
     out.append('</PointData>\n<CellData>\n<DataArray Name="tags" type="Float64" NumberOfComponents="1" format="ascii">\n')
     out.append(_fmt(np.asarray(tag, dtype=np.float64), 1))
-    out.append("</DataArray>\n</CellData>\n</Piece>\n</UnstructuredGrid>\n</VTKFile>\n")
+    out.append("</DataArray>\n")
+    for name, arr in (cell_data or {}).items():
+        arr = np.asarray(arr, dtype=np.float64)
+        nc = arr.size // e
+        out.append(f'<DataArray Name="{name}" type="Float64" NumberOfComponents="{nc}" format="ascii">\n')
+        out.append(_fmt(arr, nc))
+        out.append("</DataArray>\n")
+    out.append("</CellData>\n</Piece>\n</UnstructuredGrid>\n</VTKFile>\n")
     with open(path, "w") as f:
         f.write("".join(out))
 
 
 def read_point_data(path, names=("m", "u")) -> dict:
-    """Point-data arrays of an ASCII ``.vtu`` written by this module or by weipa."""
+    """Named data arrays (point or cell data) of an ASCII ``.vtu`` written by this module or
+    by weipa."""
     text = open(path).read()
     res = {}
     for name in names:
