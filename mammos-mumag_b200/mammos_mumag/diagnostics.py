@@ -12,7 +12,11 @@ known-answer scripts of the reference, run in the directory that holds ``<name>.
 * ``hmag`` (``scripts/hmag.py:119-165``): magnetostatic energy density of the uniform +z
   state from the field, from the gradient and analytically (``Js^2 / 6 mu0``); writes
   ``<name>.csv`` and ``<name>_hmag.vtu`` (point data ``m``, ``U``, ``h_nodes``; cell data
-  ``tags``, ``h``).
+  ``tags``, ``h``);
+* ``mapping`` (``scripts/mapping.py:20-131, 238-295``): the same four energies and the total
+  energy of the ``.p2`` initial state at ``mu0 Hext = hstart - hstep``; writes
+  ``<name>_{zeeman,exchange,anisotropy,hmag,energy}.csv`` (rows named ``E_jax`` as in the
+  reference's tables, the values from this library) and ``<name>_stats.txt``.
 
 The energies from the gradient are evaluations of ``total_eg`` by the library
 (``mm_energy_grad``) with the other terms switched off: the exchange + anisotropy energy
@@ -194,3 +198,63 @@ def run_hmag(workdir, name, device=0) -> dict:
     vtu.write_vtu(wd / f"{name}_hmag.vtu", X, T, tag, {"m": m, "U": u, "h_nodes": h_nodes},
                   cell_data={"h": h_cells})
     return {"E_field": ef, "E_gradient": eg, "E_analytic": ea}
+
+
+def run_mapping(workdir, name, device=0) -> dict:
+    """``scripts/mapping.py:238-295`` with its checks (``:20-131``): writes
+    ``<name>_zeeman.csv``, ``<name>_exchange.csv``, ``<name>_anisotropy.csv``,
+    ``<name>_hmag.csv``, ``<name>_energy.csv`` and ``<name>_stats.txt``.  The total energy's
+    analytic row is the sum of the Zeeman, exchange + anisotropy and magnetostatic energies
+    of the checks on the initial state (the reference's table holds that sum)."""
+    import time
+
+    wd = pathlib.Path(workdir)
+    par = runner.read_script_params(wd / f"{name}.p2")
+    t0 = time.perf_counter()
+    X, T, tag, krn, mesh = _open(wd, name, device)
+    value = par["hstart"] - par["hstep"]  # scripts/mapping.py:26
+    try:
+        meas, V = mesh.meas()
+        m = runner.initial_m(X, meas, par["m"], par["state_id"])
+        off = _native.solver_params(hdir=par["hdir"], hmag_on=0)
+        on = _native.solver_params(hdir=par["hdir"], hmag_on=1, tol_u=1e-10)  # scripts/mapping.py:107
+        e_c = _energy(mesh, m, 0.0, off)  # exchange + anisotropy of the initial state
+        e_zee = _energy(mesh, m, value, off) - e_c
+        mv, k = vortex_m(X, meas, V)
+        e_vortex = _energy(mesh, mv, 0.0, off)
+        e_hmag = _energy(mesh, m, 0.0, on) - e_c
+        t1 = time.perf_counter()
+        full = _native.solver_params(hdir=par["hdir"], hmag_on=par["hmag_on"], tol_u=par["tol_u"])
+        e_total = _energy(mesh, m, value, full)
+        t2 = time.perf_counter()
+    finally:
+        mesh.close()
+    mdir, hdir, js, A = par["m"], par["hdir"], krn[0][4], krn[0][5]
+    uniform = [0.0, 0.0, 1.0]
+    rows = {
+        "zeeman": (f"Zeeman energy density for an external field of mu_0 Hext {value} (T).", e_zee / MU0_OUT,
+                   -js * value * (mdir[0] * hdir[0] + mdir[1] * hdir[1] + mdir[2] * hdir[2]) / MU0_OUT),
+        "exchange": ("Exchange energy density of a vortex on a, b plane.", e_vortex / MU0_OUT,
+                     (2 * k * k * MU0_OUT * A / (SIZE * SIZE)) / MU0_OUT),
+        "anisotropy": ("Magnetocrystalline anisotropy energy density of uniformly magnetized sample in direction "
+                       f"{uniform}.", e_c / MU0_OUT, anisotropy_energy(krn[0], uniform) / MU0_OUT),
+        "hmag": ("Magnetostatic energy density of uniformly magnetized cube.", e_hmag / MU0_OUT,
+                 (js * js / 6) / MU0_OUT),
+        "energy": ("Total energy density of uniformly magnetized state.", e_total / MU0_OUT,
+                   (e_zee + e_c + e_hmag) / MU0_OUT),
+    }
+    out = {}
+    for key, (title, e_num, e_ana) in rows.items():
+        write_csv(wd / f"{name}_{key}.csv", title, [
+            ("E_jax", e_num, "Energy evaluated with jax backend (J/m^3)."),
+            ("E_analytic", e_ana, "Energy evaluated analytically (J/m^3)."),
+        ])
+        out[key] = {"E_jax": e_num, "E_analytic": e_ana}
+    (wd / f"{name}_stats.txt").write_text("\n".join([
+        "MAP FINITE ELEMENT BACKEND TO THE B200 LIBRARY.",
+        "Timing and statistics.",
+        f"set-up and checks: {t1 - t0}",
+        f"elapsed time: {t2 - t1}",
+        "function_calls: 1",
+    ]))
+    return out

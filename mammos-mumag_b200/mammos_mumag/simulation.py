@@ -5,9 +5,9 @@
 ``<name>_stats.txt`` and ``info.json`` there -- but runs the loop in process on the GPU
 (``mammos_mumag.runner``) instead of ``run-escript scripts/loop.py <name>``.  Failures raise
 ``RuntimeError("Simulation has failed. ...")`` as the reference's subprocess wrapper does
-(``simulation.py:437-458``).  ``run_exani``, ``run_external`` and ``run_hmag`` run the
-reference's energy known-answer scripts the same way (``mammos_mumag.diagnostics``); the
-other escript-only scripts raise ``NotImplementedError``.
+(``simulation.py:437-458``).  ``run_exani``, ``run_external``, ``run_hmag`` and
+``run_mapping`` run the reference's energy known-answer scripts the same way
+(``mammos_mumag.diagnostics``); the other escript-only scripts raise ``NotImplementedError``.
 """
 
 from __future__ import annotations
@@ -125,8 +125,14 @@ class Simulation:
     def run_magnetization(self, outdir="magnetization", name="out"):
         self._out_of_scope("magnetization")
 
-    def run_mapping(self, outdir="magnetization", name="out"):
-        self._out_of_scope("mapping")
+    def run_mapping(self, outdir="magnetization", name="out", device=0):
+        """Energy checks and the total energy of the initial state (the reference's
+        ``mapping`` script, on the GPU path): writes ``<name>.fly``, ``<name>.krn``,
+        ``<name>.p2``, ``<name>_{zeeman,exchange,anisotropy,hmag,energy}.csv`` and
+        ``<name>_stats.txt``."""
+        outdir = check_dir(outdir)
+        self._write_inputs(outdir, name)
+        self._run(diagnostics.run_mapping, outdir, name, device=device)
 
     def run_materials(self, outdir="materials", name="out"):
         self._out_of_scope("materials")

@@ -108,3 +108,23 @@ def test_vortex_and_analytic_helpers(cube_mesh, energies):
     assert k == ko and np.array_equal(m, mo)
     ea = diagnostics.anisotropy_energy(krn[0], [0.0, 0.0, 1.0]) / diagnostics.MU0_OUT
     assert ea == pytest.approx(energies["exani_uniform"]["E_analytic"], rel=1e-15)
+
+
+def test_mapping_tables(sim, tmp_path, energies):
+    """The mapping script's five tables.  The reference's values came from float32 JAX; its
+    own test compares with np.allclose, which FP64 values meet; the FP64 rows also match
+    the FP64 diagnostics (exani, external, hmag) of the same reference run."""
+    sim.run_mapping(outdir=tmp_path / "mapping")
+    for key, gold in energies["mapping"].items():
+        out = diagnostics.read_csv(tmp_path / "mapping" / f"out_{key}.csv")
+        assert set(out) == set(gold)
+        for k, v in gold.items():
+            assert np.allclose(out[k], v), (key, k)
+    d = {k: diagnostics.read_csv(tmp_path / "mapping" / f"out_{k}.csv") for k in energies["mapping"]}
+    assert d["anisotropy"]["E_jax"] == pytest.approx(energies["exani_uniform"]["E_gradient"], rel=1e-11)
+    assert d["exchange"]["E_jax"] == pytest.approx(energies["exani_vortex"]["E_gradient"], rel=1e-11)
+    assert d["zeeman"]["E_jax"] == pytest.approx(energies["external"]["E_gradient"], rel=1e-9)
+    assert d["hmag"]["E_jax"] == pytest.approx(energies["hmag"]["E_gradient"], rel=1e-9)
+    tot = d["zeeman"]["E_jax"] + d["anisotropy"]["E_jax"] + d["hmag"]["E_jax"]
+    assert d["energy"]["E_jax"] == pytest.approx(tot, rel=1e-9)
+    assert (tmp_path / "mapping" / "out_stats.txt").exists()

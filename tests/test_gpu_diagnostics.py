@@ -1,4 +1,4 @@
-"""The reference's energy known-answer scripts (exani, external, hmag) through
+"""The reference's energy known-answer scripts (exani, external, hmag, mapping) through
 ``Simulation.run_*`` on the GPU path, compared with the tables the reference itself wrote
 (tests/data/{exani,external,hmag}/*.csv of the reference; the reference's tests compare them
 with np.allclose, the bounds here are tighter)."""
@@ -47,3 +47,17 @@ def test_hmag_on_gpu(sim, tmp_path, cube_mesh, energies):
     X, T, tag = cube_mesh
     d = diagnostics.vtu.read_point_data(tmp_path / "hmag" / "out_hmag.vtu", ("U", "h_nodes", "h"))
     assert d["U"].size == len(X) and d["h_nodes"].size == 3 * len(X) and d["h"].size == 3 * len(T)
+
+
+def test_mapping_on_gpu(sim, tmp_path, energies):
+    """The mapping tables (the reference's are float32 JAX: np.allclose, its own bound; the
+    FP64 rows also against the FP64 known answers of the other scripts)."""
+    sim.run_mapping(outdir=tmp_path / "mapping")
+    d = {k: diagnostics.read_csv(tmp_path / "mapping" / f"out_{k}.csv") for k in energies["mapping"]}
+    for key, gold in energies["mapping"].items():
+        for k, v in gold.items():
+            assert np.allclose(d[key][k], v), (key, k)
+    assert d["anisotropy"]["E_jax"] == pytest.approx(energies["exani_uniform"]["E_gradient"], rel=1e-11)
+    assert d["exchange"]["E_jax"] == pytest.approx(energies["exani_vortex"]["E_gradient"], rel=1e-11)
+    assert d["zeeman"]["E_jax"] == pytest.approx(energies["external"]["E_gradient"], rel=1e-9)
+    assert d["hmag"]["E_jax"] == pytest.approx(energies["hmag"]["E_gradient"], rel=1e-9)
