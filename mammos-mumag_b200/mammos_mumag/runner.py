@@ -158,9 +158,26 @@ def run_loop(workdir, name, m0=None, device=0, grid_ctas=0, block_threads=0, ret
     return (out, steps) if return_steps else out
 
 
+SCRIPTS = ("loop", "exani", "external", "hmag", "mapping")
+
+
+def run_script(script, workdir, name, device=0):
+    """The in-process counterpart of ``run-escript scripts/<script>.py <name>`` for the
+    scripts this build provides: the loop (:func:`run_loop`) and the energy known-answer
+    scripts (``mammos_mumag.diagnostics``)."""
+    if script == "loop":
+        return run_loop(workdir, name, device=device)
+    if script not in SCRIPTS:
+        raise ValueError(f"script {script!r} is not provided (one of {', '.join(SCRIPTS)})")
+    from . import diagnostics
+
+    return getattr(diagnostics, f"run_{script}")(workdir, name, device=device)
+
+
 if __name__ == "__main__":
     import sys
 
-    if len(sys.argv) < 2:
-        sys.exit("usage: python -m mammos_mumag.runner modelname   (in the directory of modelname.*)")
-    run_loop(".", sys.argv[1])
+    if len(sys.argv) < 2 or len(sys.argv) > 3:
+        sys.exit("usage: python -m mammos_mumag.runner modelname [" + "|".join(SCRIPTS) + "]"
+                 "   (in the directory of modelname.*; default loop)")
+    run_script(sys.argv[2] if len(sys.argv) == 3 else "loop", ".", sys.argv[1])

@@ -128,3 +128,18 @@ def test_mapping_tables(sim, tmp_path, energies):
     tot = d["zeeman"]["E_jax"] + d["anisotropy"]["E_jax"] + d["hmag"]["E_jax"]
     assert d["energy"]["E_jax"] == pytest.approx(tot, rel=1e-9)
     assert (tmp_path / "mapping" / "out_stats.txt").exists()
+
+
+def test_runner_dispatches_scripts(monkeypatch, tmp_path, cube_mesh, energies):
+    """``python -m mammos_mumag.runner <name> <script>``: the script table and its errors."""
+    from mammos_mumag import runner
+
+    monkeypatch.setattr(diagnostics._native, "Mesh", OracleMesh)
+    X, T, tag = cube_mesh
+    fly.write_mesh(tmp_path / "c.fly", X, T, tag)
+    (tmp_path / "c.krn").write_text(energies["krn"]["exani"])
+    out = runner.run_script("exani", tmp_path, "c")
+    assert out["uniform"]["E_gradient"] == pytest.approx(energies["exani_uniform"]["E_gradient"], rel=1e-11)
+    assert (tmp_path / "c_vortex.csv").exists()
+    with pytest.raises(ValueError, match="not provided"):
+        runner.run_script("materials", tmp_path, "c")
