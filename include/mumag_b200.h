@@ -336,9 +336,9 @@ mm_status mm_debug_stall_barriers(mm_mesh* mesh, int32_t stall);
 /* ---- allocation-free Poisson solve ------------------------------------------------------
  *
  * No counterpart in the reference: an extra entry point of this library for callers that
- * cannot allocate device memory -- code running while a CUDA graph is captured, plug-ins
- * whose host application owns every device byte through its own pool, services that
- * forbid allocation on their serving path.  It solves A x = b (A symmetric positive
+ * cannot allocate device memory -- plug-ins whose host application owns every device byte
+ * through its own pool, services that allocate everything at start-up and forbid
+ * allocation on their serving path.  It solves A x = b (A symmetric positive
  * definite, CSR) by Jacobi-preconditioned CG with the mesh path's iteration (the
  * reference's jax.scipy.sparse.linalg.cg: stop when r.r <= tol^2 b.b or after max_iter
  * iterations), x holding the initial guess on entry and the solution on return.

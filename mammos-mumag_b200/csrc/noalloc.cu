@@ -1,10 +1,11 @@
 // mm_poisson_pcg_noalloc: the Jacobi-preconditioned CG solve of the magnetostatic Poisson
 // system for callers that cannot allocate device memory.
 //
-// Some callers cannot call cudaMalloc at all: code that runs while a CUDA graph is being
-// captured, plug-ins living inside a host application that owns every device byte through
-// its own pool, and long-running services that pre-allocate and then forbid allocation on
-// the serving path.  They hold their matrix and vectors in memory they already own and need
+// Some callers cannot call cudaMalloc at all: plug-ins living inside a host application
+// that owns every device byte through its own pool (a cudaMalloc of theirs would take memory
+// the host has already promised elsewhere, or fail), and long-running services that
+// pre-allocate at start-up and then forbid allocation on the serving path (an allocation
+// there can stall every stream of the device and fragments memory over hours).  They hold their matrix and vectors in memory they already own and need
 // a solve that takes nothing more.  This entry point takes a CSR matrix, a right-hand side
 // and an initial guess (all device pointers the caller owns) and keeps every intermediate
 // vector, reduction partial and barrier counter in one file-scope static device array,

@@ -1,7 +1,7 @@
 """The allocation-free Poisson solve (mm_poisson_pcg_noalloc) through the C ABI.
 
-Callers that cannot allocate device memory (graph capture, host applications that own every
-device byte, allocation-free serving paths) solve the magnetostatic Poisson system through
+Callers that cannot allocate device memory (plug-ins whose host application owns every
+device byte, services that forbid allocation while serving) solve the magnetostatic Poisson system through
 this entry point with their own device buffers; its scratch is a static device array.  The
 solution must match the one the mesh path computes inside an energy evaluation, on two calls
 in a row (the second call reuses the static array the first one left behind).  This file
