@@ -16,6 +16,7 @@ import pathlib
 import scipy.constants
 import yaml
 from jinja2 import Environment, FileSystemLoader
+from pydantic import TypeAdapter
 
 from .tools import check_path
 
@@ -23,16 +24,21 @@ MU0 = scipy.constants.mu_0
 _TEMPLATES = pathlib.Path(__file__).parent / "templates"
 
 
+_FLOAT = TypeAdapter(float)
+
+
 def _value(x, unit: str) -> float:
-    """Float value of a number or of a unit-carrying object (astropy-like ``.to``)."""
+    """Float value of a number or of a unit-carrying object (astropy-like ``.to``); anything
+    else raises ``pydantic.ValidationError``, as the reference's pydantic ``MaterialDomain``
+    does (``materials.py:17-60`` of the reference)."""
     if hasattr(x, "to") and hasattr(x, "unit"):
         try:
-            return float(x.to(unit).value)
+            return _FLOAT.validate_python(x.to(unit).value)
         except Exception:
-            return float(x.value)
+            return _FLOAT.validate_python(x.value)
     if hasattr(x, "value") and not isinstance(x, (int, float)):
-        return float(x.value)
-    return float(x)
+        return _FLOAT.validate_python(x.value)
+    return _FLOAT.validate_python(x)
 
 
 @dataclasses.dataclass
@@ -53,8 +59,8 @@ class MaterialDomain:
     """Exchange stiffness, J/m."""
 
     def __post_init__(self):
-        self.theta = float(self.theta)
-        self.phi = float(self.phi)
+        self.theta = _FLOAT.validate_python(self.theta)
+        self.phi = _FLOAT.validate_python(self.phi)
         self.K1 = _value(self.K1, "J / m3")
         self.K2 = _value(self.K2, "J / m3")
         self.Ms = _value(self.Ms, "A / m")

@@ -30,6 +30,19 @@ def test_materials_roundtrip(golden, tmp_path):
         Materials().read(golden / "io" / "cube.p2")
 
 
+def test_material_domain_types_and_validation():
+    """As the reference's tests/test_materials_file.py:119-185: equal values give equal
+    domains whatever their numeric type; the default domain is all zeros; values that are not
+    numbers raise pydantic's ValidationError."""
+    a = MaterialDomain(theta=0, phi=0, K1=1, K2=2, Ms=3, A=4)
+    b = MaterialDomain(theta=0.0, phi=0.0, K1=np.float64(1), K2=2.0, Ms=np.int64(3), A=4.0)
+    assert a == b
+    assert MaterialDomain() == MaterialDomain(theta=0, phi=0, K1=0, K2=0, Ms=0, A=0)
+    for bad in (dict(K1="K1"), dict(theta="x"), dict(A=[1, 2]), dict(Ms=None)):
+        with pytest.raises(ValidationError):
+            MaterialDomain(**bad)
+
+
 def test_parameters_roundtrip_and_validation(golden, tmp_path):
     for bad in (1, 1.0, [1], [1, 2], [1, 2, 3, 4]):
         with pytest.raises(ValidationError):
