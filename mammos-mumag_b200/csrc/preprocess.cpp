@@ -11,6 +11,7 @@
 #include <numeric>
 #include <stdexcept>
 #include <string>
+#include <thread>
 
 #include "mumag_internal.h"
 
@@ -22,6 +23,27 @@ struct Graph {
   std::vector<int64_t> off;
   std::vector<int32_t> adj;
 };
+
+// Runs fn(begin, end, part) over `parts` contiguous chunks of [0, n) on their own threads
+// (the calling thread takes chunk 0).  Every chunk writes only its own outputs, so the
+// results do not depend on the number of parts.
+template <class F>
+void parallel_chunks(int64_t n, int parts, F&& fn) {
+  if (parts <= 1 || n < 2) {
+    fn(int64_t(0), n, 0);
+    return;
+  }
+  std::vector<std::thread> th;
+  for (int p = 1; p < parts; ++p) th.emplace_back([&, p] { fn(n * p / parts, n * (p + 1) / parts, p); });
+  fn(int64_t(0), n / parts, 0);
+  for (auto& t : th) t.join();
+}
+
+// Host threads for a pass over n items: one below 2^16 items, at most 16.
+int host_parts(int64_t n) {
+  const int hw = static_cast<int>(std::max(1u, std::thread::hardware_concurrency()));
+  return static_cast<int>(std::max<int64_t>(1, std::min<int64_t>({int64_t(hw), int64_t(16), n >> 16})));
+}
 
 // Undirected node graph, CSR with sorted unique neighbours.  A node is its own neighbour
 // only if an element lists it twice.  Built from the node -> element incidence with a
@@ -37,34 +59,51 @@ Graph node_graph(int64_t N, const int32_t* T, int64_t E) {
     for (int64_t e = 0; e < E; ++e)
       for (int a = 0; a < 4; ++a) inc[pos[T[4 * e + a]]++] = e;
   }
-  Graph g;
-  g.off.assign(N + 1, 0);
-  g.adj.reserve(static_cast<size_t>(eoff[N]) / 2);
-  std::vector<int64_t> mark(N, -1);
-  std::vector<int32_t> nb;
-  for (int64_t i = 0; i < N; ++i) {
-    nb.clear();
-    mark[i] = i;  // the node itself, unless an element repeats it
-    for (int64_t k = eoff[i]; k < eoff[i + 1]; ++k) {
-      const int32_t* t = T + 4 * inc[k];
-      int self = 0;
-      for (int a = 0; a < 4; ++a) {
-        const int32_t j = t[a];
-        if (j == i) {
-          ++self;
-        } else if (mark[j] != i) {
-          mark[j] = i;
-          nb.push_back(j);
+  // each chunk of nodes gathers its lists into its own buffer; the buffers are then joined
+  const int parts = host_parts(N);
+  std::vector<std::vector<int32_t>> cadj(parts);
+  std::vector<std::vector<int64_t>> clen(parts);
+  parallel_chunks(N, parts, [&](int64_t b, int64_t e, int p) {
+    std::vector<int64_t> mark(N, -1);
+    std::vector<int32_t> nb;
+    auto& out = cadj[p];
+    auto& len = clen[p];
+    out.reserve(static_cast<size_t>(eoff[e] - eoff[b]) / 2);
+    len.reserve(e - b);
+    for (int64_t i = b; i < e; ++i) {
+      nb.clear();
+      mark[i] = i;  // the node itself, unless an element repeats it
+      for (int64_t k = eoff[i]; k < eoff[i + 1]; ++k) {
+        const int32_t* t = T + 4 * inc[k];
+        int self = 0;
+        for (int a = 0; a < 4; ++a) {
+          const int32_t j = t[a];
+          if (j == i) {
+            ++self;
+          } else if (mark[j] != i) {
+            mark[j] = i;
+            nb.push_back(j);
+          }
+        }
+        if (self > 1 && mark[i] == i) {
+          mark[i] = -2;  // listed twice: a self loop, once
+          nb.push_back(static_cast<int32_t>(i));
         }
       }
-      if (self > 1 && mark[i] == i) {
-        mark[i] = -2;  // listed twice: a self loop, once
-        nb.push_back(static_cast<int32_t>(i));
-      }
+      std::sort(nb.begin(), nb.end());
+      out.insert(out.end(), nb.begin(), nb.end());
+      len.push_back(static_cast<int64_t>(nb.size()));
     }
-    std::sort(nb.begin(), nb.end());
-    g.adj.insert(g.adj.end(), nb.begin(), nb.end());
-    g.off[i + 1] = static_cast<int64_t>(g.adj.size());
+  });
+  Graph g;
+  g.off.assign(N + 1, 0);
+  int64_t i = 0, total = 0;
+  for (int p = 0; p < parts; ++p)
+    for (int64_t l : clen[p]) g.off[++i] = (total += l);
+  g.adj.resize(static_cast<size_t>(total));
+  for (int p = 0, at = 0; p < parts; ++p) {
+    std::copy(cadj[p].begin(), cadj[p].end(), g.adj.begin() + at);
+    at += static_cast<int>(cadj[p].size());
   }
   return g;
 }
@@ -213,19 +252,30 @@ void preprocess(const double* X, int64_t N, const int32_t* T, const int32_t* tag
   }
   std::vector<int32_t> rows(roff[N]);
   h.nnz = roff[N];
-  for (int64_t inew = 0; inew < N; ++inew) {
-    const int32_t iold = h.perm[inew];
-    int32_t* r = rows.data() + roff[inew];
-    int32_t* w = r;
-    *w++ = static_cast<int32_t>(inew);
-    for (int64_t k = g.off[iold]; k < g.off[iold + 1]; ++k) {
-      const int32_t jnew = h.iperm[g.adj[k]];
-      *w++ = jnew;
-      h.bandwidth_before = std::max<int64_t>(h.bandwidth_before, std::llabs(int64_t(g.adj[k]) - iold));
-      h.bandwidth_after = std::max<int64_t>(h.bandwidth_after, std::llabs(int64_t(jnew) - inew));
+  const int parts = host_parts(N);
+  std::vector<int64_t> bw0(parts, 0), bw1(parts, 0);
+  parallel_chunks(N, parts, [&](int64_t b, int64_t e, int p) {
+    int64_t m0 = 0, m1 = 0;
+    for (int64_t inew = b; inew < e; ++inew) {
+      const int32_t iold = h.perm[inew];
+      int32_t* r = rows.data() + roff[inew];
+      int32_t* w = r;
+      *w++ = static_cast<int32_t>(inew);
+      for (int64_t k = g.off[iold]; k < g.off[iold + 1]; ++k) {
+        const int32_t jnew = h.iperm[g.adj[k]];
+        *w++ = jnew;
+        m0 = std::max<int64_t>(m0, std::llabs(int64_t(g.adj[k]) - iold));
+        m1 = std::max<int64_t>(m1, std::llabs(int64_t(jnew) - inew));
+      }
+      std::sort(r, w);
+      h.rowlen[inew] = static_cast<int32_t>(w - r);
     }
-    std::sort(r, w);
-    h.rowlen[inew] = static_cast<int32_t>(w - r);
+    bw0[p] = m0;
+    bw1[p] = m1;
+  });
+  for (int p = 0; p < parts; ++p) {
+    h.bandwidth_before = std::max(h.bandwidth_before, bw0[p]);
+    h.bandwidth_after = std::max(h.bandwidth_after, bw1[p]);
   }
   h.sl_off.assign(h.nslices + 1, 0);
   h.sl_w.assign(h.nslices, 0);
@@ -237,28 +287,32 @@ void preprocess(const double* X, int64_t N, const int32_t* T, const int32_t* tag
   }
   h.nent = h.sl_off[h.nslices];
   h.col.assign(h.nent, 0);
-  for (int64_t s = 0; s < h.nslices; ++s)
-    for (int l = 0; l < kSlice; ++l) {
-      int64_t i = s * kSlice + l;
-      for (int32_t k = 0; k < h.sl_w[s]; ++k) {
-        int32_t c = static_cast<int32_t>(i);  // padding entries point at the row itself
-        if (i < N && k < h.rowlen[i]) c = rows[roff[i] + k];
-        h.col[h.sl_off[s] + static_cast<int64_t>(k) * kSlice + l] = c;
+  parallel_chunks(h.nslices, host_parts(N), [&](int64_t b, int64_t e, int) {
+    for (int64_t s = b; s < e; ++s)
+      for (int l = 0; l < kSlice; ++l) {
+        int64_t i = s * kSlice + l;
+        for (int32_t k = 0; k < h.sl_w[s]; ++k) {
+          int32_t c = static_cast<int32_t>(i);  // padding entries point at the row itself
+          if (i < N && k < h.rowlen[i]) c = rows[roff[i] + k];
+          h.col[h.sl_off[s] + static_cast<int64_t>(k) * kSlice + l] = c;
+        }
       }
-    }
+  });
   rows = std::vector<int32_t>();
   // ---- elements: device node ids, colour classes sorted by first node (locality)
   std::vector<int32_t> cn(4 * E);
-  for (int64_t k = 0; k < 4 * E; ++k) cn[k] = h.iperm[T[k]];
+  std::vector<int32_t> emin(E);
+  parallel_chunks(E, host_parts(E), [&](int64_t b, int64_t e_end, int) {
+    for (int64_t e = b; e < e_end; ++e) {
+      for (int a = 0; a < 4; ++a) cn[4 * e + a] = h.iperm[T[4 * e + a]];
+      emin[e] = std::min(std::min(cn[4 * e], cn[4 * e + 1]), std::min(cn[4 * e + 2], cn[4 * e + 3]));
+    }
+  });
   // elements by their smallest device node id, ties in input order (a stable counting sort)
   std::vector<int64_t> eorder(E);
   {
-    std::vector<int32_t> emin(E);
     std::vector<int64_t> cnt(N + 1, 0);
-    for (int64_t e = 0; e < E; ++e) {
-      emin[e] = std::min(std::min(cn[4 * e], cn[4 * e + 1]), std::min(cn[4 * e + 2], cn[4 * e + 3]));
-      cnt[emin[e] + 1]++;
-    }
+    for (int64_t e = 0; e < E; ++e) cnt[emin[e] + 1]++;
     for (int64_t i = 0; i < N; ++i) cnt[i + 1] += cnt[i];
     for (int64_t e = 0; e < E; ++e) eorder[cnt[emin[e]]++] = e;
   }
@@ -279,16 +333,13 @@ void preprocess(const double* X, int64_t N, const int32_t* T, const int32_t* tag
   h.econn.resize(4 * E);
   h.etag.resize(E);
   {
-    std::vector<int32_t> tix(E);  // tag index of every element, in input order
-    for (int64_t e = 0; e < E; ++e)
-      tix[e] = (e > 0 && tag[e] == tag[e - 1])
-                   ? tix[e - 1]
-                   : static_cast<int32_t>(std::lower_bound(h.tags.begin(), h.tags.end(), tag[e]) - h.tags.begin());
-    for (int64_t q = 0; q < E; ++q) {
-      const int64_t e = byc[q];
-      for (int a = 0; a < 4; ++a) h.econn[4 * q + a] = cn[4 * e + a];
-      h.etag[q] = tix[e];
-    }
+    parallel_chunks(E, host_parts(E), [&](int64_t b, int64_t en, int) {
+      for (int64_t q = b; q < en; ++q) {
+        const int64_t e = byc[q];
+        for (int a = 0; a < 4; ++a) h.econn[4 * q + a] = cn[4 * e + a];
+        h.etag[q] = static_cast<int32_t>(std::lower_bound(h.tags.begin(), h.tags.end(), tag[e]) - h.tags.begin());
+      }
+    });
   }
   // ---- coordinates in device order
   h.Xd.assign(3 * h.Npad, 0.0);
