@@ -7,6 +7,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <exception>
 #include <limits>
 #include <numeric>
 #include <stdexcept>
@@ -26,17 +27,28 @@ struct Graph {
 
 // Runs fn(begin, end, part) over `parts` contiguous chunks of [0, n) on their own threads
 // (the calling thread takes chunk 0).  Every chunk writes only its own outputs, so the
-// results do not depend on the number of parts.
+// results do not depend on the number of parts.  An exception in any chunk is rethrown on
+// the calling thread after all chunks have finished.
 template <class F>
 void parallel_chunks(int64_t n, int parts, F&& fn) {
   if (parts <= 1 || n < 2) {
     fn(int64_t(0), n, 0);
     return;
   }
+  std::vector<std::exception_ptr> err(parts);
+  auto run = [&](int p) {
+    try {
+      fn(n * p / parts, n * (p + 1) / parts, p);
+    } catch (...) {
+      err[p] = std::current_exception();
+    }
+  };
   std::vector<std::thread> th;
-  for (int p = 1; p < parts; ++p) th.emplace_back([&, p] { fn(n * p / parts, n * (p + 1) / parts, p); });
-  fn(int64_t(0), n / parts, 0);
+  for (int p = 1; p < parts; ++p) th.emplace_back(run, p);
+  run(0);
   for (auto& t : th) t.join();
+  for (auto& e : err)
+    if (e) std::rethrow_exception(e);
 }
 
 // Host threads for a pass over n items: one below 2^16 items, at most 16.
