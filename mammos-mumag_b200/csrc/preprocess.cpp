@@ -6,6 +6,7 @@
 //    with escript's whereZero tolerance, sqrt(eps) * Lsup(arg).
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <exception>
 #include <limits>
@@ -51,10 +52,15 @@ void parallel_chunks(int64_t n, int parts, F&& fn) {
     if (e) std::rethrow_exception(e);
 }
 
-// Host threads for a pass over n items: one below 2^16 items, at most 16.
+// Host threads for a pass over n items: one below 2^17 items, at most 16, at most the
+// hardware threads and at most MUMAG_HOST_THREADS when that is set to a positive number.
 int host_parts(int64_t n) {
-  const int hw = static_cast<int>(std::max(1u, std::thread::hardware_concurrency()));
-  return static_cast<int>(std::max<int64_t>(1, std::min<int64_t>({int64_t(hw), int64_t(16), n >> 16})));
+  int64_t hw = static_cast<int64_t>(std::max(1u, std::thread::hardware_concurrency()));
+  if (const char* env = std::getenv("MUMAG_HOST_THREADS")) {
+    const long cap = std::strtol(env, nullptr, 10);
+    if (cap > 0) hw = std::min<int64_t>(hw, cap);
+  }
+  return static_cast<int>(std::max<int64_t>(1, std::min<int64_t>({hw, int64_t(16), n >> 16})));
 }
 
 // Undirected node graph, CSR with sorted unique neighbours.  A node is its own neighbour

@@ -71,3 +71,13 @@ def test_bad_options_are_rejected(opt):
         _native.Mesh(X, T, np.ones(len(T), np.int32), [[0, 0, 1e6, 0, 1.0, 1e-11]], **opt)
     assert ei.value.status == _native.MM_BAD_INPUT
     assert next(iter(opt)) in str(ei.value)
+
+
+def test_host_preprocessing_independent_of_threads(monkeypatch):
+    """The RCM order and the element colouring of a mesh large enough for several host
+    threads are the same with one thread (MUMAG_HOST_THREADS=1) and with the default."""
+    X, T = synthetic.cube_grid(52, 52.0)  # 148,877 nodes: the node passes use 2 threads or more
+    perm, col = _native.rcm_permutation(T, X.shape[0]), _native.color_elements(T, X.shape[0])[0]
+    monkeypatch.setenv("MUMAG_HOST_THREADS", "1")
+    assert np.array_equal(perm, _native.rcm_permutation(T, X.shape[0]))
+    assert np.array_equal(col, _native.color_elements(T, X.shape[0])[0])
