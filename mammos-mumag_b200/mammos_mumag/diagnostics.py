@@ -13,6 +13,9 @@ known-answer scripts of the reference, run in the directory that holds ``<name>.
   state from the field, from the gradient and analytically (``Js^2 / 6 mu0``); writes
   ``<name>.csv`` and ``<name>_hmag.vtu`` (point data ``m``, ``U``, ``h_nodes``; cell data
   ``tags``, ``h``);
+* ``materials`` (``scripts/materials.py:50-72``) and ``magnetization``
+  (``scripts/magnetization.py:100-112``): VTU dumps of the per-element material fields and of
+  the ``.p2`` initial state (host only: no solve is involved);
 * ``mapping`` (``scripts/mapping.py:20-131, 238-295``): the same four energies and the total
   energy of the ``.p2`` initial state at ``mu0 Hext = hstart - hstep``; writes
   ``<name>_{zeeman,exchange,anisotropy,hmag,energy}.csv`` (rows named ``E_jax`` as in the
@@ -258,3 +261,41 @@ def run_mapping(workdir, name, device=0) -> dict:
         "function_calls: 1",
     ]))
     return out
+
+
+def _magnetic_nodes(N, T, tag, krn):
+    """``wherePositive(meas)``: nodes of at least one element whose material has Js > 0."""
+    mask = np.zeros(N, dtype=bool)
+    mask[np.asarray(T)[element_js(tag, krn) > 0].ravel()] = True
+    return mask
+
+
+def run_materials(workdir, name, device=0) -> None:
+    """``scripts/materials.py:50-72`` (``Materials.write_vtk``): ``<name>_mat.vtu`` with cell
+    data ``u`` (easy axis), ``K`` (= K1, J/m^3), ``Js`` (T) and ``A`` (= mu0 A: the script
+    stores A scaled by mu0 / size^2 and writes it times size^2); zero where Js <= 0."""
+    wd = pathlib.Path(workdir)
+    X, T, tag = fly.read_mesh(wd / f"{name}.fly")
+    krn = runner.read_krn_rows(wd / f"{name}.krn")
+    tags = np.unique(tag)
+    rows = np.zeros((len(tags), 6))  # u (3), K, Js, A
+    for i in range(len(tags)):
+        theta, phi, K1, _, js, A = krn[i][:6]
+        if js > 0:
+            rows[i] = [math.sin(theta) * math.cos(phi), math.sin(theta) * math.sin(phi), math.cos(theta),
+                       (MU0_SCRIPT * K1) / MU0_SCRIPT, js, (MU0_SCRIPT * A / (SIZE * SIZE)) * (SIZE * SIZE)]
+    per = rows[np.searchsorted(tags, tag)]
+    vtu.write_vtu(wd / f"{name}_mat.vtu", X, T, tag, {},
+                  cell_data={"u": per[:, 0:3], "K": per[:, 3], "Js": per[:, 4], "A": per[:, 5]})
+
+
+def run_magnetization(workdir, name, device=0) -> None:
+    """``scripts/magnetization.py:100-112``: ``<name>.0000.vtu`` with the ``.p2`` initial state
+    (``getM``: uniform, flower, vortex, twisted or random, masked and normalised)."""
+    wd = pathlib.Path(workdir)
+    par = runner.read_script_params(wd / f"{name}.p2")
+    X, T, tag = fly.read_mesh(wd / f"{name}.fly")
+    krn = runner.read_krn_rows(wd / f"{name}.krn")
+    mask = _magnetic_nodes(len(X), T, tag, krn)
+    m = runner.initial_m(X, mask.astype(np.float64), par["m"], par["state_id"])
+    vtu.write_vtu(wd / f"{name}.0000.vtu", X, T, tag, {"m": m})

@@ -158,13 +158,13 @@ def run_loop(workdir, name, m0=None, device=0, grid_ctas=0, block_threads=0, ret
     return (out, steps) if return_steps else out
 
 
-SCRIPTS = ("loop", "exani", "external", "hmag", "mapping")
+SCRIPTS = ("loop", "exani", "external", "hmag", "mapping", "materials", "magnetization")
 
 
 def run_script(script, workdir, name, device=0):
     """The in-process counterpart of ``run-escript scripts/<script>.py <name>`` for the
-    scripts this build provides: the loop (:func:`run_loop`) and the energy known-answer
-    scripts (``mammos_mumag.diagnostics``)."""
+    scripts this build provides: the loop (:func:`run_loop`), the energy known-answer
+    scripts and the material / initial-state dumps (``mammos_mumag.diagnostics``)."""
     if script == "loop":
         return run_loop(workdir, name, device=device)
     if script not in SCRIPTS:

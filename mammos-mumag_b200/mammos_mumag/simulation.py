@@ -6,8 +6,9 @@
 (``mammos_mumag.runner``) instead of ``run-escript scripts/loop.py <name>``.  Failures raise
 ``RuntimeError("Simulation has failed. ...")`` as the reference's subprocess wrapper does
 (``simulation.py:437-458``).  ``run_exani``, ``run_external``, ``run_hmag`` and
-``run_mapping`` run the reference's energy known-answer scripts the same way
-(``mammos_mumag.diagnostics``); the other escript-only scripts raise ``NotImplementedError``.
+``run_mapping`` run the reference's energy known-answer scripts the same way, and
+``run_materials`` / ``run_magnetization`` its VTU dumps (``mammos_mumag.diagnostics``);
+``run_store`` (a pickle cache of escript's arrays) raises ``NotImplementedError``.
 """
 
 from __future__ import annotations
@@ -123,7 +124,12 @@ class Simulation:
         self._run(diagnostics.run_hmag, outdir, name, device=device)
 
     def run_magnetization(self, outdir="magnetization", name="out"):
-        self._out_of_scope("magnetization")
+        """The ``.p2`` initial state as ``<name>.0000.vtu`` (the reference's
+        ``magnetization`` script; host only): writes ``<name>.fly``, ``<name>.krn``,
+        ``<name>.p2`` and the VTU."""
+        outdir = check_dir(outdir)
+        self._write_inputs(outdir, name)
+        self._run(diagnostics.run_magnetization, outdir, name)
 
     def run_mapping(self, outdir="magnetization", name="out", device=0):
         """Energy checks and the total energy of the initial state (the reference's
@@ -135,7 +141,11 @@ class Simulation:
         self._run(diagnostics.run_mapping, outdir, name, device=device)
 
     def run_materials(self, outdir="materials", name="out"):
-        self._out_of_scope("materials")
+        """The per-element material fields as ``<name>_mat.vtu`` (the reference's
+        ``materials`` script; host only): writes ``<name>.fly``, ``<name>.krn`` and the VTU."""
+        outdir = check_dir(outdir)
+        self._write_mesh_krn(outdir, name)
+        self._run(diagnostics.run_materials, outdir, name)
 
     def run_store(self, outdir="magnetization", name="out"):
         self._out_of_scope("store")

@@ -142,4 +142,23 @@ def test_runner_dispatches_scripts(monkeypatch, tmp_path, cube_mesh, energies):
     assert out["uniform"]["E_gradient"] == pytest.approx(energies["exani_uniform"]["E_gradient"], rel=1e-11)
     assert (tmp_path / "c_vortex.csv").exists()
     with pytest.raises(ValueError, match="not provided"):
-        runner.run_script("materials", tmp_path, "c")
+        runner.run_script("store", tmp_path, "c")
+
+
+def test_materials_and_magnetization_dumps(sim, tmp_path, cube_mesh, energies):
+    """run_materials: per-element u, K (= K1), Js and A (= mu0 A) of the magnet, zero in the
+    air and shell; run_magnetization: the .p2 initial state, masked to the magnet's nodes."""
+    X, T, tag = cube_mesh
+    krn = O.read_krn_rows(energies["krn"]["exani"])
+    sim.run_materials(outdir=tmp_path / "mat")
+    d = diagnostics.vtu.read_point_data(tmp_path / "mat" / "out_mat.vtu", ("u", "K", "Js", "A"))
+    magnet = diagnostics.element_js(tag, krn) > 0
+    assert magnet.any() and not magnet.all()
+    assert np.allclose(d["Js"][magnet], krn[0][4]) and np.all(d["Js"][~magnet] == 0)
+    assert np.allclose(d["K"][magnet], krn[0][2], rtol=1e-12)
+    assert np.allclose(d["A"][magnet], diagnostics.MU0_SCRIPT * krn[0][5], rtol=1e-12)
+    assert np.allclose(d["u"].reshape(-1, 3)[magnet], [0.0, 0.0, 1.0])
+    sim.run_magnetization(outdir=tmp_path / "mag")
+    m = diagnostics.vtu.read_point_data(tmp_path / "mag" / "out.0000.vtu", ("m",))["m"]
+    P = O.Problem(X, T, tag, krn)
+    np.testing.assert_allclose(m, O.initial_m_uniform(P, [0.0, 0.0, 1.0]), atol=1e-6)  # %e text
