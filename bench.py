@@ -102,16 +102,10 @@ def workload(name: str, seed: int):
 
 
 def hc_mr(rows):
-    """Coercive field |mu0 H| at the zero crossing of mh and remanence mh(H=0), linear
-    interpolation between adjacent field steps."""
-    h, mh = rows[:, 1], rows[:, 2]
-    hc = mr = float("nan")
-    for i in range(len(h) - 1):
-        if mh[i] > 0 >= mh[i + 1] and np.isnan(hc):
-            hc = abs(h[i] + (h[i + 1] - h[i]) * mh[i] / (mh[i] - mh[i + 1]))
-        if h[i] >= 0 >= h[i + 1] and np.isnan(mr) and h[i] != h[i + 1]:
-            mr = mh[i] + (mh[i + 1] - mh[i]) * (0 - h[i]) / (h[i + 1] - h[i])
-    return hc, mr
+    """Coercive field and remanence of the sweep's rows (``mammos_mumag.hysteresis``)."""
+    from mammos_mumag.hysteresis import coercivity_remanence
+
+    return coercivity_remanence(rows)
 
 
 def algorithmic_bytes(steps, Z: int, N: int, s: int = 8, s_pcg: int | None = None) -> float:

@@ -52,6 +52,23 @@ def run(Ms, A, K1, mesh_filepath, hstart, hfinal, hstep=None, hnsteps: int = 20,
     )
 
 
+def coercivity_remanence(rows):
+    """Coercive field and remanence of a descending loop, from ``.dat`` rows
+    ``[counter, mu0 Hext, mh, energy]`` (the reference computes neither; ``Result`` holds only
+    H and M): ``Hc = |mu0 H|`` where ``mh`` first crosses zero and ``Mr = mh`` at ``H = 0``,
+    both by linear interpolation between adjacent field steps, in tesla; NaN when the loop
+    does not reach them."""
+    rows = np.asarray(rows, dtype=np.float64)
+    h, mh = rows[:, 1], rows[:, 2]
+    hc = mr = float("nan")
+    for i in range(len(h) - 1):
+        if mh[i] > 0 >= mh[i + 1] and np.isnan(hc):
+            hc = abs(h[i] + (h[i + 1] - h[i]) * mh[i] / (mh[i] - mh[i + 1]))
+        if h[i] >= 0 >= h[i + 1] and np.isnan(mr) and h[i] != h[i + 1]:
+            mr = mh[i] + (mh[i + 1] - mh[i]) * (0 - h[i]) / (h[i + 1] - h[i])
+    return hc, mr
+
+
 @dataclasses.dataclass(frozen=True)
 class Result:
     """Hysteresis loop result."""

@@ -102,16 +102,10 @@ def train(feats, targets, epochs: int = 30, batch: int = 256, lr: float = 1e-3, 
 
 
 def hc_mr(rows):
-    """Coercive field |mu0 H| where mh crosses zero and remanence mh at H = 0, both by linear
-    interpolation between adjacent steps (NaN when the loop does not reach them)."""
-    h, mh = rows[:, 1], rows[:, 2]
-    hc = mr = np.nan
-    for i in range(len(h) - 1):
-        if mh[i] > 0 >= mh[i + 1] and np.isnan(hc):
-            hc = abs(h[i] + (h[i + 1] - h[i]) * mh[i] / (mh[i] - mh[i + 1]))
-        if h[i] >= 0 >= h[i + 1] and np.isnan(mr):
-            mr = mh[i] + (mh[i + 1] - mh[i]) * (0 - h[i]) / (h[i + 1] - h[i])
-    return hc, mr
+    """Coercive field and remanence of a loop's rows (``hysteresis.coercivity_remanence``)."""
+    from .hysteresis import coercivity_remanence
+
+    return coercivity_remanence(rows)
 
 
 def compare(model, seeds, spec: LoopSpec | None = None, device: int = 0, modes=(0, 1, 2), max_steps: int = 0):

@@ -10,19 +10,11 @@ import pytest
 
 import oracle as O
 from mammos_mumag import _native, synthetic
+from mammos_mumag.hysteresis import coercivity_remanence as hc_mr
 
 pytestmark = pytest.mark.gpu
 
 
-def hc_mr(rows):
-    h, mh = rows[:, 1], rows[:, 2]
-    hc = mr = np.nan
-    for i in range(len(h) - 1):
-        if mh[i] > 0 >= mh[i + 1] and np.isnan(hc):
-            hc = abs(h[i] + (h[i + 1] - h[i]) * mh[i] / (mh[i] - mh[i + 1]))
-        if h[i] >= 0 >= h[i + 1] and np.isnan(mr):
-            mr = mh[i] + (mh[i + 1] - mh[i]) * (0 - h[i]) / (h[i + 1] - h[i])
-    return hc, mr
 
 
 @pytest.fixture(scope="module")

@@ -104,3 +104,20 @@ def test_multigrain_labels():
     assert len(rows) == len(np.unique(tag))
     assert tag.max() == 6 and (tag == 6).any()  # boundary phase present
     assert np.allclose(np.linalg.norm(m0.reshape(-1, 3), axis=1), 1.0)
+
+
+def test_coercivity_remanence_definitions():
+    """Hc = |mu0 H| at the first zero crossing of mh, Mr = mh at H = 0, linear interpolation;
+    NaN when the loop does not reach them."""
+    from mammos_mumag.hysteresis import coercivity_remanence
+
+    h = np.array([1.0, 0.5, 0.0, -0.5, -1.0, -1.5])
+    mh = np.array([1.0, 0.9, 0.8, 0.4, -0.6, -0.9])
+    rows = np.column_stack([np.arange(6), h, mh, np.zeros(6)])
+    hc, mr = coercivity_remanence(rows)
+    assert hc == pytest.approx(0.5 + 0.5 * 0.4 / 1.0) and mr == pytest.approx(0.8)
+    hc, mr = coercivity_remanence(rows[:2])
+    assert np.isnan(hc) and np.isnan(mr)
+    rows2 = rows.copy()
+    rows2[:, 1] = [1.0, 0.25, -0.25, -0.5, -1.0, -1.5]  # H = 0 between two steps
+    assert coercivity_remanence(rows2)[1] == pytest.approx(0.85)
