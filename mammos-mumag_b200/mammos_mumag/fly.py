@@ -35,9 +35,14 @@ def read_mesh(path) -> tuple[np.ndarray, np.ndarray, np.ndarray]:
         ne = int(hdr[1])
         el = np.array(" ".join(f.readline() for _ in range(ne)).split(), dtype=np.int64).reshape(ne, 6)
     ids = nodes[:, 0].astype(np.int64)
+    if nn == 0 or ne == 0 or ids.min() < 0:
+        raise ValueError(f"{path}: needs nodes and Tet4 elements with non-negative node ids")
+    ref = el[:, 2:6]
+    if ref.min() < 0 or ref.max() > ids.max():
+        raise ValueError(f"{path}: element references an undefined node id")
     lookup = np.full(ids.max() + 1, -1, dtype=np.int64)
     lookup[ids] = np.arange(nn)
-    T = lookup[el[:, 2:6]]
+    T = lookup[ref]
     if (T < 0).any():
         raise ValueError(f"{path}: element references an undefined node id")
     return np.ascontiguousarray(nodes[:, 3:6]), T.astype(np.int32), el[:, 1].astype(np.int32)
