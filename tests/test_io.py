@@ -8,6 +8,7 @@ import oracle as O
 from mammos_mumag import fly, runner, synthetic, vtu
 from mammos_mumag.materials import MaterialDomain, Materials
 from mammos_mumag.parameters import Parameters
+from conftest import ROOT
 
 
 def test_materials_roundtrip(golden, tmp_path):
@@ -121,3 +122,47 @@ def test_coercivity_remanence_definitions():
     rows2 = rows.copy()
     rows2[:, 1] = [1.0, 0.25, -0.25, -0.5, -1.0, -1.5]  # H = 0 between two steps
     assert coercivity_remanence(rows2)[1] == pytest.approx(0.85)
+
+
+def test_write_dat_matches_reference_text(golden, tmp_path):
+    """scripts/tools.py:20-24: ``f'{int(n)} {hext} {mh} {E/mu0}'`` -- the counter, field and
+    polarisation columns of the reference's cube.dat are reproduced as text."""
+    gold = (golden / "loop_cube.dat").read_text().splitlines()
+    rows = np.loadtxt(golden / "loop_cube.dat")
+    rows[:, 3] *= runner.MU0_OUT
+    runner.write_dat(tmp_path / "x.dat", rows)
+    out = (tmp_path / "x.dat").read_text().splitlines()
+    assert len(out) == len(gold)
+    for a, b in zip(out, gold):
+        fa, fb = a.split(), b.split()
+        assert fa[:3] == fb[:3]
+        assert float(fa[3]) == pytest.approx(float(fb[3]), rel=1e-15)
+
+
+def test_initial_states(cube_mesh):
+    """scripts/magnetization.py:9-70 getM: mask * state, normalised; non-magnetic nodes 0."""
+    X, T, tag = cube_mesh
+    krn = O.read_krn_rows((ROOT / "tests" / "golden" / "loop_cube.krn").read_text())
+    P = O.Problem(X, T, tag, krn)
+    meas = P.meas
+    mask = meas > 0
+    x0, x1, x2 = X[:, 0], X[:, 1], X[:, 2]
+    m = runner.initial_m(X, meas, [0.0, 0.0, 1.0], 0).reshape(-1, 3)
+    assert np.array_equal(m, O.initial_m_uniform(P, [0.0, 0.0, 1.0]).reshape(-1, 3))
+    s = X.max()
+    flower = np.column_stack([x0 * x2 / (10 * s), x1 * x2 / (10 * s), np.ones(len(X))])
+    r = np.sqrt(x1 ** 2 + x2 ** 2)
+    rc = 0.14 * r.max()
+    with np.errstate(divide="ignore", invalid="ignore"):
+        vortex = np.column_stack([np.exp(-2 * r / rc), -(x2 / r) * np.sqrt(1 - np.exp(-4 * r * r / rc ** 2)),
+                                  (x1 / r) * np.sqrt(1 - np.exp(-4 * r * r / rc ** 2))])
+    for sid, ref in ((1, flower), (2, vortex)):
+        got = runner.initial_m(X, meas, [0.0, 0.0, 1.0], sid).reshape(-1, 3)
+        ok = mask & np.isfinite(ref).all(axis=1)  # the vortex axis r = 0 is 0/0 in the formula
+        want = ref[ok] / np.linalg.norm(ref[ok], axis=1, keepdims=True)
+        np.testing.assert_allclose(got[ok], want, rtol=1e-13, atol=1e-15)
+        assert np.all(got[~mask] == 0)
+    for sid in (3, 4):
+        got = runner.initial_m(X, meas, [0.0, 0.0, 1.0], sid, seed=5).reshape(-1, 3)
+        assert np.allclose(np.linalg.norm(got[mask], axis=1), 1.0) and np.all(got[~mask] == 0)
+    assert np.array_equal(runner.initial_m(X, meas, [0, 0, 1], 4, seed=5), runner.initial_m(X, meas, [0, 0, 1], 4, seed=5))
