@@ -35,7 +35,7 @@ def test_loop_matches_cube_dat(cube_problem, golden):
     assert np.array_equal(out[:, 1], gold[:, 1])  # cumulative float field values, bit-exact
     np.testing.assert_allclose(out[:, 2], gold[:, 2], rtol=1e-12)
     np.testing.assert_allclose(out[:, 3], gold[:, 3], rtol=1e-12)
-    # the work the reference does on this loop (survey probe counts)
+    # the work of this loop in the reference's algorithm: 67 NCG iterations, 113 evaluations
     assert sum(s.ncg_iters for s in st) == 67
     assert sum(s.evals for s in st) == 113
     # the written .dat rows parse to the golden values
