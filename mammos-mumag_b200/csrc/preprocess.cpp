@@ -82,7 +82,7 @@ Graph node_graph(int64_t N, const int32_t* T, int64_t E) {
   std::vector<std::vector<int32_t>> cadj(parts);
   std::vector<std::vector<int64_t>> clen(parts);
   parallel_chunks(N, parts, [&](int64_t b, int64_t e, int p) {
-    std::vector<int64_t> mark(N, -1);
+    std::vector<int32_t> mark(N, -1);  // node ids fit in 32 bits (validate)
     std::vector<int32_t> nb;
     auto& out = cadj[p];
     auto& len = clen[p];
@@ -90,7 +90,7 @@ Graph node_graph(int64_t N, const int32_t* T, int64_t E) {
     len.reserve(e - b);
     for (int64_t i = b; i < e; ++i) {
       nb.clear();
-      mark[i] = i;  // the node itself, unless an element repeats it
+      mark[i] = static_cast<int32_t>(i);  // the node itself, unless an element repeats it
       for (int64_t k = eoff[i]; k < eoff[i + 1]; ++k) {
         const int32_t* t = T + 4 * inc[k];
         int self = 0;
@@ -99,7 +99,7 @@ Graph node_graph(int64_t N, const int32_t* T, int64_t E) {
           if (j == i) {
             ++self;
           } else if (mark[j] != i) {
-            mark[j] = i;
+            mark[j] = static_cast<int32_t>(i);
             nb.push_back(j);
           }
         }
