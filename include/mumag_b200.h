@@ -3,7 +3,7 @@
  * hysteresis-loop hot path of mammos-mumag.
  *
  * The reference runs its hot path as a subprocess, `run-escript scripts/loop.py <name>`
- * (src/mammos_mumag/simulation.py:114-140, :285-332), whose solver core is a set of
+ * (src/mammos_mumag/simulation.py:88-113 run_script, :258-305 run_loop), whose solver core is a set of
  * jitted JAX functions over escript-assembled sparse operators.  This library replaces
  * that subprocess: the Python host (mammos_mumag.Simulation.run_loop) calls it in process.
  * Plain C types only; host arrays are owned by the caller; device state lives behind an
@@ -330,7 +330,9 @@ mm_status mm_mesh_read_samples(mm_mesh* mesh, float* feats, float* target, int32
  * that releases the other CTAs, and the kernel returns; the call then returns MM_TIMEOUT and
  * the mesh stays usable.  This hook makes that happen on purpose, without a fault: with
  * stall > 0 every barrier of the mesh's later launches waits for `stall` arrivals that never
- * come.  stall = 0 restores normal operation.  For tests of the failure path only. */
+ * come.  stall = 0 restores normal operation.  With mesh == NULL the setting applies to the
+ * barriers of mm_poisson_pcg_noalloc instead (its later calls then return MM_TIMEOUT after
+ * about two seconds).  For tests of the failure path only. */
 mm_status mm_debug_stall_barriers(mm_mesh* mesh, int32_t stall);
 
 /* ---- allocation-free Poisson solve ------------------------------------------------------
@@ -347,13 +349,17 @@ mm_status mm_debug_stall_barriers(mm_mesh* mesh, int32_t stall);
  * iters (may be NULL) is a host pointer.  The call allocates nothing: every intermediate
  * lives in one static device array sized for at most 65,536 rows (about 4.8 MB, held by each
  * GPU that loads the library until exit); n outside [1, 65536] is rejected with
- * MM_BAD_INPUT, as is a CSR structure with out-of-range row pointers or columns.  All calls
- * on a device share that array, which keeps the last call's contents; each call clears
- * what must start at zero.  Calls that overlap on the GPU race on the array: serialise them.
- * The first call on a device does a one-time set-up there (the array's device address,
- * the kernel's occupancy); make it before any stream capture.  The call runs on `stream`
- * (a cudaStream_t; NULL = the legacy default stream) of the current device and returns
- * when the solve has finished. */
+ * MM_BAD_INPUT, as is a CSR structure with out-of-range row pointers or columns or a row
+ * whose diagonal is missing, zero or not finite (nothing is iterated then).  Reaching
+ * max_iter before the tolerance is not an error: x holds the last iterate, as in the
+ * reference's cg.  *iters receives the iterations completed on every return (0 when
+ * nothing was iterated).  All calls on a device share that array, which keeps the last
+ * call's contents; each call clears what must start at zero.  Calls that overlap on the
+ * GPU race on the array: serialise them.  The first call on a device does a one-time
+ * set-up there (the array's device address, the kernel's occupancy); make it before any
+ * stream capture.  The call runs on `stream` (a cudaStream_t; NULL = the legacy default
+ * stream) of the current device and is synchronous: it waits for its own work on that
+ * stream and returns when the solve has finished. */
 mm_status mm_poisson_pcg_noalloc(int32_t n, int32_t nnz, const int32_t* row_ptr, const int32_t* col,
                                  const double* val, const double* b, double* x, double tol,
                                  int32_t max_iter, int32_t* iters, void* stream);

@@ -1034,14 +1034,18 @@ mm_status mm_autotune(mm_mesh* mesh, const mm_solver_params* sp, int32_t* grid_o
 // ---- learned warm start and sample recording --------------------------------------------
 namespace mumag {
 MlpDev model_view(const mm_model* m);
+void set_noalloc_stall(int stall);  // noalloc.cu
 }
 
 extern "C" {
 
 mm_status mm_debug_stall_barriers(mm_mesh* mesh, int32_t stall) {
   API_BEGIN
-  check_mesh(mesh);
   if (stall < 0 || stall > 1024) throw std::runtime_error("stall must be in [0, 1024]");
+  if (!mesh) {  // the allocation-free Poisson solve's barriers
+    set_noalloc_stall(stall);
+    return MM_OK;
+  }
   mesh->dm.bar_stall = stall;
   return MM_OK;
   API_END

@@ -21,7 +21,13 @@
 //    on the array and produce garbage; serialise them;
 //  * the first call on a device does a one-time set-up on that device (looks up the array's
 //    device address with cudaGetSymbolAddress and queries the occupancy of the kernel); make
-//    that first call before any stream capture.
+//    that first call before any stream capture;
+//  * the call is synchronous: it waits for its work on `stream` to finish and returns the
+//    status, the iteration count and the result in x.
+//
+// Bad input is reported, never dereferenced: a row pointer or column outside the matrix,
+// and a row whose diagonal is missing, zero or not finite (the Jacobi preconditioner
+// divides by it), make the call return MM_BAD_INPUT before any iteration.
 //
 // The iteration is the same as the mesh path's Poisson PCG (the reference's
 // jax.scipy.sparse.linalg.cg, scripts/solvers.py:221-231): z = r * (1/diag A), stop when
@@ -59,8 +65,16 @@ static __device__ __align__(256) unsigned char g_pcg_scratch[kScratchBytes];
 struct Ctl {
   unsigned long long bar;
   int flags[2];  // abort, status
-  long long iters;
+  long long iters;  // iterations completed (kept current, so a timed-out call reports them too)
+  int bad;          // kind of bad input: 1 = row pointers or columns, 2 = diagonal
+  int pad;
 };
+static_assert(sizeof(Ctl) <= kOffRed, "control block overlaps the reduction partials");
+
+// Test hook: extra arrivals every barrier of the next calls waits for (0 = none; 1 makes
+// every wait run out, so a call returns MM_TIMEOUT without a fault).  Set through
+// mm_debug_stall_barriers(NULL, stall).
+int g_noalloc_stall = 0;
 
 __device__ __forceinline__ unsigned long long ld_acq(const unsigned long long* p) {
   unsigned long long v;
@@ -76,6 +90,7 @@ struct GridSync {
   double* red;
   unsigned long long epoch;
   int slot;
+  int stall;
 };
 
 __device__ bool barrier(GridSync& g) {
@@ -83,7 +98,7 @@ __device__ bool barrier(GridSync& g) {
   __syncthreads();
   if (threadIdx.x == 0) {
     g.epoch += 1;
-    const unsigned long long target = g.epoch * gridDim.x;
+    const unsigned long long target = g.epoch * gridDim.x + (unsigned long long)g.stall;
     red_rel(&g.ctl->bar, 1ull);
     int a = 0;
     for (unsigned it = 0; ld_acq(&g.ctl->bar) < target; ++it) {
@@ -151,20 +166,36 @@ __device__ __forceinline__ double znext(const Rec& q, double alpha, double beta,
 __global__ void __launch_bounds__(kThreads, 1)
     k_pcg_csr(int n, int nnz, const int32_t* __restrict__ rp, const int32_t* __restrict__ ci,
               const double* __restrict__ av, const double* __restrict__ b, double* x, double tol, int max_iter,
-              unsigned char* scratch) {
+              unsigned char* scratch, int stall) {
   Ctl* ctl = reinterpret_cast<Ctl*>(scratch + kOffCtl);
   Rec* rec[2] = {reinterpret_cast<Rec*>(scratch + kOffRec), reinterpret_cast<Rec*>(scratch + kOffRec) + kMaxRows};
   double* pv = reinterpret_cast<double*>(scratch + kOffP);
-  GridSync g{ctl, reinterpret_cast<double*>(scratch + kOffRed), 0ull, 0};
+  GridSync g{ctl, reinterpret_cast<double*>(scratch + kOffRed), 0ull, 0, stall};
   const int r0 = (int)(((long long)n * blockIdx.x) / gridDim.x);
   const int r1 = (int)(((long long)n * (blockIdx.x + 1)) / gridDim.x);
-  // validate this CTA's rows: 0 <= rp[i] <= rp[i+1] <= nnz and every column in [0, n);
-  // entries that fail are skipped and reported as MM_BAD_INPUT
+  // validate this CTA's rows: 0 <= rp[i] <= rp[i+1] <= nnz, every column in [0, n), and a
+  // diagonal (the sum of the row's entries in column i) that is present, nonzero and finite;
+  // rows that fail are skipped and reported as MM_BAD_INPUT
   for (int i = r0 + threadIdx.x; i < r1; i += blockDim.x) {
     const int e0 = rp[i], e1 = rp[i + 1];
     bool ok = 0 <= e0 && e0 <= e1 && e1 <= nnz;
     for (int e = ok ? e0 : 0; ok && e < e1; ++e) ok = 0 <= ci[e] && ci[e] < n;
-    if (!ok) atomicCAS(&ctl->flags[1], 0, (int)MM_BAD_INPUT);
+    if (!ok) {
+      atomicCAS(&ctl->bad, 0, 1);
+      atomicCAS(&ctl->flags[1], 0, (int)MM_BAD_INPUT);
+      continue;
+    }
+    double d = 0.0;
+    bool has = false;
+    for (int e = e0; e < e1; ++e)
+      if (ci[e] == i) {
+        d += av[e];
+        has = true;
+      }
+    if (!has || !(d != 0.0) || !isfinite(d)) {
+      atomicCAS(&ctl->bad, 0, 2);
+      atomicCAS(&ctl->flags[1], 0, (int)MM_BAD_INPUT);
+    }
   }
   // r0 = b - A x0, z0 = r0 / diag
   double gamma, rr, bb;
@@ -230,6 +261,7 @@ __global__ void __launch_bounds__(kThreads, 1)
       }
       if (!reduce<3>(g, v)) return;
       ++k;
+      if (blockIdx.x == 0 && threadIdx.x == 0) ctl->iters = k;
       rr = v[2];
       if (!(rr > atol2 && k < max_iter)) break;
       const double bn = v[0] / gamma;
@@ -238,7 +270,6 @@ __global__ void __launch_bounds__(kThreads, 1)
       gamma = v[0];
     }
   }
-  if (blockIdx.x == 0 && threadIdx.x == 0) ctl->iters = k;
 }
 
 // one-time set-up per device: the scratch array's device address and the launch shape
@@ -286,6 +317,7 @@ extern "C" mm_status mm_poisson_pcg_noalloc(int32_t n, int32_t nnz, const int32_
                                             const double* val, const double* b, double* x, double tol,
                                             int32_t max_iter, int32_t* iters, void* stream) {
   using namespace mumag;
+  if (iters) *iters = 0;
   if (n <= 0 || n > kMaxRows) {
     set_error("mm_poisson_pcg_noalloc: n = " + std::to_string(n) + " rows is outside [1, " +
               std::to_string(kMaxRows) + "], the size of its static scratch");
@@ -314,7 +346,8 @@ extern "C" mm_status mm_poisson_pcg_noalloc(int32_t n, int32_t nnz, const int32_
   e = cudaMemsetAsync(ds->scratch + kOffCtl, 0, sizeof(Ctl), s);
   if (e == cudaSuccess) {
     unsigned char* sc = ds->scratch;
-    void* args[] = {&n, &nnz, (void*)&row_ptr, (void*)&col, (void*)&val, (void*)&b, &x, &tol, &max_iter, &sc};
+    int stall = g_noalloc_stall;
+    void* args[] = {&n, &nnz, (void*)&row_ptr, (void*)&col, (void*)&val, (void*)&b, &x, &tol, &max_iter, &sc, &stall};
     e = cudaLaunchCooperativeKernel((const void*)k_pcg_csr, dim3(grid), dim3(kThreads), args, 0, s);
   }
   Ctl ctl{};
@@ -324,14 +357,24 @@ extern "C" mm_status mm_poisson_pcg_noalloc(int32_t n, int32_t nnz, const int32_
     set_error(std::string("mm_poisson_pcg_noalloc: ") + cudaGetErrorString(e));
     return MM_CUDA_ERROR;
   }
+  if (iters) *iters = (int32_t)ctl.iters;
   if (ctl.flags[1] == MM_TIMEOUT) {
-    set_error("mm_poisson_pcg_noalloc: a grid barrier timed out");
+    set_error("mm_poisson_pcg_noalloc: a grid barrier timed out after " + std::to_string(ctl.iters) +
+              " iterations");
     return MM_TIMEOUT;
   }
   if (ctl.flags[1] == MM_BAD_INPUT) {
-    set_error("mm_poisson_pcg_noalloc: CSR row pointers or column indices out of range");
+    set_error(ctl.bad == 2 ? "mm_poisson_pcg_noalloc: a row's diagonal is missing, zero or not finite"
+                           : "mm_poisson_pcg_noalloc: CSR row pointers or column indices out of range");
     return MM_BAD_INPUT;
   }
-  if (iters) *iters = (int32_t)ctl.iters;
+  if (ctl.flags[1] != MM_OK) {
+    set_error("mm_poisson_pcg_noalloc: the kernel left an invalid status word");
+    return MM_CUDA_ERROR;
+  }
   return MM_OK;
 }
+
+namespace mumag {
+void set_noalloc_stall(int stall) { g_noalloc_stall = stall; }
+}  // namespace mumag

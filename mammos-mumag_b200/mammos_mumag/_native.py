@@ -314,15 +314,26 @@ def solver_params(hdir=(0.0, 0.0, 1.0), tol_fun=1e-10, tol_u=None, precond_iter=
     return sp
 
 
-def poisson_pcg_noalloc(n, nnz, row_ptr, col, val, b, x, tol=1e-10, max_iter=10000, stream=0) -> int:
+def poisson_pcg_noalloc(n, nnz, row_ptr, col, val, b, x, tol=1e-10, max_iter=10000, stream=0, raise_error=True):
     """Allocation-free Jacobi-PCG solve (``mm_poisson_pcg_noalloc``) on device pointers
     (integers); ``x`` holds the initial guess and receives the solution.  Returns the
-    iteration count."""
-    it = C.c_int32()
-    check(load().mm_poisson_pcg_noalloc(n, nnz, C.c_void_p(row_ptr), C.c_void_p(col), C.c_void_p(val),
-                                        C.c_void_p(b), C.c_void_p(x), float(tol), int(max_iter), C.byref(it),
-                                        C.c_void_p(stream)))
+    iteration count, or ``(status, iterations)`` without raising when ``raise_error`` is
+    false."""
+    it = C.c_int32(-1)
+    st = load().mm_poisson_pcg_noalloc(n, nnz, C.c_void_p(row_ptr), C.c_void_p(col), C.c_void_p(val),
+                                       C.c_void_p(b), C.c_void_p(x), float(tol), int(max_iter), C.byref(it),
+                                       C.c_void_p(stream))
+    if not raise_error:
+        return st, it.value
+    check(st)
     return it.value
+
+
+def noalloc_stall_barriers(stall: int):
+    """Test hook of the failure path of ``poisson_pcg_noalloc``: with stall > 0 every grid
+    barrier of its later calls waits for arrivals that never come, gives up after its
+    bounded wait and the call returns MM_TIMEOUT.  0 restores normal operation."""
+    check(load().mm_debug_stall_barriers(None, int(stall)))
 
 
 def rcm_permutation(T: np.ndarray, N: int) -> np.ndarray:

@@ -5,7 +5,7 @@
 ``<name>_stats.txt`` and ``info.json`` there -- but runs the loop in process on the GPU
 (``mammos_mumag.runner``) instead of ``run-escript scripts/loop.py <name>``.  Failures raise
 ``RuntimeError("Simulation has failed. ...")`` as the reference's subprocess wrapper does
-(``simulation.py:437-458``).  ``run_exani``, ``run_external``, ``run_hmag`` and
+(``simulation.py:410-431``).  ``run_exani``, ``run_external``, ``run_hmag`` and
 ``run_mapping`` run the reference's energy known-answer scripts the same way, and
 ``run_materials`` / ``run_magnetization`` its VTU dumps (``mammos_mumag.diagnostics``);
 ``run_store`` (a pickle cache of escript's arrays) raises ``NotImplementedError``.
@@ -78,8 +78,8 @@ class Simulation:
     @staticmethod
     def _run(fn, outdir, name, **kw):
         """Run one script replacement in ``outdir``; failures raise as the reference's
-        subprocess wrapper does (``simulation.py:437-458``), and ``info.json`` is written as
-        its ``run_script`` writes it (``simulation.py:114-140``)."""
+        subprocess wrapper does (``simulation.py:410-431``), and ``info.json`` is written as
+        its ``run_script`` writes it (``simulation.py:88-113``)."""
         try:
             fn(outdir, name, **kw)
         except Exception as e:

@@ -16,9 +16,9 @@ This script reads them as plain text and stores compact copies here:
 * ``energies.json``       -- the energy densities of ``tests/data/{hmag,exani,external,mapping}/*.csv``.
 * ``io/``                 -- the reference's material/parameter file fixtures, verbatim.
 
-Usage (needs the reference checkout; the fixtures are committed, so tests never need it)::
+Usage (needs a checkout of the reference; the fixtures are committed, so tests never need it)::
 
-    python tests/golden/make_golden.py /root/reference
+    python tests/golden/make_golden.py <path of the reference checkout>
 """
 
 import json
@@ -105,4 +105,6 @@ def main(ref_root):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    if len(sys.argv) != 2:
+        sys.exit("usage: python tests/golden/make_golden.py <path of the reference checkout>")
+    main(sys.argv[1])

@@ -2,7 +2,7 @@
 non-finite inputs, bad options.  Each fails before any device work, so these run (and mean
 the same) with or without a GPU; the reference surfaces such failures as
 ``RuntimeError("Simulation has failed. ...")`` from its subprocess wrapper
-(``simulation.py:437-458``), and so does the in-process drop-in."""
+(``simulation.py:410-431``), and so does the in-process drop-in."""
 
 import numpy as np
 import pytest

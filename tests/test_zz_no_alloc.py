@@ -77,3 +77,91 @@ def test_noalloc_rejects_oversize_and_bad_structure():
     x = torch.zeros(1, dtype=torch.float64, device=dev)
     with pytest.raises(_native.NativeError, match="out of range"):
         _native.poisson_pcg_noalloc(1, 1, rp.data_ptr(), ci.data_ptr(), v.data_ptr(), v.data_ptr(), x.data_ptr())
+    # rows whose diagonal is missing, zero or not finite: the Jacobi preconditioner would
+    # divide by it, so the call refuses them before iterating and reports 0 iterations
+    rp2 = torch.tensor([0, 1, 2], dtype=torch.int32, device=dev)
+    b2 = torch.ones(2, dtype=torch.float64, device=dev)
+    x2 = torch.zeros(2, dtype=torch.float64, device=dev)
+    cases = {
+        "missing": ([1, 0], [2.0, 2.0]),   # row 0 holds only column 1
+        "zero": ([0, 1], [0.0, 2.0]),
+        "nan": ([0, 1], [float("nan"), 2.0]),
+        "inf": ([0, 1], [2.0, float("inf")]),
+    }
+    for name, (cols, vals) in cases.items():
+        ci2 = torch.tensor(cols, dtype=torch.int32, device=dev)
+        av2 = torch.tensor(vals, dtype=torch.float64, device=dev)
+        st, it = _native.poisson_pcg_noalloc(2, 2, rp2.data_ptr(), ci2.data_ptr(), av2.data_ptr(), b2.data_ptr(),
+                                             x2.data_ptr(), raise_error=False)
+        assert st == _native.MM_BAD_INPUT, name
+        assert it == 0, name
+        assert "diagonal" in _native.load().mm_last_error().decode(), name
+        assert torch.all(x2 == 0), name
+
+
+def _laplacian_1d(n):
+    """The 1-D Dirichlet Laplacian (tridiagonal 2, -1): CG needs about n/2 iterations."""
+    main = 2.0 * np.ones(n)
+    off = -np.ones(n - 1)
+    A = sp.diags([off, main, off], [-1, 0, 1], format="csr")
+    A.sort_indices()
+    return A
+
+
+def test_noalloc_max_iter_caps_an_unconverged_solve():
+    """max_iter stops the solve early, as the reference's cg does: the call succeeds, reports
+    exactly max_iter iterations and returns the CG iterate after them (the oracle's CG with
+    the same cap), whose residual is still far above the tolerance."""
+    import torch
+
+    n, cap = 3000, 7
+    A = _laplacian_1d(n)
+    rng = np.random.default_rng(11)
+    b = rng.standard_normal(n)
+    dev = torch.device("cuda:0")
+    rp = torch.from_numpy(A.indptr.astype(np.int32)).to(dev)
+    ci = torch.from_numpy(A.indices.astype(np.int32)).to(dev)
+    av = torch.from_numpy(A.data.astype(np.float64)).to(dev)
+    bd = torch.from_numpy(b).to(dev)
+    xd = torch.zeros(n, dtype=torch.float64, device=dev)
+    it = _native.poisson_pcg_noalloc(n, A.nnz, rp.data_ptr(), ci.data_ptr(), av.data_ptr(), bd.data_ptr(),
+                                     xd.data_ptr(), tol=1e-10, max_iter=cap)
+    assert it == cap
+    x = xd.cpu().numpy()
+    xo, ko = O.pcg(A, A.diagonal(), b, np.zeros(n), 1e-10, maxiter=cap)
+    assert ko == cap
+    # the same iterate in another arrangement of the same recurrences: rounding-level agreement
+    assert np.abs(x - xo).max() <= 1e-10 * np.abs(xo).max()
+    assert np.linalg.norm(A @ x - b) > 1e-3 * np.linalg.norm(b)
+
+
+def test_noalloc_barrier_timeout_then_recovers():
+    """Every wait of the kernel is bounded: with the test hook making each grid barrier wait
+    for an arrival that never comes, the call gives up after about two seconds and returns
+    MM_TIMEOUT (no fault, no hang); with the hook cleared the next call solves normally."""
+    import torch
+
+    n = 2000
+    A = _laplacian_1d(n)
+    b = np.random.default_rng(12).standard_normal(n)
+    dev = torch.device("cuda:0")
+    rp = torch.from_numpy(A.indptr.astype(np.int32)).to(dev)
+    ci = torch.from_numpy(A.indices.astype(np.int32)).to(dev)
+    av = torch.from_numpy(A.data.astype(np.float64)).to(dev)
+    bd = torch.from_numpy(b).to(dev)
+    xd = torch.zeros(n, dtype=torch.float64, device=dev)
+    args = (n, A.nnz, rp.data_ptr(), ci.data_ptr(), av.data_ptr(), bd.data_ptr(), xd.data_ptr())
+    _native.noalloc_stall_barriers(1)
+    try:
+        st, it = _native.poisson_pcg_noalloc(*args, raise_error=False)
+    finally:
+        _native.noalloc_stall_barriers(0)
+    assert st == _native.MM_TIMEOUT
+    assert it == 0  # the first barrier never opened: nothing was iterated
+    xd.zero_()
+    it = _native.poisson_pcg_noalloc(*args, tol=1e-10, max_iter=10000)
+    assert 0 < it < 10000
+    x = xd.cpu().numpy()
+    # the stop test reads the recursively updated residual; the true one agrees to rounding
+    # (condition number ~1e6 here)
+    assert np.linalg.norm(A @ x - b) <= 1e-8 * np.linalg.norm(b)
