@@ -66,6 +66,13 @@ typedef struct {
   int stage_operators; /* 1 (default): each CTA keeps its SELL columns and Poisson values in
                           shared memory when they fit; 0: always read them from HBM (the
                           large-mesh path, selectable on any mesh; results are identical) */
+  int coarse_box_nodes; /* Poisson preconditioner: 0 (default) = Jacobi, the reference's
+                          (scripts/solvers.py:221-231); > 0 = two-level additive
+                          M^-1 = D^-1 + P (P^T S P)^-1 P^T with P constant on spatial boxes
+                          of about this many interior nodes (at most 2,048 boxes; nodes are
+                          then numbered box by box).  No counterpart in the reference: only
+                          the path to the solution changes, the stop test r.r <= tol_u^2 b.b
+                          stays.  Batched launches always use Jacobi. */
 } mm_options;
 
 /* Solver settings of one field step (scripts/tools.py:64-120, scripts/minimizers.py:140-190). */
@@ -111,6 +118,7 @@ typedef struct {
   int32_t kernel_ctas_per_sm;          /* build of the persistent kernel in use: 2 or 3 resident
                                           CTAs per SM (128 or 80 registers per thread) */
   int32_t staged;                      /* 1: SELL columns + Poisson values in shared memory */
+  int32_t coarse_boxes;                /* boxes of the two-level preconditioner (0 = Jacobi) */
 } mm_mesh_info;
 
 /* Field-sweep parameters (the .p2 [field] section; scripts/loop.py:71-142). */
@@ -169,6 +177,11 @@ mm_status mm_mesh_create(const double* X, int64_t N, const int32_t* T, const int
                          const mm_options* opt, mm_mesh** out);
 mm_status mm_mesh_destroy(mm_mesh* mesh);
 mm_status mm_mesh_get_info(const mm_mesh* mesh, mm_mesh_info* info);
+
+/* The two-level preconditioner's aggregates: box [N] (mesh-file order) receives the box of
+ * every node (-1 for Dirichlet nodes), *nboxes their number (0 = Jacobi, box untouched).
+ * No counterpart in the reference; for checks of the preconditioner. */
+mm_status mm_mesh_get_coarse(const mm_mesh* mesh, int32_t* box, int32_t* nboxes);
 
 /* Node measure meas [N] (mesh-file order) and the magnetic volume. */
 mm_status mm_get_meas(mm_mesh* mesh, double* meas, double* volume);

@@ -220,10 +220,10 @@ __global__ void k_finalize(const int64_t* __restrict__ sl_off, const int32_t* __
   Dex[i] = (meas[i] == 0.0) ? 1.0 : dA;
 }
 
-// FP32 copies of the planes the mixed-precision iterations read (S, Aex, K[6]).
-__global__ void k_to_f32(const double* __restrict__ vals, float* __restrict__ v32, int64_t nent) {
-  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < 8 * nent; t += (int64_t)gridDim.x * blockDim.x)
-    v32[t] = (float)vals[t];  // planes 0..7 of vals are S, Aex, K[6] in that order
+// FP32 copies of every operator plane (mixed precision reads them, accumulating in FP64).
+__global__ void k_to_f32(const double* __restrict__ vals, float* __restrict__ v32, int64_t n) {
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < n; t += (int64_t)gridDim.x * blockDim.x)
+    v32[t] = (float)vals[t];
 }
 
 }  // namespace
@@ -277,8 +277,8 @@ void assemble_operators(DevMesh& m) {
       (int)h.Npad, m.opt.dirichlet_rhs == MM_DIRICHLET_RHS_ZERO);
   CK(cudaGetLastError());
   if (m.vals32) {
-    static_assert(P_S == 0 && P_AEX == 1 && P_K == 2, "FP32 planes mirror the first 8 FP64 planes");
-    k_to_f32<<<592, 256, 0, st>>>(m.vals, m.vals32, h.nent);
+    static_assert(kNumPlanes32 == kNumPlanes, "FP32 planes mirror the FP64 planes");
+    k_to_f32<<<592, 256, 0, st>>>(m.vals, m.vals32, (int64_t)kNumPlanes * h.nent);
     CK(cudaGetLastError());
   }
   CK(cudaStreamSynchronize(st));

@@ -110,6 +110,12 @@ void release(DevMesh& m) {
   dfree(m.rs_node);
   dfree(m.rs_slot);
   dfree(m.rs_count);
+  dfree(m.rbox);
+  dfree(m.Ainv);
+  dfree(m.Ainv32);
+  dfree(m.bslots);
+  dfree(m.bslot);
+  dfree(m.ctabox);
   if (m.h_resd) cudaFreeHost(m.h_resd);
   if (m.h_resi) cudaFreeHost(m.h_resi);
   if (m.h_flags) cudaFreeHost(m.h_flags);
@@ -124,6 +130,46 @@ void release(DevMesh& m) {
   m.ev0 = m.ev1 = nullptr;
   if (m.stream) cudaStreamDestroy(m.stream);
   m.stream = nullptr;
+}
+
+// The two-level preconditioner's coarse operator: Ac = P^T S P summed on the host from the
+// assembled Poisson plane (rows in device order, so the sums are deterministic), inverted
+// densely (banded Cholesky; Ac couples only neighbouring boxes), uploaded in FP64 and FP32.
+void build_coarse(DevMesh& m) {
+  const HostMesh& h = m.h;
+  const int nc = h.nc;
+  m.nc = nc;
+  if (nc <= 0) return;
+  std::vector<double> S;
+  d2h(S, m.vals + (size_t)P_S * h.nent, h.nent, m.stream);
+  std::vector<double> A((size_t)nc * nc, 0.0);
+  int32_t bw = 0;
+  for (int64_t s = 0; s < h.nslices; ++s)
+    for (int l = 0; l < kSlice; ++l) {
+      const int64_t i = s * kSlice + l;
+      if (i >= h.N || h.rbox[i] < 0) continue;
+      const int32_t ci = h.rbox[i];
+      for (int32_t k = 0; k < h.rowlen[i]; ++k) {
+        const int64_t e = h.sl_off[s] + (int64_t)k * kSlice + l;
+        const int32_t cj = h.rbox[h.col[e]];
+        if (cj < 0) continue;
+        A[(size_t)ci * nc + cj] += S[e];
+        bw = std::max(bw, std::abs(ci - cj));
+      }
+    }
+  spd_inverse(nc, bw, A);
+  std::vector<float> A32(A.size());
+  for (size_t q = 0; q < A.size(); ++q) A32[q] = (float)A[q];
+  dalloc(m.rbox, h.Npad);
+  dalloc(m.Ainv, A.size());
+  dalloc(m.Ainv32, A32.size());
+  dalloc(m.bslots, (size_t)nc + kMaxGrid);
+  dalloc(m.bslot, (size_t)nc + 1);
+  dalloc(m.ctabox, (size_t)3 * kMaxGrid);
+  upload(m.rbox, h.rbox, m.stream);
+  upload(m.Ainv, A, m.stream);
+  upload(m.Ainv32, A32, m.stream);
+  MM_CK(cudaStreamSynchronize(m.stream));
 }
 
 mm_status fail(mm_status st, const std::string& msg) {
@@ -203,6 +249,7 @@ void mm_default_options(mm_options* opt) {
   opt->pcg_variant = 0;
   opt->ctas_per_sm = 0;
   opt->stage_operators = 1;
+  opt->coarse_box_nodes = 0;
 }
 
 void mm_default_solver_params(mm_solver_params* sp) {
@@ -267,6 +314,7 @@ mm_status mm_mesh_create(const double* X, int64_t N, const int32_t* T, const int
     throw std::runtime_error("options.ctas_per_sm must be 0, 2 or 3");
   if (o.stage_operators != 0 && o.stage_operators != 1)
     throw std::runtime_error("options.stage_operators must be 0 or 1");
+  if (o.coarse_box_nodes < 0) throw std::runtime_error("options.coarse_box_nodes must be >= 0");
   for (int64_t i = 0; i < 3 * N; ++i)
     if (!std::isfinite(X[i])) throw std::runtime_error("non-finite node coordinate");
   int ndev = 0;
@@ -282,9 +330,15 @@ mm_status mm_mesh_create(const double* X, int64_t N, const int32_t* T, const int
   DevMesh& m = mesh->dm;
   m.device = o.device;
   m.opt = o;
-  preprocess(X, N, T, tag, E, nmats, o.reorder != 0, m.h);
-  // PCG arrangement: fixed by the caller, else by size until mm_autotune times both
+  preprocess(X, N, T, tag, E, nmats, o.reorder != 0, o.coarse_box_nodes, m.h);
+  // PCG arrangement: fixed by the caller, else by size until mm_autotune times both; the
+  // two-level preconditioner runs in the two-sync arrangement only
   m.pcg2 = o.pcg_variant == 2 ? 1 : o.pcg_variant == 1 ? 0 : (m.h.N >= kPcg2Nodes ? 1 : 0);
+  if (m.h.nc > 0) {
+    if (o.pcg_variant == 1)
+      throw std::runtime_error("the two-level preconditioner runs in the two-sync PCG arrangement (pcg_variant 0 or 2)");
+    m.pcg2 = 1;
+  }
   m.kernel_mb = o.ctas_per_sm == 3 ? 3 : 2;
   HostMesh& h = m.h;
   m.ncolours = (int32_t)h.colour_off.size() - 1;
@@ -332,6 +386,7 @@ mm_status mm_mesh_create(const double* X, int64_t N, const int32_t* T, const int
     upload(m.etag, h.etag, m.stream);
     upload(m.dmats, m.mats, m.stream);
     assemble_operators(m);
+    build_coarse(m);
     // solver state: 12 three-vectors, 2 node vectors, 2 x Npad PCG records (4 doubles each);
     // the total is computed from the same list that carves the buffer
     const size_t np = h.Npad;
@@ -418,6 +473,19 @@ mm_status mm_mesh_get_info(const mm_mesh* mesh, mm_mesh_info* info) {
   info->pcg_variant = m.pcg2 ? 2 : 1;
   info->kernel_ctas_per_sm = m.kernel_mb;
   info->staged = m.stage;
+  info->coarse_boxes = m.nc;
+  return MM_OK;
+  API_END
+}
+
+mm_status mm_mesh_get_coarse(const mm_mesh* mesh, int32_t* box, int32_t* nboxes) {
+  API_BEGIN
+  check_mesh(mesh);
+  if (!nboxes) throw std::runtime_error("nboxes is NULL");
+  const DevMesh& m = mesh->dm;
+  *nboxes = m.nc;
+  if (box && m.nc > 0)
+    for (int64_t i = 0; i < m.h.N; ++i) box[i] = m.h.rbox[m.h.iperm[i]];
   return MM_OK;
   API_END
 }
@@ -707,6 +775,7 @@ mm_status batch_run(mm_batch* b, const double* h, const mm_solver_params* sp, co
     a.meta_max = b->plan.meta_max[q];
     a.prof = nullptr;
     a.tc_off = -1;  // batched launches run the network on mma.sync
+    a.nc = 0;       // and the Jacobi preconditioner
     b->h_args[q] = a;
     MM_CK(launch_prep(m, b->stream));
   }
@@ -840,6 +909,7 @@ mm_status mm_batch_loop(mm_batch* batch, const mm_loop_params* lp, const mm_solv
       a.meta_max = batch->plan.meta_max[q];
       a.prof = nullptr;
       a.tc_off = -1;  // batched launches run the network on mma.sync
+      a.nc = 0;       // and the Jacobi preconditioner
       batch->h_args[q] = a;
       MM_CK(launch_prep(m, batch->stream));
     }
@@ -938,7 +1008,8 @@ mm_status mm_autotune(mm_mesh* mesh, const mm_solver_params* sp, int32_t* grid_o
   MM_CK(cudaSetDevice(m.device));
   cudaDeviceProp prop;
   MM_CK(cudaGetDeviceProperties(&prop, m.device));
-  const auto key = std::make_tuple(m.h.nslices, m.h.nent, (m.vals32 ? 1 : 0) + (m.warm == WARM_LEARNED ? 2 : 0),
+  const auto key = std::make_tuple(m.h.nslices, m.h.nent,
+                                   (m.vals32 ? 1 : 0) + (m.warm == WARM_LEARNED ? 2 : 0) + 4 * m.nc,
                                    m.device, (m.opt.pcg_variant * 4 + m.opt.ctas_per_sm) * 2 + m.opt.stage_operators);
   {
     std::lock_guard<std::mutex> lk(g_tune_mu);
@@ -972,7 +1043,9 @@ mm_status mm_autotune(mm_mesh* mesh, const mm_solver_params* sp, int32_t* grid_o
     add(3, 3 * sms, 3);
   }
   std::vector<int> variants;
-  if (m.opt.pcg_variant == 1)
+  if (m.nc > 0)
+    variants = {1};
+  else if (m.opt.pcg_variant == 1)
     variants = {0};
   else if (m.opt.pcg_variant == 2)
     variants = {1};

@@ -48,7 +48,7 @@ struct __align__(16) PcgRec32 {
   float r, w, s, invd;
 };
 
-constexpr int kNumPlanes32 = 8;  // FP32 copies of S, Aex, K[6] (mixed precision)
+constexpr int kNumPlanes32 = kNumPlanes;  // FP32 copies of every plane (mixed precision)
 
 // Arguments of the persistent solver kernel (passed by value, __grid_constant__).
 struct SolveArgs {
@@ -70,7 +70,7 @@ struct SolveArgs {
   double* pp;       // PCG search direction
   // mixed precision: FP32 operator planes and inner-solve state
   int mixed;
-  const float* vals32;  // [kNumPlanes32][nent]: S, Aex, K[6]
+  const float* vals32;  // [kNumPlanes32][nent]: FP32 copies of the planes of vals
   PcgRec32* rec32[2];
   float *pp32, *e32;    // inner search direction and correction
   double* r64;          // FP64 residual of the outer refinement
@@ -83,6 +83,16 @@ struct SolveArgs {
   float* du;            // [Npad] its predicted correction (units of sigma)
   int tc_off;           // >= 0: dynamic shared-memory offset of the tensor-core network's
                         // region (learned start on tcgen05); -1: the network runs on mma.sync
+  // two-level Poisson preconditioner (nc > 0; 0 = Jacobi): z = r/diag + P Ac^-1 P^T r with P
+  // constant on aggregates ("boxes") of rows and Ac = P^T S P
+  int nc;
+  const int32_t* rbox;  // [Npad] box of each row, -1 for Dirichlet and padding rows
+  const double* Ainv;   // [nc][nc] Ac^-1
+  const float* Ainv32;  // [nc][nc] Ac^-1 in FP32 (mixed precision's inner iterations)
+  double* bslots;       // box partial sums, one slot per (CTA, box it holds rows of)
+  const int32_t* bslot; // [nc+1] box c's partial sums are slots [bslot[c], bslot[c+1])
+  const int32_t* ctabox;  // [grid][3] first box, number of boxes and first slot of each CTA
+  int co_off;           // dynamic shared-memory offset of the coarse vectors
   // training-sample recording (rec_cap > 0): at a hash-selected 1/rec_stride of the
   // (node, solve) pairs, the node's features at the warm start and, after the solve,
   // the target (u - u0) / sigma
@@ -186,6 +196,15 @@ struct DevMesh {
   int64_t stage_max = 0, meta_max = 0;
   size_t smem = 0;
   int tc_off = -1;  // SolveArgs::tc_off
+  // two-level preconditioner (SolveArgs): nc boxes, 0 = Jacobi
+  int nc = 0;
+  int32_t* rbox = nullptr;
+  double* Ainv = nullptr;
+  float* Ainv32 = nullptr;
+  double* bslots = nullptr;
+  int32_t* bslot = nullptr;
+  int32_t* ctabox = nullptr;
+  int co_off = -1;
 };
 
 // A batched persistent launch over several meshes: mesh q runs on CTAs

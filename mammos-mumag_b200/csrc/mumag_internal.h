@@ -15,6 +15,8 @@ constexpr int kMaxRed = 8;      // values per grid reduction
 constexpr int kNumPlanes = 14;  // S, Aex, K[6], D[3], G[3]
 constexpr int kMaxGrid = 480;   // CTAs a persistent launch may use (reduction coverage)
 constexpr int64_t kPcg2Nodes = 100000;  // default to the two-sync PCG from this many nodes
+constexpr int kMaxCoarse = 2048;        // aggregates of the two-level Poisson preconditioner
+constexpr int kMinBoxNodes = 32;        // smallest aggregate box (so a SELL slice meets <= 2 boxes)
 
 // Value planes of the node-pair operators, all on one SELL-32 pattern.
 enum Plane {
@@ -43,11 +45,23 @@ struct HostMesh {
   int airbox = 0;
   double R = 0.0, Rinf = 0.0;    // shell radii (shell branch)
   int64_t bandwidth_before = 0, bandwidth_after = 0;
+  // two-level Poisson preconditioner: aggregate ("box") of each device row, -1 for Dirichlet
+  // and padding rows; nc aggregates, numbered in device-row order
+  int32_t nc = 0;
+  std::vector<int32_t> rbox;     // [Npad]
 };
 
 // Build everything the device needs. Throws std::runtime_error on bad input.
+// coarse_nodes > 0 also groups the interior nodes into spatial boxes of about that many nodes
+// for the two-level preconditioner and numbers the nodes box by box (reverse Cuthill-McKee
+// order inside a box).
 void preprocess(const double* X, int64_t N, const int32_t* T, const int32_t* tag, int64_t E,
-                int32_t nmats, bool reorder, HostMesh& out);
+                int32_t nmats, bool reorder, int32_t coarse_nodes, HostMesh& out);
+
+// In place: A [n][n] (symmetric positive definite, nonzero only within `bw` of the
+// diagonal) becomes A^-1, by a banded Cholesky factorisation and one pair of triangular
+// solves per column (columns on host threads).  Throws if A is not positive definite.
+void spd_inverse(int32_t n, int32_t bw, std::vector<double>& A);
 
 std::vector<int32_t> rcm_order(int64_t N, const int32_t* T, int64_t E);
 int32_t greedy_colour(int64_t N, const int32_t* T, int64_t E, const int64_t* order,

@@ -206,7 +206,190 @@ std::vector<int32_t> rcm_of_graph(const Graph& g, int64_t N) {
   return order;  // order[new] = old
 }
 
+// The Poisson boundary branch, scripts/matrix.py:49-64 and scripts/trafo.py:4-16: airbox
+// (exactly 8 nodes at the largest radius: Dirichlet nodes on the bounding-box faces) or
+// spherical shell (Dirichlet nodes at the largest radius; R from the second-to-last tag).
+// bold[i] = 1 for Dirichlet node i (mesh-file order).
+void boundary_nodes(const double* X, int64_t N, const int32_t* T, const int32_t* tag, int64_t E, HostMesh& h,
+                    std::vector<uint8_t>& bold) {
+  const double rtol = std::sqrt(std::numeric_limits<double>::epsilon());
+  std::vector<double> rn(N);
+  double Rinf = 0.0;
+  for (int64_t i = 0; i < N; ++i) {
+    rn[i] = std::sqrt(X[3 * i] * X[3 * i] + X[3 * i + 1] * X[3 * i + 1] + X[3 * i + 2] * X[3 * i + 2]);
+    Rinf = std::max(Rinf, rn[i]);
+  }
+  h.Rinf = Rinf;
+  double lsup = 0.0;
+  for (int64_t i = 0; i < N; ++i) lsup = std::max(lsup, std::fabs(rn[i] - Rinf));
+  int64_t at_rinf = 0;
+  for (int64_t i = 0; i < N; ++i) at_rinf += std::fabs(rn[i] - Rinf) <= rtol * lsup;
+  h.airbox = (at_rinf == 8);
+  bold.assign(N, 0);
+  if (h.airbox) {
+    for (int c = 0; c < 3; ++c) {
+      double xe = -std::numeric_limits<double>::infinity();
+      for (int64_t i = 0; i < N; ++i) xe = std::max(xe, X[3 * i + c]);
+      for (int sgn = -1; sgn <= 1; sgn += 2) {
+        double ls = 0.0;
+        for (int64_t i = 0; i < N; ++i) ls = std::max(ls, std::fabs(X[3 * i + c] + sgn * xe));
+        for (int64_t i = 0; i < N; ++i)
+          if (std::fabs(X[3 * i + c] + sgn * xe) <= rtol * ls) bold[i] = 1;
+      }
+    }
+  } else {
+    if (h.tags.size() < 2)
+      throw std::runtime_error("spherical-shell boundary needs at least two element tags");
+    for (int64_t i = 0; i < N; ++i) bold[i] = std::fabs(rn[i] - Rinf) <= rtol * lsup;
+    int32_t t2 = h.tags[h.tags.size() - 2];
+    double R = 0.0;
+    for (int64_t e = 0; e < E; ++e)
+      if (tag[e] == t2)
+        for (int a = 0; a < 4; ++a) R = std::max(R, rn[T[4 * e + a]]);
+    h.R = R;
+  }
+}
+
+// Spatial aggregates of the interior nodes for the two-level preconditioner: a grid of
+// boxes over the interior nodes' bounding box, sized for about `target` nodes per box.
+// Boxes with fewer than kMinBoxNodes nodes (interior and Dirichlet) are merged into the
+// previous box in lexicographic order (the first ones into the next), so every box spans at
+// least kMinBoxNodes consecutive device rows and a 32-row slice meets at most two boxes.
+// key[i] = the (merged) box of node i, used for the node order; cbox[i] = the aggregate of
+// interior node i (aggregates numbered in ascending key), -1 for a Dirichlet node.  The box
+// size grows until there are at most kMaxCoarse aggregates.
+void coarse_boxes(const double* X, int64_t N, const std::vector<uint8_t>& bold, int32_t target,
+                  std::vector<int64_t>& key, std::vector<int32_t>& cbox, int32_t& nc) {
+  key.assign(N, 0);
+  cbox.assign(N, -1);
+  nc = 0;
+  double lo[3] = {std::numeric_limits<double>::infinity(), std::numeric_limits<double>::infinity(),
+                  std::numeric_limits<double>::infinity()};
+  double hi[3] = {-lo[0], -lo[1], -lo[2]};
+  int64_t nint = 0;
+  for (int64_t i = 0; i < N; ++i) {
+    if (bold[i]) continue;
+    ++nint;
+    for (int d = 0; d < 3; ++d) {
+      lo[d] = std::min(lo[d], X[3 * i + d]);
+      hi[d] = std::max(hi[d], X[3 * i + d]);
+    }
+  }
+  if (nint == 0) return;
+  double ext[3];
+  int nd = 0;
+  double vol = 1.0;
+  for (int d = 0; d < 3; ++d) {
+    ext[d] = hi[d] - lo[d];
+    if (ext[d] > 0) {
+      ++nd;
+      vol *= ext[d];
+    }
+  }
+  for (int64_t tgt = std::max<int64_t>(target, kMinBoxNodes);; tgt = tgt * 3 / 2 + 1) {
+    const double want = std::max(1.0, static_cast<double>(nint) / static_cast<double>(tgt));
+    const double b = nd > 0 ? std::pow(vol / want, 1.0 / nd) : 1.0;
+    int64_t nb[3];
+    for (int d = 0; d < 3; ++d)
+      nb[d] = ext[d] > 0 ? std::max<int64_t>(1, std::llround(ext[d] / b)) : 1;
+    const int64_t nkeys = nb[0] * nb[1] * nb[2];
+    std::vector<int64_t> cnt(nkeys, 0), cint(nkeys, 0);
+    for (int64_t i = 0; i < N; ++i) {
+      int64_t k[3];
+      for (int d = 0; d < 3; ++d) {
+        const double t = ext[d] > 0 ? std::floor((X[3 * i + d] - lo[d]) / ext[d] * static_cast<double>(nb[d])) : 0.0;
+        k[d] = std::min<int64_t>(nb[d] - 1, std::max<int64_t>(0, static_cast<int64_t>(t)));
+      }
+      key[i] = (k[2] * nb[1] + k[1]) * nb[0] + k[0];
+      cnt[key[i]]++;
+      cint[key[i]] += bold[i] ? 0 : 1;
+    }
+    // merge small boxes: into the last kept box before them, else into the first kept after
+    std::vector<int64_t> map(nkeys, -1);
+    int64_t last = -1;
+    std::vector<int64_t> pending;
+    for (int64_t k = 0; k < nkeys; ++k) {
+      if (cnt[k] == 0) continue;
+      if (cnt[k] >= kMinBoxNodes) {
+        map[k] = k;
+        last = k;
+        for (int64_t q : pending) map[q] = k;
+        pending.clear();
+      } else if (last >= 0) {
+        map[k] = last;
+      } else {
+        pending.push_back(k);
+      }
+    }
+    for (int64_t q : pending) map[q] = pending.front();  // no box reached kMinBoxNodes
+    if (!pending.empty()) map[pending.front()] = pending.front();
+    std::vector<int64_t> mint(nkeys, 0);
+    for (int64_t k = 0; k < nkeys; ++k)
+      if (cnt[k]) mint[map[k]] += cint[k];
+    std::vector<int32_t> cid(nkeys, -1);
+    int32_t n = 0;
+    for (int64_t k = 0; k < nkeys; ++k)
+      if (map[k] == k && mint[k] > 0) cid[k] = n++;
+    if (n > kMaxCoarse) continue;
+    nc = n;
+    for (int64_t i = 0; i < N; ++i) {
+      key[i] = map[key[i]];
+      cbox[i] = bold[i] ? -1 : cid[key[i]];
+    }
+    return;
+  }
+}
 }  // namespace
+
+void spd_inverse(int32_t n, int32_t bw, std::vector<double>& A) {
+  if (n <= 0) return;
+  if (A.size() != static_cast<size_t>(n) * n) throw std::logic_error("spd_inverse: matrix size");
+  bw = std::max<int32_t>(0, std::min<int32_t>(bw, n - 1));
+  const size_t N = static_cast<size_t>(n);
+  // lower Cholesky factor L (row-major), and U = L^T row-major for the backward solves
+  std::vector<double> L(N * N, 0.0);
+  for (int32_t j = 0; j < n; ++j) {
+    const double* Lj = L.data() + j * N;
+    double d = A[j * N + j];
+    for (int32_t k = std::max(0, j - bw); k < j; ++k) d -= Lj[k] * Lj[k];
+    if (!(d > 0.0) || !std::isfinite(d))
+      throw std::runtime_error("coarse Poisson matrix is not positive definite (aggregate " + std::to_string(j) + ")");
+    const double djj = std::sqrt(d);
+    L[j * N + j] = djj;
+    const int32_t iend = std::min(n - 1, j + bw);
+    for (int32_t i = j + 1; i <= iend; ++i) {
+      double* Li = L.data() + i * N;
+      double v = A[i * N + j];
+      for (int32_t k = std::max(0, i - bw); k < j; ++k) v -= Li[k] * Lj[k];
+      Li[j] = v / djj;
+    }
+  }
+  std::vector<double> U(N * N, 0.0);
+  for (size_t i = 0; i < N; ++i)
+    for (size_t k = (i > static_cast<size_t>(bw) ? i - bw : 0); k <= i; ++k) U[k * N + i] = L[i * N + k];
+  // column j of A^-1: L y = e_j (y is zero above j), then L^T x = y
+  parallel_chunks(n, std::max(1, std::min(host_parts(int64_t(1) << 20), n)), [&](int64_t c0, int64_t c1, int) {
+    std::vector<double> y(N);
+    for (int64_t j = c0; j < c1; ++j) {
+      std::fill(y.begin(), y.end(), 0.0);
+      y[j] = 1.0 / L[j * N + j];
+      for (int32_t i = static_cast<int32_t>(j) + 1; i < n; ++i) {
+        const double* Li = L.data() + i * N;
+        double v = 0.0;
+        for (int32_t k = std::max<int32_t>(static_cast<int32_t>(j), i - bw); k < i; ++k) v += Li[k] * y[k];
+        y[i] = -v / Li[i];
+      }
+      for (int32_t i = n - 1; i >= 0; --i) {
+        const double* Ui = U.data() + i * N;
+        double v = y[i];
+        const int32_t kend = std::min(n - 1, i + bw);
+        for (int32_t k = i + 1; k <= kend; ++k) v -= Ui[k] * y[k];
+        y[i] = v / Ui[i];
+      }
+      for (int32_t i = 0; i < n; ++i) A[i * N + j] = y[i];
+    }
+  });
+}
 
 std::vector<int32_t> rcm_order(int64_t N, const int32_t* T, int64_t E) {
   validate(N, T, E);
@@ -234,7 +417,7 @@ int32_t greedy_colour(int64_t N, const int32_t* T, int64_t E, const int64_t* ord
 }
 
 void preprocess(const double* X, int64_t N, const int32_t* T, const int32_t* tag, int64_t E,
-                int32_t nmats, bool reorder, HostMesh& h) {
+                int32_t nmats, bool reorder, int32_t coarse_nodes, HostMesh& h) {
   validate(N, T, E);
   h.N = N;
   h.E = E;
@@ -249,6 +432,8 @@ void preprocess(const double* X, int64_t N, const int32_t* T, const int32_t* tag
   if (static_cast<int32_t>(h.tags.size()) > nmats)
     throw std::runtime_error("materials file has " + std::to_string(nmats) + " rows for " +
                              std::to_string(h.tags.size()) + " element tags");
+  std::vector<uint8_t> bold;
+  boundary_nodes(X, N, T, tag, E, h, bold);
   // ---- node order
   const Graph g = node_graph(N, T, E);
   if (reorder) {
@@ -256,6 +441,13 @@ void preprocess(const double* X, int64_t N, const int32_t* T, const int32_t* tag
   } else {
     h.perm.resize(N);
     std::iota(h.perm.begin(), h.perm.end(), 0);
+  }
+  std::vector<int32_t> cbox;
+  h.nc = 0;
+  if (coarse_nodes > 0) {  // box by box, the order above inside each box
+    std::vector<int64_t> key;
+    coarse_boxes(X, N, bold, coarse_nodes, key, cbox, h.nc);
+    std::stable_sort(h.perm.begin(), h.perm.end(), [&](int32_t a, int32_t b) { return key[a] < key[b]; });
   }
   h.iperm.assign(N, 0);
   for (int64_t i = 0; i < N; ++i) h.iperm[h.perm[i]] = static_cast<int32_t>(i);
@@ -363,45 +555,11 @@ void preprocess(const double* X, int64_t N, const int32_t* T, const int32_t* tag
   h.Xd.assign(3 * h.Npad, 0.0);
   for (int64_t i = 0; i < N; ++i)
     for (int c = 0; c < 3; ++c) h.Xd[3 * h.iperm[i] + c] = X[3 * i + c];
-  // ---- boundary branch, scripts/matrix.py:49-64 and scripts/trafo.py:4-16
-  const double rtol = std::sqrt(std::numeric_limits<double>::epsilon());
-  std::vector<double> rn(N);
-  double Rinf = 0.0;
-  for (int64_t i = 0; i < N; ++i) {
-    rn[i] = std::sqrt(X[3 * i] * X[3 * i] + X[3 * i + 1] * X[3 * i + 1] + X[3 * i + 2] * X[3 * i + 2]);
-    Rinf = std::max(Rinf, rn[i]);
-  }
-  h.Rinf = Rinf;
-  double lsup = 0.0;
-  for (int64_t i = 0; i < N; ++i) lsup = std::max(lsup, std::fabs(rn[i] - Rinf));
-  int64_t at_rinf = 0;
-  for (int64_t i = 0; i < N; ++i) at_rinf += std::fabs(rn[i] - Rinf) <= rtol * lsup;
-  h.airbox = (at_rinf == 8);
-  std::vector<uint8_t> bold(N, 0);
-  if (h.airbox) {
-    for (int c = 0; c < 3; ++c) {
-      double xe = -std::numeric_limits<double>::infinity();
-      for (int64_t i = 0; i < N; ++i) xe = std::max(xe, X[3 * i + c]);
-      for (int sgn = -1; sgn <= 1; sgn += 2) {
-        double ls = 0.0;
-        for (int64_t i = 0; i < N; ++i) ls = std::max(ls, std::fabs(X[3 * i + c] + sgn * xe));
-        for (int64_t i = 0; i < N; ++i)
-          if (std::fabs(X[3 * i + c] + sgn * xe) <= rtol * ls) bold[i] = 1;
-      }
-    }
-  } else {
-    if (h.tags.size() < 2)
-      throw std::runtime_error("spherical-shell boundary needs at least two element tags");
-    for (int64_t i = 0; i < N; ++i) bold[i] = std::fabs(rn[i] - Rinf) <= rtol * lsup;
-    int32_t t2 = h.tags[h.tags.size() - 2];
-    double R = 0.0;
-    for (int64_t e = 0; e < E; ++e)
-      if (tag[e] == t2)
-        for (int a = 0; a < 4; ++a) R = std::max(R, rn[T[4 * e + a]]);
-    h.R = R;
-  }
   h.bnd.assign(h.Npad, 0);
   for (int64_t i = 0; i < N; ++i) h.bnd[h.iperm[i]] = bold[i];
+  h.rbox.assign(h.Npad, -1);
+  if (h.nc > 0)
+    for (int64_t i = 0; i < N; ++i) h.rbox[h.iperm[i]] = cbox[i];
 }
 
 }  // namespace mumag

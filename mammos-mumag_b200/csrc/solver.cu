@@ -30,6 +30,7 @@
 
 #include <algorithm>
 #include <cfloat>
+#include <climits>
 #include <cmath>
 #include <stdexcept>
 #include <string>
@@ -199,6 +200,13 @@ struct Ctx {
   unsigned char* tcsm = nullptr;
   uint32_t tctm = 0, tcph = 0;
   bool tcbad = false;
+  // two-level preconditioner (a.nc > 0), shared memory: the restricted search direction
+  // Ps = P^T s and residual Pr = P^T r of every box (each CTA keeps all of them, updated
+  // by the same recurrences in the same order), xc = Ac^-1 Pr of the CTA's own boxes, and
+  // per slice of the CTA the (at most two) boxes its rows belong to with their partial sums
+  double *cPs = nullptr, *cPr = nullptr, *cxc = nullptr, *csv = nullptr;
+  int* csb = nullptr;
+  int cb0 = 0, cnb = 0, cslot0 = 0;
   __device__ Ctx(const SolveArgs& args) : a(args), h(args.h) {}
 };
 
@@ -812,7 +820,7 @@ __device__ __noinline__ bool pcg_inner2(Ctx& c, double alpha, double beta, doubl
 template <bool TC>
 __device__ __noinline__ bool pcg_solve_mixed(Ctx& c, const double* x) {
   const SolveArgs& a = c.a;
-  const double* Dk = plane(a, P_D);
+  const float* Dk = a.vals32 + (size_t)P_D * a.nent;  // FP32 divergence planes, FP64 sums
   const double* S64 = plane(a, P_S);
   const int64_t ps = a.nent;
   const int n = a.Npad;
@@ -942,6 +950,400 @@ __device__ __noinline__ bool pcg_solve_mixed(Ctx& c, const double* x) {
 }
 
 // ---------------------------------------------------------------------------------------
+// Two-level additive preconditioner of the Poisson PCG (no counterpart in the reference,
+// whose jax.scipy.sparse.linalg.cg at scripts/solvers.py:221-231 uses Jacobi):
+//   z = M^-1 r = r / diag S + P xc,   xc = Ac^-1 P^T r,   Ac = P^T S P,
+// with P constant on spatial boxes of interior rows (rows are numbered box by box).  The
+// Jacobi part removes the local error, the box part the smooth, mesh-wide error that sets
+// Jacobi-CG's iteration count.  The stop test stays the reference's r.r <= tol_u^2 b.b, so
+// only the path to the solution changes.
+//
+// P^T r is carried by the same recurrence as r (P^T r <- P^T r - alpha P^T s,
+// P^T s <- P^T w + beta P^T s), so the only new exchange per iteration is the box sums of
+// w = S z: each CTA sums its rows per box (warp sums per slice, then slices in order) and
+// publishes one partial per box it holds rows of, in slots ordered CTA by CTA; after the
+// iteration's reduction every CTA adds up every box's slots in slot order (bit-identical in
+// all CTAs) and updates its copy of P^T s and P^T r.  Each CTA then needs xc only for its
+// own boxes: its rows of the dense Ac^-1 (L2-resident) times P^T r.
+// ---------------------------------------------------------------------------------------
+__device__ __forceinline__ int warp_min_i(int v) {
+  for (int o = 16; o > 0; o >>= 1) v = min(v, __shfl_xor_sync(0xffffffffu, v, o));
+  return v;
+}
+__device__ __forceinline__ int warp_max_i(int v) {
+  for (int o = 16; o > 0; o >>= 1) v = max(v, __shfl_xor_sync(0xffffffffu, v, o));
+  return v;
+}
+
+// Sums of v over the rows of slice t (CTA-local index) in each of the slice's boxes; called
+// by all 32 lanes of the warp (lane = row i of the slice).
+__device__ __forceinline__ void coarse_slice_sum(const Ctx& c, int t, int i, double v) {
+  const int lo = c.csb[2 * t], hi = c.csb[2 * t + 1];
+  const int rb = __ldg(c.a.rbox + i);
+  const double slo = warp_sum((lo >= 0 && rb == lo) ? v : 0.0);
+  const double shi = hi != lo ? warp_sum(rb == hi ? v : 0.0) : 0.0;
+  if (c.lane == 0) {
+    c.csv[2 * t] = slo;
+    c.csv[2 * t + 1] = shi;
+  }
+}
+
+// The CTA's partial sum of each of its boxes, slices in order, into its slots.  Must come
+// before the grid reduction (or barrier) that publishes them.
+__device__ __forceinline__ void coarse_publish(const Ctx& c) {
+  __syncthreads();
+  const int ns = c.s1 - c.s0;
+  for (int q = threadIdx.x; q < c.cnb; q += blockDim.x) {
+    const int box = c.cb0 + q;
+    double acc = 0.0;
+    for (int t = 0; t < ns; ++t) {
+      if (c.csb[2 * t] == box)
+        acc += c.csv[2 * t];
+      else if (c.csb[2 * t + 1] == box)
+        acc += c.csv[2 * t + 1];
+    }
+    c.a.bslots[c.cslot0 + q] = acc;
+  }
+}
+
+// After the barrier: every box's total (its slots in order) folded into the coarse vectors.
+// restart: Pr = total, Ps = 0 (a fresh residual); else Ps = total + beta Ps, Pr -= alpha Ps.
+__device__ __forceinline__ void coarse_gather(const Ctx& c, bool restart, double alpha, double beta) {
+  const SolveArgs& a = c.a;
+  for (int q = threadIdx.x; q < a.nc; q += blockDim.x) {
+    const int t0 = __ldg(a.bslot + q), t1 = __ldg(a.bslot + q + 1);
+    double w = 0.0;
+    for (int t = t0; t < t1; ++t) w += __ldcg(a.bslots + t);
+    if (restart) {
+      c.cPr[q] = w;
+      c.cPs[q] = 0.0;
+    } else {
+      const double ps = w + beta * c.cPs[q];
+      c.cPs[q] = ps;
+      c.cPr[q] -= alpha * ps;
+    }
+  }
+  __syncthreads();
+}
+
+// xc = Ac^-1 Pr for the CTA's own boxes: a warp per box, lanes along the row.
+template <class AT>
+__device__ __forceinline__ void coarse_solve_own(const Ctx& c, const AT* Ainv) {
+  const int nc = c.a.nc;
+  for (int q = c.warp; q < c.cnb; q += c.nwarps) {
+    const int box = c.cb0 + q;
+    const AT* row = Ainv + (size_t)box * nc;
+    double acc = 0.0;
+    for (int j = c.lane; j < nc; j += 32) acc += (double)__ldg(row + j) * c.cPr[j];
+    acc = warp_sum(acc);
+    if (c.lane == 0) c.cxc[box] = acc;
+  }
+  __syncthreads();
+}
+
+// Pr = P^T v for a residual v given per row by val(i) (after a warm start changed it).
+template <class F>
+__device__ __noinline__ bool coarse_restrict(Ctx& c, F val) {
+  FOR_ROWS(c)
+  (void)w_;
+  coarse_slice_sum(c, s_ - c.s0, i, val(i));
+  END_ROWS
+  coarse_publish(c);
+  CHECK(grid_barrier(c.sy));
+  coarse_gather(c, true, 0.0, 0.0);
+  return true;
+}
+
+// The FP64 Poisson solve with the two-level preconditioner, in the two-sync
+// Chronopoulos-Gear arrangement of pcg_loop2 (update phase, barrier, SpMV phase,
+// reduction): r, w, s, 1/diag in the planes of rec[0], z in the first plane of rec[1].
+template <bool TC>
+__device__ __noinline__ bool pcg_solve_coarse(Ctx& c, const double* x) {
+  const SolveArgs& a = c.a;
+  const double* Dk = plane(a, P_D);
+  const int64_t ps = a.nent;
+  const int n = a.Npad;
+  double* pl = reinterpret_cast<double*>(a.rec[0]);
+  double* z = reinterpret_cast<double*>(a.rec[1]);
+  double rr, bb, zz;
+  const bool zero_start = a.warm == WARM_ZERO;
+  {  // b = sum_k dk x_k, r0 = b - S u, and its box sums
+    double pr2 = 0, pb = 0, pz = 0;
+    FOR_ROWS(c)
+    double b = 0, su = 0;
+#pragma unroll 4
+    for (int k = 0; k < w_; ++k) {
+      const int64_t e = ENTRY(k);
+      const int j = c.scol[LENTRY(k)];
+      b += __ldg(Dk + e) * x[j] + __ldg(Dk + ps + e) * x[n + j] + __ldg(Dk + 2 * ps + e) * x[2 * n + j];
+      if (!zero_start) su += c.sS[LENTRY(k)] * a.u[j];
+    }
+    if (zero_start) a.u[i] = 0.0;
+    const double r = b - su;
+    const double invd = __ldg(a.invdS + i);
+    rec_store(a.rec[0], i, n, PcgRec{r, 0.0, 0.0, invd});
+    pr2 += r * r;
+    pb += b * b;
+    if (i < a.nreal) pz += (r * invd) * (r * invd);
+    coarse_slice_sum(c, s_ - c.s0, i, r);
+    END_ROWS
+    coarse_publish(c);
+    double v[3] = {pr2, pb, pz};
+    CHECK(grid_reduce<3>(c.sy, v, 0u));
+    rr = v[0];
+    bb = v[1];
+    zz = v[2];
+  }
+  const double atol2 = fmax(a.tol_u * a.tol_u * bb, 0.0);
+  int k = 0;
+  if (!(rr > atol2 && k < a.max_pcg)) return true;
+  coarse_gather(c, true, 0.0, 0.0);
+  const double sig = sqrt(zz / (double)a.nreal);
+  const bool recording = a.rec_cap > 0 && sig > 0.0;
+  if (recording) record_features(c, x, pl, 1.0 / sig);
+  if (a.warm == WARM_LEARNED && sig > 0.0) {
+    double gunused;
+    CHECK(learned_start<TC>(c, x, sig, gunused, rr));
+    if (!(rr > atol2)) {
+      if (recording) record_targets(c, sig);
+      return true;
+    }
+    CHECK(coarse_restrict(c, [&](int i) { return pl[i]; }));
+  }
+  // z0 = r0/diag + P xc, p = 0, gamma = r0.z0
+  double gamma, delta;
+  coarse_solve_own(c, a.Ainv);
+  {
+    double pg = 0;
+    FOR_ROWS(c)
+    (void)w_;
+    const double r = pl[i], invd = pl[3 * n + i];
+    const int rb = __ldg(a.rbox + i);
+    const double z0 = r * invd + (rb >= 0 ? c.cxc[rb] : 0.0);
+    z[i] = z0;
+    a.pp[i] = 0.0;
+    pg += r * z0;
+    END_ROWS
+    double v[1] = {pg};
+    CHECK(grid_reduce<1>(c.sy, v, 0u));
+    gamma = v[0];
+  }
+  {  // w0 = S z0, delta = w0.z0, box sums of w0
+    double pd = 0;
+    FOR_ROWS(c)
+    const double acc = gather_row<double, double, double, 8>(c, c.sS, loff_, w_, z);
+    rec_store_w(a.rec[0], i, n, acc);
+    pd += acc * z[i];
+    coarse_slice_sum(c, s_ - c.s0, i, acc);
+    END_ROWS
+    coarse_publish(c);
+    double v[1] = {pd};
+    CHECK(grid_reduce<1>(c.sy, v, 0u));
+    delta = v[0];
+  }
+  double alpha = gamma / delta, beta = 0.0;
+  coarse_gather(c, false, alpha, beta);
+  for (;;) {
+    if (c.sy.timing && threadIdx.x == 0) c.t_phase_start = globaltimer();
+    coarse_solve_own(c, a.Ainv);
+    double pg = 0, pd = 0, pr2 = 0;
+    FOR_ROWS(c)
+    (void)w_;
+    const PcgRec q = rec_load(a.rec[0], i, n);
+    const double sn = q.w + beta * q.s;
+    const double r = q.r - alpha * sn;
+    const int rb = __ldg(a.rbox + i);
+    const double zn = r * q.invd + (rb >= 0 ? c.cxc[rb] : 0.0);
+    const double p = z[i] + beta * a.pp[i];
+    a.pp[i] = p;
+    a.u[i] = a.u[i] + alpha * p;
+    pl[i] = r;
+    pl[2 * n + i] = sn;
+    z[i] = zn;
+    pg += r * zn;
+    pr2 += r * r;
+    END_ROWS
+    CHECK(grid_barrier(c.sy));
+    FOR_ROWS(c)
+    const double acc = gather_row<double, double, double, 8>(c, c.sS, loff_, w_, z);
+    rec_store_w(a.rec[0], i, n, acc);
+    pd += acc * z[i];
+    coarse_slice_sum(c, s_ - c.s0, i, acc);
+    END_ROWS
+    coarse_publish(c);
+    double v[3] = {pg, pd, pr2};
+    if (c.sy.timing && threadIdx.x == 0) c.t_pcg_phase += globaltimer() - c.t_phase_start;
+    CHECK(grid_reduce<3>(c.sy, v, 0u));
+    ++k;
+    rr = v[2];
+    if (!(rr > atol2 && k < a.max_pcg)) break;
+    const double bn = v[0] / gamma;
+    alpha = v[0] / (v[1] - bn * v[0] / alpha);
+    beta = bn;
+    gamma = v[0];
+    coarse_gather(c, false, alpha, beta);
+  }
+  c.pcg_iters += k;
+  if (recording) record_targets(c, sig);
+  return true;
+}
+
+// Mixed precision with the two-level preconditioner: pcg_solve_mixed's FP64 residual
+// refinement around FP32 inner solves, each inner solve preconditioned as above (FP32
+// Ac^-1 rows, FP64 box sums and coarse vectors); records in rec32[0], z in rec32[1].
+template <bool TC>
+__device__ __noinline__ bool pcg_solve_mixed_coarse(Ctx& c, const double* x) {
+  const SolveArgs& a = c.a;
+  const float* Dk = a.vals32 + (size_t)P_D * a.nent;  // FP32 divergence planes, FP64 sums
+  const int64_t ps = a.nent;
+  const int n = a.Npad;
+  PcgRec32* rc = a.rec32[0];
+  float* z = reinterpret_cast<float*>(a.rec32[1]);
+  double rr, bb, zz;
+  const bool zero_start = a.warm == WARM_ZERO;
+  {  // FP64 residual of the warm start, FP32 inner record, box sums of the FP32 residual
+    double p0 = 0, p1 = 0, pz = 0;
+    FOR_ROWS(c)
+    double b = 0, su = 0;
+#pragma unroll 4
+    for (int k = 0; k < w_; ++k) {
+      const int64_t e = ENTRY(k);
+      const int j = c.scol[LENTRY(k)];
+      b += __ldg(Dk + e) * x[j] + __ldg(Dk + ps + e) * x[n + j] + __ldg(Dk + 2 * ps + e) * x[2 * n + j];
+      if (!zero_start) su += c.sS[LENTRY(k)] * a.u[j];
+    }
+    if (zero_start) a.u[i] = 0.0;
+    const double r = b - su;
+    const double invd = __ldg(a.invdS + i);
+    const float rf = (float)r, inv = (float)invd;
+    a.r64[i] = r;
+    rc[i] = PcgRec32{rf, 0.f, 0.f, inv};
+    p0 += r * r;
+    p1 += b * b;
+    if (i < a.nreal) pz += (r * invd) * (r * invd);
+    coarse_slice_sum(c, s_ - c.s0, i, (double)rf);
+    END_ROWS
+    coarse_publish(c);
+    double v[3] = {p0, p1, pz};
+    CHECK(grid_reduce<3>(c.sy, v, 0u));
+    rr = v[0];
+    bb = v[1];
+    zz = v[2];
+  }
+  const double atol2 = fmax(a.tol_u * a.tol_u * bb, 0.0);
+  int k = 0;
+  const double sig = sqrt(zz / (double)a.nreal);
+  const bool active = rr > atol2 && a.max_pcg > 0;
+  const bool recording = active && a.rec_cap > 0 && sig > 0.0;
+  if (active) coarse_gather(c, true, 0.0, 0.0);
+  if (recording) record_features(c, x, a.r64, 1.0 / sig);
+  if (active && a.warm == WARM_LEARNED && sig > 0.0) {
+    double rin2, gin;
+    CHECK(learned_start_mixed<TC>(c, x, sig, rr, rin2, gin));
+    if (rr > atol2) CHECK(coarse_restrict(c, [&](int i) { return (double)rc[i].r; }));
+  }
+  for (int outer = 0; rr > atol2 && k < a.max_pcg && outer < 32; ++outer) {
+    // z0 = rf/diag + P xc, p = e = 0; gamma = rf.z0, rin2 = rf.rf
+    double gamma, rin2, delta;
+    coarse_solve_own(c, a.Ainv32);
+    {
+      double pg = 0, p2 = 0;
+      FOR_ROWS(c)
+      (void)w_;
+      const PcgRec32 q = rc[i];
+      const int rb = __ldg(a.rbox + i);
+      const float z0 = q.r * q.invd + (rb >= 0 ? (float)c.cxc[rb] : 0.f);
+      z[i] = z0;
+      a.pp32[i] = 0.f;
+      a.e32[i] = 0.f;
+      pg += (double)q.r * (double)z0;
+      p2 += (double)q.r * (double)q.r;
+      END_ROWS
+      double v[2] = {pg, p2};
+      CHECK(grid_reduce<2>(c.sy, v, 0u));
+      gamma = v[0];
+      rin2 = v[1];
+    }
+    const double inner_tol2 = fmax(1e-10 * rin2, 0.25 * atol2);  // 1e-5 relative, or the outer target
+    {  // w0 = S32 z0, delta = w0.z0, box sums of w0
+      double pd = 0;
+      FOR_ROWS(c)
+      const float acc = gather_row<float, float, float, kChunk32>(c, c.sS32, loff_, w_, z);
+      rc[i].w = acc;
+      pd += (double)acc * (double)z[i];
+      coarse_slice_sum(c, s_ - c.s0, i, (double)acc);
+      END_ROWS
+      coarse_publish(c);
+      double v[1] = {pd};
+      CHECK(grid_reduce<1>(c.sy, v, 0u));
+      delta = v[0];
+    }
+    double alpha = gamma / delta, beta = 0.0;
+    coarse_gather(c, false, alpha, beta);
+    for (;;) {
+      coarse_solve_own(c, a.Ainv32);
+      const float af = (float)alpha, bf = (float)beta;
+      double pg = 0, pd = 0, pr2 = 0;
+      FOR_ROWS(c)
+      (void)w_;
+      const PcgRec32 q = rc[i];
+      const float sn = q.w + bf * q.s;
+      const float r = q.r - af * sn;
+      const int rb = __ldg(a.rbox + i);
+      const float zn = r * q.invd + (rb >= 0 ? (float)c.cxc[rb] : 0.f);
+      const float p = z[i] + bf * a.pp32[i];
+      a.pp32[i] = p;
+      a.e32[i] = a.e32[i] + af * p;
+      rc[i] = PcgRec32{r, q.w, sn, q.invd};
+      z[i] = zn;
+      pg += (double)r * (double)zn;
+      pr2 += (double)r * (double)r;
+      END_ROWS
+      CHECK(grid_barrier(c.sy));
+      FOR_ROWS(c)
+      const float acc = gather_row<float, float, float, kChunk32>(c, c.sS32, loff_, w_, z);
+      rc[i].w = acc;
+      pd += (double)acc * (double)z[i];
+      coarse_slice_sum(c, s_ - c.s0, i, (double)acc);
+      END_ROWS
+      coarse_publish(c);
+      double v[3] = {pg, pd, pr2};
+      CHECK(grid_reduce<3>(c.sy, v, 0u));
+      ++k;
+      if (!(v[2] > inner_tol2 && k < a.max_pcg)) break;
+      const double bn = v[0] / gamma;
+      alpha = v[0] / (v[1] - bn * v[0] / alpha);
+      beta = bn;
+      gamma = v[0];
+      coarse_gather(c, false, alpha, beta);
+    }
+    {  // u += e, r -= S e in FP64; next inner record and its box sums
+      double p0 = 0;
+      FOR_ROWS(c)
+      double se = 0;
+#pragma unroll 8
+      for (int k2 = 0; k2 < w_; ++k2) se += c.sS[LENTRY(k2)] * (double)a.e32[c.scol[LENTRY(k2)]];
+      a.u[i] = a.u[i] + (double)a.e32[i];
+      const double r = a.r64[i] - se;
+      a.r64[i] = r;
+      const float rf = (float)r, inv = (float)__ldg(a.invdS + i);
+      rc[i] = PcgRec32{rf, 0.f, 0.f, inv};
+      p0 += r * r;
+      coarse_slice_sum(c, s_ - c.s0, i, (double)rf);
+      END_ROWS
+      coarse_publish(c);
+      double v[1] = {p0};
+      CHECK(grid_reduce<1>(c.sy, v, 0u));
+      rr = v[0];
+    }
+    if (rr > atol2 && k < a.max_pcg) coarse_gather(c, true, 0.0, 0.0);
+  }
+  c.pcg_iters += k;
+  if (recording) record_targets(c, sig);
+  return true;
+}
+
+// ---------------------------------------------------------------------------------------
 // total_eg, scripts/energies.py:67-99
 // ---------------------------------------------------------------------------------------
 struct EvalOut {
@@ -954,7 +1356,12 @@ struct EvalOut {
 template <bool TC>
 __device__ bool eval(Ctx& c, const double* x, const double* xref, const double* d, double* gout, EvalOut& o) {
   const SolveArgs& a = c.a;
-  if (a.hmag_on > 0) CHECK(a.mixed ? pcg_solve_mixed<TC>(c, x) : pcg_solve<TC>(c, x));
+  if (a.hmag_on > 0) {
+    if (a.nc > 0)
+      CHECK(a.mixed ? pcg_solve_mixed_coarse<TC>(c, x) : pcg_solve_coarse<TC>(c, x));
+    else
+      CHECK(a.mixed ? pcg_solve_mixed<TC>(c, x) : pcg_solve<TC>(c, x));
+  }
   const int n = a.Npad;
   const double* G = plane(a, P_G);
   const int64_t ps = a.nent;
@@ -964,16 +1371,32 @@ __device__ bool eval(Ctx& c, const double* x, const double* xref, const double* 
   double pE = 0, pgd = 0, pdx = 0, px = 0, pgi = 0;
   FOR_ROWS(c)
   double gc[3];
-  apply_C_row(c, x, off_, loff_, w_, gc);
   double gh0 = 0, gh1 = 0, gh2 = 0;
-  if (a.hmag_on > 0) {
+  if (a.mixed) {  // FP32 operator values, FP64 vectors and sums
+    apply_C_row_t<float>(c, a.vals32 + (size_t)P_AEX * a.nent, a.vals32 + (size_t)P_K * a.nent, x, off_, loff_, w_,
+                         gc);
+    if (a.hmag_on > 0) {
+      const float* G32 = a.vals32 + (size_t)P_G * a.nent;
 #pragma unroll 4
-    for (int k = 0; k < w_; ++k) {
-      const int64_t e = ENTRY(k);
-      const double uj = a.u[c.scol[LENTRY(k)]];
-      gh0 += __ldg(G + e) * uj;
-      gh1 += __ldg(G + ps + e) * uj;
-      gh2 += __ldg(G + 2 * ps + e) * uj;
+      for (int k = 0; k < w_; ++k) {
+        const int64_t e = ENTRY(k);
+        const double uj = a.u[c.scol[LENTRY(k)]];
+        gh0 += (double)__ldg(G32 + e) * uj;
+        gh1 += (double)__ldg(G32 + ps + e) * uj;
+        gh2 += (double)__ldg(G32 + 2 * ps + e) * uj;
+      }
+    }
+  } else {
+    apply_C_row(c, x, off_, loff_, w_, gc);
+    if (a.hmag_on > 0) {
+#pragma unroll 4
+      for (int k = 0; k < w_; ++k) {
+        const int64_t e = ENTRY(k);
+        const double uj = a.u[c.scol[LENTRY(k)]];
+        gh0 += __ldg(G + e) * uj;
+        gh1 += __ldg(G + ps + e) * uj;
+        gh2 += __ldg(G + 2 * ps + e) * uj;
+      }
     }
   }
   const double mi = __ldg(a.meas + i);
@@ -1444,6 +1867,26 @@ __device__ __forceinline__ void solve_body(const SolveArgs& args, int nblk, int 
     c.scol = args.col;
     c.cbase = 0;
   }
+  if (args.nc > 0) {  // the coarse vectors and the boxes of each of the CTA's slices
+    double* base = reinterpret_cast<double*>(smem + args.co_off);
+    c.cPs = base;
+    c.cPr = base + args.nc;
+    c.cxc = base + 2 * args.nc;
+    c.csv = base + 3 * args.nc;
+    c.csb = reinterpret_cast<int*>(c.csv + 2 * args.meta_max);
+    c.cb0 = __ldg(args.ctabox + 3 * blk);
+    c.cnb = __ldg(args.ctabox + 3 * blk + 1);
+    c.cslot0 = __ldg(args.ctabox + 3 * blk + 2);
+    for (int t = c.warp; t < c.s1 - c.s0; t += c.nwarps) {
+      const int rb = __ldg(args.rbox + (size_t)(c.s0 + t) * 32 + c.lane);
+      const int lo = warp_min_i(rb >= 0 ? rb : INT_MAX), hi = warp_max_i(rb);
+      if (c.lane == 0) {
+        c.csb[2 * t] = lo == INT_MAX ? -1 : lo;
+        c.csb[2 * t + 1] = hi;
+      }
+    }
+    __syncthreads();
+  }
   if constexpr (TC) {
     if (args.warm == WARM_LEARNED && args.tc_off >= 0 && blockDim.x == kTcThreads &&
         (args.mode == MODE_EVAL || args.mode == MODE_MINIMIZE || args.mode == MODE_SWEEP)) {
@@ -1522,8 +1965,12 @@ struct StagePlan {
   int64_t stage_max, meta_max;
   size_t smem;
   int extra_off;  // offset of the extra region, -1 = none
+  int co_off;     // offset of the coarse region, -1 = none
 };
-StagePlan stage_plan(const DevMesh& m, int grid, size_t limit, size_t extra = 0, bool allow_stage = true) {
+// Regions: [staged entries][slice metadata][coarse vectors: Ps, Pr, xc (nc doubles each),
+// per slice two partial sums and two box ids][tensor-core network]
+StagePlan stage_plan(const DevMesh& m, int grid, size_t limit, size_t extra = 0, bool allow_stage = true,
+                     int nc = 0) {
   int64_t emax = 0, smax = 0;
   for (int b = 0; b < grid; ++b) {
     const int64_t s0 = (m.h.nslices * b) / grid, s1 = (m.h.nslices * (b + 1)) / grid;
@@ -1531,18 +1978,69 @@ StagePlan stage_plan(const DevMesh& m, int grid, size_t limit, size_t extra = 0,
     smax = std::max(smax, s1 - s0);
   }
   const size_t meta = (size_t)smax * (sizeof(int64_t) + sizeof(int32_t));
+  const size_t coarse =
+      nc > 0 ? (size_t)(3 * nc + 2 * smax) * sizeof(double) + (size_t)2 * smax * sizeof(int) + 16 : 0;
   const size_t need = (size_t)emax * (sizeof(double) + sizeof(int32_t) + (m.vals32 ? sizeof(float) : 0));
   StagePlan p;
-  p.stage = (allow_stage && need + meta + 16 + (extra ? extra + 1024 : 0) <= limit) ? 1 : 0;
+  p.stage = (allow_stage && need + meta + 16 + coarse + (extra ? extra + 1024 : 0) <= limit) ? 1 : 0;
   p.stage_max = emax;
   p.meta_max = smax;
   p.smem = (p.stage ? ((need + 15) & ~(size_t)15) : 0) + meta;
+  p.co_off = -1;
+  if (coarse) {
+    p.co_off = (int)((p.smem + 15) & ~(size_t)15);
+    p.smem = (size_t)p.co_off + coarse;
+  }
   p.extra_off = -1;
   if (extra) {  // the tensor-core network's region, 1024-byte aligned, after the metadata
     p.extra_off = (int)((p.smem + 1023) & ~(size_t)1023);
     p.smem = (size_t)p.extra_off + extra;
   }
   return p;
+}
+
+// The two-level preconditioner's per-CTA plan for a grid: the boxes each CTA holds rows of
+// (a contiguous range: rows are numbered box by box), one partial-sum slot per (CTA, box)
+// in CTA order, and each box's slot range (contiguous: consecutive CTAs share at most their
+// boundary box).  Also checks that no SELL slice meets more than two boxes.
+void coarse_plan(DevMesh& m) {
+  const HostMesh& h = m.h;
+  const int nc = m.nc, grid = m.grid;
+  for (int64_t s = 0; s < h.nslices; ++s) {
+    int lo = INT_MAX, hi = -1;
+    for (int l = 0; l < kSlice; ++l) {
+      const int rb = h.rbox[s * kSlice + l];
+      if (rb >= 0) {
+        lo = std::min(lo, rb);
+        hi = std::max(hi, rb);
+      }
+    }
+    if (hi >= 0 && hi - lo > 1) throw std::logic_error("a SELL slice meets more than two aggregate boxes");
+  }
+  std::vector<int32_t> cta(3 * (size_t)grid), bsl(nc + 1, -1);
+  int32_t slot = 0;
+  for (int b = 0; b < grid; ++b) {
+    const int64_t s0 = (h.nslices * b) / grid, s1 = (h.nslices * (b + 1)) / grid;
+    int lo = INT_MAX, hi = -1;
+    for (int64_t i = s0 * kSlice; i < s1 * kSlice; ++i)
+      if (h.rbox[i] >= 0) {
+        lo = std::min(lo, h.rbox[i]);
+        hi = std::max(hi, h.rbox[i]);
+      }
+    const int nb = hi >= 0 ? hi - lo + 1 : 0;
+    cta[3 * b] = nb ? lo : 0;
+    cta[3 * b + 1] = nb;
+    cta[3 * b + 2] = slot;
+    for (int q = 0; q < nb; ++q)
+      if (bsl[lo + q] < 0) bsl[lo + q] = slot + q;
+    slot += nb;
+  }
+  bsl[nc] = slot;
+  for (int q = 0; q < nc; ++q)
+    if (bsl[q] < 0 || bsl[q + 1] < bsl[q]) throw std::logic_error("aggregate box without rows in the CTA plan");
+  if (slot > nc + kMaxGrid) throw std::logic_error("aggregate box slots overflow");
+  MM_CK(cudaMemcpy(m.ctabox, cta.data(), sizeof(int32_t) * cta.size(), cudaMemcpyHostToDevice));
+  MM_CK(cudaMemcpy(m.bslot, bsl.data(), sizeof(int32_t) * bsl.size(), cudaMemcpyHostToDevice));
 }
 }  // namespace
 
@@ -1576,12 +2074,13 @@ void solver_configure(DevMesh& m) {
   // share SMs, would lose residency to the region and keep the network on mma.sync.
   const size_t extra =
       (m.warm == WARM_LEARNED && block == kTcThreads && grid <= prop.multiProcessorCount) ? (size_t)kSmTc : 0;
-  const StagePlan sp = stage_plan(m, grid, limit, extra, m.opt.stage_operators != 0);
+  const StagePlan sp = stage_plan(m, grid, limit, extra, m.opt.stage_operators != 0, m.nc);
   m.stage = sp.stage;
   m.stage_max = sp.stage_max;
   m.meta_max = sp.meta_max;
   m.smem = sp.smem;
   m.tc_off = sp.extra_off;
+  m.co_off = sp.co_off;
   // The attribute is per kernel, shared by every mesh: raise it to the device limit once
   // (occupancy follows each launch's actual request).
   const int dsm = (int)(prop.sharedMemPerBlockOptin - 16 * 1024);
@@ -1597,6 +2096,7 @@ void solver_configure(DevMesh& m) {
   grid = std::min(grid, occ * prop.multiProcessorCount);
   m.grid = grid;
   m.block = block;
+  if (m.nc > 0) coarse_plan(m);
 }
 
 void batch_configure(const std::vector<DevMesh*>& ms, BatchPlan& plan) {
@@ -1725,6 +2225,14 @@ SolveArgs solver_args(const DevMesh& m, int mode, double h, const mm_solver_para
   a.r64 = m.r64;
   a.pcg2 = m.pcg2;
   a.tc_off = m.tc_off;
+  a.nc = m.nc;
+  a.rbox = m.rbox;
+  a.Ainv = m.Ainv;
+  a.Ainv32 = m.Ainv32;
+  a.bslots = m.bslots;
+  a.bslot = m.bslot;
+  a.ctabox = m.ctabox;
+  a.co_off = m.co_off;
   a.bar_stall = m.bar_stall;
   a.warm = m.warm;
   a.nreal = (int32_t)m.h.N;

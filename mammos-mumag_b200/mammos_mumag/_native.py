@@ -73,6 +73,7 @@ EXPORTED = (
     "mm_mesh_record_samples",
     "mm_mesh_read_samples",
     "mm_debug_stall_barriers",
+    "mm_mesh_get_coarse",
 )
 WARM_PREVIOUS, WARM_ZERO, WARM_LEARNED = 0, 1, 2
 MLP_FEATURES = 16
@@ -94,6 +95,7 @@ class Options(C.Structure):
         ("pcg_variant", C.c_int),
         ("ctas_per_sm", C.c_int),
         ("stage_operators", C.c_int),
+        ("coarse_box_nodes", C.c_int),
     ]
 
 
@@ -148,6 +150,7 @@ class MeshInfo(C.Structure):
         ("pcg_variant", C.c_int32),
         ("kernel_ctas_per_sm", C.c_int32),
         ("staged", C.c_int32),
+        ("coarse_boxes", C.c_int32),
     ]
 
     def as_dict(self):
@@ -251,6 +254,7 @@ def load():
         "mm_mesh_record_samples": (C.c_int, [C.c_void_p, C.c_int64, C.c_int32, C.c_uint64]),
         "mm_mesh_read_samples": (C.c_int, [C.c_void_p, _F, _F, _I32, C.c_int64, _I64]),
         "mm_debug_stall_barriers": (C.c_int, [C.c_void_p, C.c_int32]),
+        "mm_mesh_get_coarse": (C.c_int, [C.c_void_p, _I32, _I32]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -355,7 +359,8 @@ class Mesh:
     """Device operators of one mesh (an ``mm_mesh`` handle)."""
 
     def __init__(self, X, T, tag, materials, size=1e-9, dirichlet_rhs=0, precision=PREC_FP64, device=0,
-                 grid_ctas=0, block_threads=0, reorder=1, pcg_variant=0, ctas_per_sm=0, stage_operators=1):
+                 grid_ctas=0, block_threads=0, reorder=1, pcg_variant=0, ctas_per_sm=0, stage_operators=1,
+                 coarse_box_nodes=0):
         lib = load()
         self.X = np.ascontiguousarray(X, dtype=np.float64)
         self.T = np.ascontiguousarray(T, dtype=np.int32)
@@ -366,7 +371,7 @@ class Mesh:
         opt = default_options(size=size, dirichlet_rhs=dirichlet_rhs, precision=precision, device=device,
                               grid_ctas=grid_ctas, block_threads=block_threads, reorder=reorder,
                               pcg_variant=pcg_variant, ctas_per_sm=ctas_per_sm,
-                              stage_operators=stage_operators)
+                              stage_operators=stage_operators, coarse_box_nodes=coarse_box_nodes)
         h = C.c_void_p()
         check(lib.mm_mesh_create(_dp(self.X), self.N, self.T.ctypes.data_as(_I32), self.tag.ctypes.data_as(_I32),
                                  self.E, mats, len(rows), C.byref(opt), C.byref(h)))
@@ -409,6 +414,14 @@ class Mesh:
         check(load().mm_mesh_read_samples(self._h, _fp(f), _fp(t), n.ctypes.data_as(_I32), cap, C.byref(k)))
         k = k.value
         return f[:k].copy(), t[:k].copy(), n[:k].copy()
+
+    def coarse(self):
+        """The two-level preconditioner's aggregates: ``(box [N] int32 in mesh-file order,
+        -1 for Dirichlet nodes; number of boxes)``; ``(None, 0)`` with the Jacobi preconditioner."""
+        box = np.empty(self.N, np.int32)
+        nb = C.c_int32()
+        check(load().mm_mesh_get_coarse(self._h, box.ctypes.data_as(_I32), C.byref(nb)))
+        return (box, nb.value) if nb.value > 0 else (None, 0)
 
     def debug_stall_barriers(self, stall: int):
         """Test hook of the failure path: with stall > 0 every grid barrier of later launches

@@ -68,6 +68,7 @@ __all__ = [
     "alpha_init",
     "dot_magnetizations",
     "pcg",
+    "pcg_twolevel",
     "truncated_cg",
     "m_inv",
     "hestenes_stiefel_ncg",
@@ -336,6 +337,43 @@ def pcg(A, D, b, x0, tol, atol=0.0, maxiter=10000):
         gamma_ = r @ z
         beta = gamma_ / gamma
         p = z + beta * p
+        gamma = gamma_
+        k += 1
+    return x, k
+
+
+def pcg_twolevel(A, D, b, x0, tol, box, atol=0.0, maxiter=10000):
+    """PCG with the CUDA path's optional two-level additive preconditioner (no counterpart
+    in the reference, whose ``scripts/solvers.py:221-231`` uses Jacobi):
+    ``z = r / D + P Ac^-1 P^T r`` with ``P[i, box[i]] = 1`` (``box[i] = -1``: no box) and
+    ``Ac = P^T A P``.  Same stop rule as ``pcg`` (the reference's).  Returns ``(x, iterations)``."""
+    box = np.asarray(box)
+    nc = int(box.max()) + 1
+    rows = np.nonzero(box >= 0)[0]
+    P = sp.csr_matrix((np.ones(len(rows)), (rows, box[rows])), shape=(A.shape[0], nc))
+    Ac = (P.T @ A @ P).toarray()
+    Ainv = np.linalg.inv(Ac)
+    invD = 1.0 / D
+
+    def prec(r):
+        return r * invD + P @ (Ainv @ (P.T @ r))
+
+    bs = b @ b
+    atol2 = max(tol * tol * bs, atol * atol)
+    x = x0.copy()
+    r = b - A @ x
+    z = prec(r)
+    p = z.copy()
+    gamma = r @ z
+    k = 0
+    while (r @ r) > atol2 and k < maxiter:
+        Ap = A @ p
+        alpha = gamma / (p @ Ap)
+        x = x + alpha * p
+        r = r - alpha * Ap
+        z = prec(r)
+        gamma_ = r @ z
+        p = z + (gamma_ / gamma) * p
         gamma = gamma_
         k += 1
     return x, k

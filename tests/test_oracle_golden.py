@@ -1,9 +1,13 @@
 """Pin the CPU oracle against the reference's own recorded outputs (tests/golden)."""
 
+import pathlib
+
 import numpy as np
 import pytest
 
 import oracle as O
+
+ROOT = pathlib.Path(__file__).resolve().parent.parent
 
 
 @pytest.fixture(scope="module")
@@ -104,3 +108,28 @@ def test_pcg_matches_dense_solve():
     x, k = O.pcg(A, np.diag(A).copy(), b, np.zeros(40), 1e-12)
     np.testing.assert_allclose(x, np.linalg.solve(A, b), rtol=1e-9)
     assert 0 < k < 40
+
+
+def test_single_grain_sweep_fixture_is_the_oracles():
+    """tests/golden/sweep_single.npz (the single-grain sweep through switching that the GPU
+    sweeps are compared with) is what the oracle computes: regenerated here (a few seconds)."""
+    import json
+    import sys
+
+    sys.path.insert(0, str(ROOT / "tests" / "golden"))
+    import make_sweeps
+    from mammos_mumag.hysteresis import coercivity_remanence
+
+    f = np.load(ROOT / "tests" / "golden" / "sweep_single.npz")
+    assert json.loads(str(f["params"])) == make_sweeps.CASES["single"]
+    X, T, tag, krn, m0, par = make_sweeps.build_case("single")
+    rows, stats = O.run_loop(O.Problem(X, T, tag, krn), par, m0=m0)
+    # the BLAS thread count changes the summation order of the dense dot products: rows
+    # agree to a few 1e-10, far inside the loop tolerance
+    np.testing.assert_array_equal(rows[:, :2], f["rows"][:, :2])
+    np.testing.assert_allclose(rows[:, 2:], f["rows"][:, 2:], rtol=1e-8, atol=1e-10)
+    hc, mr = coercivity_remanence(rows)
+    assert hc == pytest.approx(float(f["hc"]), rel=1e-8)
+    assert mr == pytest.approx(float(f["mr"]), rel=1e-8)
+    # the sweep crosses the coercive field: a switched, saturated end state
+    assert rows[0, 2] > 1.5 and rows[-1, 2] < -1.5
