@@ -270,9 +270,12 @@ mm_status mm_batch_timer_start(mm_batch* batch);
 mm_status mm_batch_timer_stop(mm_batch* batch, double* elapsed_ms);
 
 /* Diagnostic per-CTA phase timers, collected only when the environment variable
- * MUMAG_PROFILE is set at mm_mesh_create: out [nctas][4] ns accumulated since the last read
+ * MUMAG_PROFILE is set at mm_mesh_create: out [nctas][12] ns accumulated since the last read
  * (Poisson-PCG row phases, reduction before the grid barrier, barrier wait, partial read
- * after the barrier); the counters are reset.  *nctas = 0 when profiling is off. */
+ * after the barrier, whole Poisson solves, M_inv applications, energy evaluations with their
+ * solves, whole launches, and the two-level preconditioner's box-sum publish, box-sum
+ * gather and own-box coarse solve); the counters are reset.  *nctas = 0 when profiling is
+ * off. */
 mm_status mm_profile_read(mm_mesh* mesh, long long* out, int32_t* nctas);
 mm_status mm_timer_stop(mm_mesh* mesh, double* elapsed_ms);
 

@@ -427,8 +427,8 @@ mm_status mm_mesh_create(const double* X, int64_t N, const int32_t* T, const int
     dalloc(m.resd, 2);
     dalloc(m.resi, 8);
     if (std::getenv("MUMAG_PROFILE")) {  // diagnostic per-CTA phase timers
-      dalloc(m.prof, 4 * (size_t)m.grid);
-      MM_CK(cudaMemsetAsync(m.prof, 0, sizeof(long long) * 4 * m.grid, m.stream));
+      dalloc(m.prof, (size_t)kProfCols * kMaxGrid);  // any grid the autotuner may choose
+      MM_CK(cudaMemsetAsync(m.prof, 0, sizeof(long long) * kProfCols * kMaxGrid, m.stream));
     }
     MM_CK(cudaHostAlloc(reinterpret_cast<void**>(&m.h_resd), 2 * sizeof(double), cudaHostAllocDefault));
     MM_CK(cudaHostAlloc(reinterpret_cast<void**>(&m.h_resi), 8 * sizeof(long long), cudaHostAllocDefault));
@@ -719,8 +719,8 @@ mm_status mm_profile_read(mm_mesh* mesh, long long* out, int32_t* nctas) {
   *nctas = m.prof ? m.grid : 0;
   if (!m.prof || !out) return MM_OK;
   MM_CK(cudaSetDevice(m.device));
-  MM_CK(cudaMemcpy(out, m.prof, sizeof(long long) * 4 * m.grid, cudaMemcpyDeviceToHost));
-  MM_CK(cudaMemset(m.prof, 0, sizeof(long long) * 4 * m.grid));
+  MM_CK(cudaMemcpy(out, m.prof, sizeof(long long) * kProfCols * m.grid, cudaMemcpyDeviceToHost));
+  MM_CK(cudaMemset(m.prof, 0, sizeof(long long) * kProfCols * kMaxGrid));
   return MM_OK;
   API_END
 }

@@ -48,6 +48,7 @@ struct __align__(16) PcgRec32 {
   float r, w, s, invd;
 };
 
+constexpr int kProfCols = 12;  // per-CTA timers of SolveArgs::prof
 constexpr int kNumPlanes32 = kNumPlanes;  // FP32 copies of every plane (mixed precision)
 
 // Arguments of the persistent solver kernel (passed by value, __grid_constant__).
@@ -123,8 +124,10 @@ struct SolveArgs {
   double* sw_rec;       // [sw_nmax][4] counter, hext, mh, energy
   long long* sw_stat;   // [sw_nmax][8] ncg, evals, pcg, shrinks, minv, ns, sync ns, barriers
   int* sw_nrec;         // rows written
-  // optional per-CTA timing [gridDim.x][4] ns (null = off): PCG row phases, reduction
-  // before the barrier, barrier wait, partial read after the barrier
+  // optional per-CTA timing [gridDim.x][kProfCols] ns (null = off): PCG row phases, reduction
+  // before the barrier, barrier wait, partial read after the barrier, whole Poisson solves,
+  // M_inv applications, energy evaluations (solves included), the launch, and the
+  // two-level preconditioner's publish, gather and own-box solve steps
   long long* prof;
   // results
   double* resd;     // [0] energy, [1] mh

@@ -194,6 +194,8 @@ struct Ctx {
   int64_t cbase;
   long long evals = 0, pcg_iters = 0, minv_iters = 0, shrinks = 0;
   unsigned long long t_phase_start = 0, t_pcg_phase = 0;
+  unsigned long long t_pcg = 0, t_minv = 0, t_eval = 0;  // profiling (thread 0): whole solves, M_inv, evaluations
+  unsigned long long t_cpub = 0, t_cgat = 0, t_csol = 0;  // profiling: coarse publish, gather, own solve
   double h;  // applied field of the current field step (mu0 H, T)
   // the tensor-core network of the learned start (tcsm = its shared-memory region, null when
   // the network runs on mma.sync), its TMEM columns and mbarrier phase
@@ -205,7 +207,10 @@ struct Ctx {
   // by the same recurrences in the same order), xc = Ac^-1 Pr of the CTA's own boxes, and
   // per slice of the CTA the (at most two) boxes its rows belong to with their partial sums
   double *cPs = nullptr, *cPr = nullptr, *cxc = nullptr, *csv = nullptr;
+  double* cslv = nullptr;  // the box slots of the last exchange, staged
   int* csb = nullptr;
+  unsigned* cmk = nullptr;    // per slice, the lanes of its first and of its second box
+  const int* cbsl = nullptr;  // the slot range of every box (a copy of SolveArgs::bslot)
   int cb0 = 0, cnb = 0, cslot0 = 0;
   __device__ Ctx(const SolveArgs& args) : a(args), h(args.h) {}
 };
@@ -222,8 +227,10 @@ struct Ctx {
 #define END_ROWS }
 #define ENTRY(k) (off_ + 32 * (int64_t)(k))
 #define LENTRY(k) (loff_ + 32 * (int64_t)(k))
-#define CHECK(x) \
-  if (!(x)) return false
+#define CHECK(x)          \
+  do {                    \
+    if (!(x)) return false; \
+  } while (0)
 
 __device__ __forceinline__ const double* plane(const SolveArgs& a, int p) { return a.vals + (size_t)p * a.nent; }
 
@@ -977,43 +984,65 @@ __device__ __forceinline__ int warp_max_i(int v) {
 
 // Sums of v over the rows of slice t (CTA-local index) in each of the slice's boxes; called
 // by all 32 lanes of the warp (lane = row i of the slice).
+// The slice's lane masks (shared memory, made at launch start) say which rows belong to
+// which box, so the hot loops read no box ids from global memory.
 __device__ __forceinline__ void coarse_slice_sum(const Ctx& c, int t, int i, double v) {
-  const int lo = c.csb[2 * t], hi = c.csb[2 * t + 1];
-  const int rb = __ldg(c.a.rbox + i);
-  const double slo = warp_sum((lo >= 0 && rb == lo) ? v : 0.0);
-  const double shi = hi != lo ? warp_sum(rb == hi ? v : 0.0) : 0.0;
+  (void)i;
+  const unsigned bit = 1u << c.lane, ml = c.cmk[2 * t], mh = c.cmk[2 * t + 1];
+  const double slo = warp_sum((ml & bit) ? v : 0.0);
+  const double shi = mh ? warp_sum((mh & bit) ? v : 0.0) : 0.0;
   if (c.lane == 0) {
     c.csv[2 * t] = slo;
     c.csv[2 * t + 1] = shi;
   }
 }
 
-// The CTA's partial sum of each of its boxes, slices in order, into its slots.  Must come
-// before the grid reduction (or barrier) that publishes them.
-__device__ __forceinline__ void coarse_publish(const Ctx& c) {
+// The box of this lane's row in slice t, -1 for Dirichlet and padding rows.
+__device__ __forceinline__ int coarse_row_box(const Ctx& c, int t) {
+  const unsigned bit = 1u << c.lane;
+  return (c.cmk[2 * t] & bit) ? c.csb[2 * t] : ((c.cmk[2 * t + 1] & bit) ? c.csb[2 * t + 1] : -1);
+}
+
+// The CTA's partial sum of each of its boxes into its slots: a warp per box, lanes over
+// the CTA's slices, a fixed-order warp sum.  Must come before the grid reduction (or
+// barrier) that publishes them.
+__device__ __forceinline__ void coarse_publish(Ctx& c) {
+  const unsigned long long t0 = (c.sy.timing && threadIdx.x == 0) ? globaltimer() : 0ull;
   __syncthreads();
   const int ns = c.s1 - c.s0;
-  for (int q = threadIdx.x; q < c.cnb; q += blockDim.x) {
+  for (int q = c.warp; q < c.cnb; q += c.nwarps) {
     const int box = c.cb0 + q;
     double acc = 0.0;
-    for (int t = 0; t < ns; ++t) {
-      if (c.csb[2 * t] == box)
-        acc += c.csv[2 * t];
-      else if (c.csb[2 * t + 1] == box)
-        acc += c.csv[2 * t + 1];
-    }
-    c.a.bslots[c.cslot0 + q] = acc;
+    for (int t = c.lane; t < ns; t += 32)
+      acc += c.csb[2 * t] == box ? c.csv[2 * t] : (c.csb[2 * t + 1] == box ? c.csv[2 * t + 1] : 0.0);
+    acc = warp_sum(acc);
+    if (c.lane == 0) c.a.bslots[c.cslot0 + q] = acc;
   }
+  if (c.sy.timing && threadIdx.x == 0) c.t_cpub += globaltimer() - t0;
 }
 
 // After the barrier: every box's total (its slots in order) folded into the coarse vectors.
 // restart: Pr = total, Ps = 0 (a fresh residual); else Ps = total + beta Ps, Pr -= alpha Ps.
-__device__ __forceinline__ void coarse_gather(const Ctx& c, bool restart, double alpha, double beta) {
+// The slots are first copied to shared memory with four independent loads in flight per
+// thread, so the step costs about one L2 round trip.
+__device__ __forceinline__ void coarse_gather(Ctx& c, bool restart, double alpha, double beta) {
+  const unsigned long long tg0 = (c.sy.timing && threadIdx.x == 0) ? globaltimer() : 0ull;
   const SolveArgs& a = c.a;
-  for (int q = threadIdx.x; q < a.nc; q += blockDim.x) {
-    const int t0 = __ldg(a.bslot + q), t1 = __ldg(a.bslot + q + 1);
+  const int nsl = c.cbsl[a.nc];
+  const int bd = blockDim.x;
+  for (int t0 = threadIdx.x; t0 < nsl; t0 += 4 * bd) {
+    double v[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) v[u] = t0 + u * bd < nsl ? __ldcg(a.bslots + t0 + u * bd) : 0.0;
+#pragma unroll
+    for (int u = 0; u < 4; ++u)
+      if (t0 + u * bd < nsl) c.cslv[t0 + u * bd] = v[u];
+  }
+  __syncthreads();
+  for (int q = threadIdx.x; q < a.nc; q += bd) {
+    const int t1 = c.cbsl[q + 1];
     double w = 0.0;
-    for (int t = t0; t < t1; ++t) w += __ldcg(a.bslots + t);
+    for (int t = c.cbsl[q]; t < t1; ++t) w += c.cslv[t];
     if (restart) {
       c.cPr[q] = w;
       c.cPs[q] = 0.0;
@@ -1024,21 +1053,55 @@ __device__ __forceinline__ void coarse_gather(const Ctx& c, bool restart, double
     }
   }
   __syncthreads();
+  if (c.sy.timing && threadIdx.x == 0) c.t_cgat += globaltimer() - tg0;
 }
 
-// xc = Ac^-1 Pr for the CTA's own boxes: a warp per box, lanes along the row.
+// xc = Ac^-1 Pr for the CTA's own boxes.  Up to kOwnBoxes boxes: every thread takes columns
+// j = tid, tid + blockDim, ... of all the boxes' rows at once (independent L2 loads in
+// flight), then a fixed-order block sum per box.  More boxes (small grids): a warp per box.
+constexpr int kOwnBoxes = 8;
 template <class AT>
-__device__ __forceinline__ void coarse_solve_own(const Ctx& c, const AT* Ainv) {
-  const int nc = c.a.nc;
-  for (int q = c.warp; q < c.cnb; q += c.nwarps) {
-    const int box = c.cb0 + q;
-    const AT* row = Ainv + (size_t)box * nc;
-    double acc = 0.0;
-    for (int j = c.lane; j < nc; j += 32) acc += (double)__ldg(row + j) * c.cPr[j];
-    acc = warp_sum(acc);
-    if (c.lane == 0) c.cxc[box] = acc;
+__device__ __forceinline__ void coarse_solve_own(Ctx& c, const AT* Ainv) {
+  __shared__ double red[32][kOwnBoxes];
+  const unsigned long long ts0 = (c.sy.timing && threadIdx.x == 0) ? globaltimer() : 0ull;
+  const int nc = c.a.nc, nb = c.cnb;
+  if (nb <= kOwnBoxes) {
+    double acc[kOwnBoxes];
+#pragma unroll
+    for (int b = 0; b < kOwnBoxes; ++b) acc[b] = 0.0;
+    const AT* rows = Ainv + (size_t)c.cb0 * nc;
+    for (int j = threadIdx.x; j < nc; j += blockDim.x) {
+      const double pr = c.cPr[j];
+      AT v[kOwnBoxes];
+#pragma unroll
+      for (int b = 0; b < kOwnBoxes; ++b) v[b] = b < nb ? __ldg(rows + (size_t)b * nc + j) : AT(0);
+#pragma unroll
+      for (int b = 0; b < kOwnBoxes; ++b) acc[b] += (double)v[b] * pr;
+    }
+#pragma unroll
+    for (int b = 0; b < kOwnBoxes; ++b) {
+      if (b >= nb) break;
+      const double w = warp_sum(acc[b]);
+      if (c.lane == 0) red[c.warp][b] = w;
+    }
+    __syncthreads();
+    if (threadIdx.x < nb) {
+      double t = 0.0;
+      for (int w = 0; w < c.nwarps; ++w) t += red[w][threadIdx.x];
+      c.cxc[c.cb0 + threadIdx.x] = t;
+    }
+  } else {
+    for (int q = c.warp; q < nb; q += c.nwarps) {
+      const int box = c.cb0 + q;
+      const AT* row = Ainv + (size_t)box * nc;
+      double acc = 0.0;
+      for (int j = c.lane; j < nc; j += 32) acc += (double)__ldg(row + j) * c.cPr[j];
+      acc = warp_sum(acc);
+      if (c.lane == 0) c.cxc[box] = acc;
+    }
   }
   __syncthreads();
+  if (c.sy.timing && threadIdx.x == 0) c.t_csol += globaltimer() - ts0;
 }
 
 // Pr = P^T v for a residual v given per row by val(i) (after a warm start changed it).
@@ -1118,7 +1181,7 @@ __device__ __noinline__ bool pcg_solve_coarse(Ctx& c, const double* x) {
     FOR_ROWS(c)
     (void)w_;
     const double r = pl[i], invd = pl[3 * n + i];
-    const int rb = __ldg(a.rbox + i);
+    const int rb = coarse_row_box(c, s_ - c.s0);
     const double z0 = r * invd + (rb >= 0 ? c.cxc[rb] : 0.0);
     z[i] = z0;
     a.pp[i] = 0.0;
@@ -1152,7 +1215,7 @@ __device__ __noinline__ bool pcg_solve_coarse(Ctx& c, const double* x) {
     const PcgRec q = rec_load(a.rec[0], i, n);
     const double sn = q.w + beta * q.s;
     const double r = q.r - alpha * sn;
-    const int rb = __ldg(a.rbox + i);
+    const int rb = coarse_row_box(c, s_ - c.s0);
     const double zn = r * q.invd + (rb >= 0 ? c.cxc[rb] : 0.0);
     const double p = z[i] + beta * a.pp[i];
     a.pp[i] = p;
@@ -1251,7 +1314,7 @@ __device__ __noinline__ bool pcg_solve_mixed_coarse(Ctx& c, const double* x) {
       FOR_ROWS(c)
       (void)w_;
       const PcgRec32 q = rc[i];
-      const int rb = __ldg(a.rbox + i);
+      const int rb = coarse_row_box(c, s_ - c.s0);
       const float z0 = q.r * q.invd + (rb >= 0 ? (float)c.cxc[rb] : 0.f);
       z[i] = z0;
       a.pp32[i] = 0.f;
@@ -1289,7 +1352,7 @@ __device__ __noinline__ bool pcg_solve_mixed_coarse(Ctx& c, const double* x) {
       const PcgRec32 q = rc[i];
       const float sn = q.w + bf * q.s;
       const float r = q.r - af * sn;
-      const int rb = __ldg(a.rbox + i);
+      const int rb = coarse_row_box(c, s_ - c.s0);
       const float zn = r * q.invd + (rb >= 0 ? (float)c.cxc[rb] : 0.f);
       const float p = z[i] + bf * a.pp32[i];
       a.pp32[i] = p;
@@ -1356,12 +1419,16 @@ struct EvalOut {
 template <bool TC>
 __device__ bool eval(Ctx& c, const double* x, const double* xref, const double* d, double* gout, EvalOut& o) {
   const SolveArgs& a = c.a;
+  const bool tm = c.sy.timing && threadIdx.x == 0;
+  const unsigned long long te0 = tm ? globaltimer() : 0ull;
   if (a.hmag_on > 0) {
-    if (a.nc > 0)
+    if (a.nc > 0) {
       CHECK(a.mixed ? pcg_solve_mixed_coarse<TC>(c, x) : pcg_solve_coarse<TC>(c, x));
-    else
+    } else {
       CHECK(a.mixed ? pcg_solve_mixed<TC>(c, x) : pcg_solve<TC>(c, x));
+    }
   }
+  if (tm) c.t_pcg += globaltimer() - te0;
   const int n = a.Npad;
   const double* G = plane(a, P_G);
   const int64_t ps = a.nent;
@@ -1426,6 +1493,7 @@ __device__ bool eval(Ctx& c, const double* x, const double* xref, const double* 
   o.xinf = v[3];
   o.ginf = v[4];
   c.evals += 1;
+  if (tm) c.t_eval += globaltimer() - te0;
   return true;
 }
 
@@ -1470,8 +1538,18 @@ __device__ __forceinline__ void apply_A_row(const Ctx& c, const double* mb, cons
   o[2] = pr[2] - md * v[2 * n + i];
 }
 
+__device__ bool minv_body(Ctx& c, const double* g, const double* mb, double* zout);
+
 // zout = M_inv(g): p with A p ~ g, or g itself when p stays zero.
 __device__ bool minv(Ctx& c, const double* g, const double* mb, double* zout) {
+  const bool tm = c.sy.timing && threadIdx.x == 0;
+  const unsigned long long t0 = tm ? globaltimer() : 0ull;
+  const bool ok = minv_body(c, g, mb, zout);
+  if (tm) c.t_minv += globaltimer() - t0;
+  return ok;
+}
+
+__device__ bool minv_body(Ctx& c, const double* g, const double* mb, double* zout) {
   const SolveArgs& a = c.a;
   const int n = a.Npad;
   if (a.precond_iter <= 0) {
@@ -1872,17 +1950,26 @@ __device__ __forceinline__ void solve_body(const SolveArgs& args, int nblk, int 
     c.cPs = base;
     c.cPr = base + args.nc;
     c.cxc = base + 2 * args.nc;
-    c.csv = base + 3 * args.nc;
+    c.cslv = base + 3 * args.nc;
+    c.csv = c.cslv + args.nc + kMaxGrid;
     c.csb = reinterpret_cast<int*>(c.csv + 2 * args.meta_max);
+    c.cmk = reinterpret_cast<unsigned*>(c.csb + 2 * args.meta_max);
+    int* bsl = reinterpret_cast<int*>(c.cmk + 2 * args.meta_max);
+    for (int q = threadIdx.x; q <= args.nc; q += blockDim.x) bsl[q] = __ldg(args.bslot + q);
+    c.cbsl = bsl;
     c.cb0 = __ldg(args.ctabox + 3 * blk);
     c.cnb = __ldg(args.ctabox + 3 * blk + 1);
     c.cslot0 = __ldg(args.ctabox + 3 * blk + 2);
     for (int t = c.warp; t < c.s1 - c.s0; t += c.nwarps) {
       const int rb = __ldg(args.rbox + (size_t)(c.s0 + t) * 32 + c.lane);
       const int lo = warp_min_i(rb >= 0 ? rb : INT_MAX), hi = warp_max_i(rb);
+      const unsigned ml = __ballot_sync(0xffffffffu, rb >= 0 && rb == lo);
+      const unsigned mh = __ballot_sync(0xffffffffu, rb >= 0 && rb == hi && hi != lo);
       if (c.lane == 0) {
         c.csb[2 * t] = lo == INT_MAX ? -1 : lo;
         c.csb[2 * t + 1] = hi;
+        c.cmk[2 * t] = ml;
+        c.cmk[2 * t + 1] = mh;
       }
     }
     __syncthreads();
@@ -1924,11 +2011,18 @@ __device__ __forceinline__ void solve_body(const SolveArgs& args, int nblk, int 
     if (c.tcsm) tc_net_teardown(c.tcsm, c.tctm, c.tcbad, c.tcph);
   }
   if (args.prof && threadIdx.x == 0) {
-    long long* p = args.prof + 4 * blk;
+    long long* p = args.prof + kProfCols * blk;
     p[0] += (long long)c.t_pcg_phase;
     p[1] += (long long)c.sy.t_pre;
     p[2] += (long long)c.sy.t_bar;
     p[3] += (long long)c.sy.t_post;
+    p[4] += (long long)c.t_pcg;
+    p[5] += (long long)c.t_minv;
+    p[6] += (long long)c.t_eval;
+    p[7] += (long long)(globaltimer() - t_start);
+    p[8] += (long long)c.t_cpub;
+    p[9] += (long long)c.t_cgat;
+    p[10] += (long long)c.t_csol;
   }
 }
 
@@ -1968,7 +2062,8 @@ struct StagePlan {
   int co_off;     // offset of the coarse region, -1 = none
 };
 // Regions: [staged entries][slice metadata][coarse vectors: Ps, Pr, xc (nc doubles each),
-// per slice two partial sums and two box ids][tensor-core network]
+// the staged box slots (nc + kMaxGrid doubles), per slice two partial sums, two box ids and
+// two lane masks, every box's first slot (nc + 1 ints)][tensor-core network]
 StagePlan stage_plan(const DevMesh& m, int grid, size_t limit, size_t extra = 0, bool allow_stage = true,
                      int nc = 0) {
   int64_t emax = 0, smax = 0;
@@ -1978,8 +2073,9 @@ StagePlan stage_plan(const DevMesh& m, int grid, size_t limit, size_t extra = 0,
     smax = std::max(smax, s1 - s0);
   }
   const size_t meta = (size_t)smax * (sizeof(int64_t) + sizeof(int32_t));
-  const size_t coarse =
-      nc > 0 ? (size_t)(3 * nc + 2 * smax) * sizeof(double) + (size_t)2 * smax * sizeof(int) + 16 : 0;
+  const size_t coarse = nc > 0 ? (size_t)(4 * nc + kMaxGrid + 2 * smax) * sizeof(double) +
+                                     (size_t)(4 * smax + nc + 1) * sizeof(int) + 16
+                               : 0;
   const size_t need = (size_t)emax * (sizeof(double) + sizeof(int32_t) + (m.vals32 ? sizeof(float) : 0));
   StagePlan p;
   p.stage = (allow_stage && need + meta + 16 + coarse + (extra ? extra + 1024 : 0) <= limit) ? 1 : 0;

@@ -445,12 +445,15 @@ class Mesh:
         return ms.value
 
     def profile(self):
-        """Per-CTA phase timers [nctas, 4] ns (MUMAG_PROFILE set at creation), else None."""
+        """Per-CTA phase timers [nctas, 12] ns (MUMAG_PROFILE set at creation), else None:
+        PCG row phases, reduction before the barrier, barrier wait, partial read after it,
+        whole Poisson solves, M_inv, energy evaluations (solves included), whole launches,
+        the two-level preconditioner's publish, gather and own-box solve."""
         n = C.c_int32()
         check(load().mm_profile_read(self._h, None, C.byref(n)))
         if n.value == 0:
             return None
-        out = np.zeros((n.value, 4), np.int64)
+        out = np.zeros((n.value, 12), np.int64)
         check(load().mm_profile_read(self._h, out.ctypes.data_as(_I64), C.byref(n)))
         return out
 
