@@ -102,6 +102,7 @@ typedef struct {
   int64_t barriers;    /* grid barriers executed */
   double device_ms;    /* duration of the launch from CUDA events on the launching stream */
   int status;          /* MM_OK, MM_NONFINITE or MM_TIMEOUT */
+  int64_t learned_starts;  /* Poisson solves that took the learned warm start */
 } mm_step_result;
 
 typedef struct {
@@ -172,6 +173,11 @@ mm_status mm_color_elements(int64_t N, const int32_t* T, int64_t E, int32_t* col
  * (scripts/matrix.py:37-47, scripts/mapping.py:203-210), divergence dk and gradient gk
  * (scripts/matrix.py:9-35), and the Poisson matrix with its boundary treatment
  * (scripts/matrix.py:49-74, scripts/trafo.py:4-45). */
+/* The host preprocessing (node order, SELL pattern, element colouring, boundary branch,
+ * aggregate boxes) and the two-level preconditioner's coarse inverse are cached per process
+ * for the last four meshes, keyed by the exact X, T, tag and the reorder / coarse_box_nodes
+ * options (the counterpart of the reference's scripts/store.py pickles, scripts/store.py:8-23):
+ * creating the same mesh again repeats only the device assembly. */
 mm_status mm_mesh_create(const double* X, int64_t N, const int32_t* T, const int32_t* tag,
                          int64_t E, const mm_material* mats, int32_t nmats,
                          const mm_options* opt, mm_mesh** out);
@@ -328,6 +334,13 @@ mm_status mm_model_predict(mm_model* model, const float* feats, int64_t n, float
  * mm_autotune after this call to tune for it); larger launches run it on mma.sync. */
 typedef enum { MM_WARM_PREVIOUS = 0, MM_WARM_ZERO = 1, MM_WARM_LEARNED = 2 } mm_warm_mode;
 mm_status mm_mesh_set_warm_start(mm_mesh* mesh, int32_t mode, const mm_model* model);
+
+/* Gate of the learned start: it runs only on Poisson solves whose initial residual exceeds
+ * `ratio` times the stop tolerance (r.r > ratio^2 tol_u^2 b.b), i.e. solves with at least
+ * log10(ratio) decades to go, where a better start can save more iterations than the
+ * network costs; other solves start from the previous u.  ratio <= 1 (the default 0): every
+ * solve.  No counterpart in the reference. */
+mm_status mm_mesh_set_learned_gate(mm_mesh* mesh, double ratio);
 
 /* Training-sample recording: from now on, in every Poisson solve of the mesh (of any entry
  * point), a hash-selected 1/stride of the nodes record their features

@@ -8,6 +8,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <algorithm>
+#include <list>
 #include <map>
 #include <memory>
 #include <mutex>
@@ -132,32 +133,98 @@ void release(DevMesh& m) {
   m.stream = nullptr;
 }
 
+// Process-wide cache of the host preprocessing (node order, SELL pattern, element colouring,
+// boundary branch, aggregate boxes) and of the coarse inverse, keyed by the exact mesh input
+// and the options that shape it -- the counterpart of the reference's scripts/store.py,
+// which pickles escript's assembled arrays so a rerun skips the set-up.  Entries compare the
+// full input (a 64-bit hash first), so a hit is exact; the last kPrepCache meshes are kept.
+constexpr size_t kPrepCache = 4;
+struct PrepEntry {
+  uint64_t hash = 0;
+  int reorder = 0, coarse = 0;
+  std::vector<double> X;
+  std::vector<int32_t> T, tag;
+  HostMesh h;
+  std::vector<double> Ainv;  // filled by the first build_coarse of this mesh
+};
+std::mutex g_prep_mu;
+std::list<std::shared_ptr<PrepEntry>> g_prep;  // most recent first
+
+uint64_t hash_bytes(uint64_t h, const void* p, size_t n) {
+  const unsigned char* b = static_cast<const unsigned char*>(p);
+  size_t k = 0;
+  for (; k + 8 <= n; k += 8) {
+    uint64_t w;
+    std::memcpy(&w, b + k, 8);
+    h = (h ^ w) * 0x9E3779B97F4A7C15ull;
+    h ^= h >> 29;
+  }
+  for (; k < n; ++k) h = (h ^ b[k]) * 0x100000001B3ull;
+  return h;
+}
+
+std::shared_ptr<PrepEntry> prep_find(uint64_t hash, const double* X, int64_t N, const int32_t* T, const int32_t* tag,
+                                     int64_t E, int reorder, int coarse) {
+  std::lock_guard<std::mutex> lk(g_prep_mu);
+  for (auto it = g_prep.begin(); it != g_prep.end(); ++it) {
+    const PrepEntry& e = **it;
+    if (e.hash != hash || e.reorder != reorder || e.coarse != coarse || (int64_t)e.X.size() != 3 * N ||
+        (int64_t)e.tag.size() != E)
+      continue;
+    if (std::memcmp(e.X.data(), X, sizeof(double) * 3 * N) || std::memcmp(e.T.data(), T, sizeof(int32_t) * 4 * E) ||
+        std::memcmp(e.tag.data(), tag, sizeof(int32_t) * E))
+      continue;
+    auto hit = *it;
+    g_prep.erase(it);
+    g_prep.push_front(hit);
+    return hit;
+  }
+  return nullptr;
+}
+
+void prep_store(std::shared_ptr<PrepEntry> e) {
+  std::lock_guard<std::mutex> lk(g_prep_mu);
+  g_prep.push_front(std::move(e));
+  while (g_prep.size() > kPrepCache) g_prep.pop_back();
+}
+
 // The two-level preconditioner's coarse operator: Ac = P^T S P summed on the host from the
 // assembled Poisson plane (rows in device order, so the sums are deterministic), inverted
 // densely (banded Cholesky; Ac couples only neighbouring boxes), uploaded in FP64 and FP32.
-void build_coarse(DevMesh& m) {
+void build_coarse(DevMesh& m, std::vector<double>* cached) {
   const HostMesh& h = m.h;
   const int nc = h.nc;
   m.nc = nc;
   if (nc <= 0) return;
-  std::vector<double> S;
-  d2h(S, m.vals + (size_t)P_S * h.nent, h.nent, m.stream);
-  std::vector<double> A((size_t)nc * nc, 0.0);
-  int32_t bw = 0;
-  for (int64_t s = 0; s < h.nslices; ++s)
-    for (int l = 0; l < kSlice; ++l) {
-      const int64_t i = s * kSlice + l;
-      if (i >= h.N || h.rbox[i] < 0) continue;
-      const int32_t ci = h.rbox[i];
-      for (int32_t k = 0; k < h.rowlen[i]; ++k) {
-        const int64_t e = h.sl_off[s] + (int64_t)k * kSlice + l;
-        const int32_t cj = h.rbox[h.col[e]];
-        if (cj < 0) continue;
-        A[(size_t)ci * nc + cj] += S[e];
-        bw = std::max(bw, std::abs(ci - cj));
+  std::vector<double> A;
+  {
+    std::lock_guard<std::mutex> lk(g_prep_mu);
+    if (cached && cached->size() == (size_t)nc * nc) A = *cached;
+  }
+  if (A.empty()) {
+    std::vector<double> S;
+    d2h(S, m.vals + (size_t)P_S * h.nent, h.nent, m.stream);
+    A.assign((size_t)nc * nc, 0.0);
+    int32_t bw = 0;
+    for (int64_t s = 0; s < h.nslices; ++s)
+      for (int l = 0; l < kSlice; ++l) {
+        const int64_t i = s * kSlice + l;
+        if (i >= h.N || h.rbox[i] < 0) continue;
+        const int32_t ci = h.rbox[i];
+        for (int32_t k = 0; k < h.rowlen[i]; ++k) {
+          const int64_t e = h.sl_off[s] + (int64_t)k * kSlice + l;
+          const int32_t cj = h.rbox[h.col[e]];
+          if (cj < 0) continue;
+          A[(size_t)ci * nc + cj] += S[e];
+          bw = std::max(bw, std::abs(ci - cj));
+        }
       }
+    spd_inverse(nc, bw, A);
+    if (cached) {
+      std::lock_guard<std::mutex> lk(g_prep_mu);
+      *cached = A;
     }
-  spd_inverse(nc, bw, A);
+  }
   std::vector<float> A32(A.size());
   for (size_t q = 0; q < A.size(); ++q) A32[q] = (float)A[q];
   dalloc(m.rbox, h.Npad);
@@ -210,7 +277,7 @@ mm_status run(DevMesh& m, const SolveArgs& a) {
   if (!m.evk1) MM_CK(cudaEventCreate(&m.evk1));
   MM_CK(solver_launch(m, a));
   MM_CK(cudaMemcpyAsync(m.h_resd, m.resd, 2 * sizeof(double), cudaMemcpyDeviceToHost, m.stream));
-  MM_CK(cudaMemcpyAsync(m.h_resi, m.resi, 8 * sizeof(long long), cudaMemcpyDeviceToHost, m.stream));
+  MM_CK(cudaMemcpyAsync(m.h_resi, m.resi, kResI * sizeof(long long), cudaMemcpyDeviceToHost, m.stream));
   MM_CK(cudaMemcpyAsync(m.h_flags, m.flags, 2 * sizeof(int), cudaMemcpyDeviceToHost, m.stream));
   MM_CK(cudaStreamSynchronize(m.stream));
   MM_CK(cudaEventElapsedTime(&m.last_launch_ms, m.evk0, m.evk1));
@@ -330,7 +397,29 @@ mm_status mm_mesh_create(const double* X, int64_t N, const int32_t* T, const int
   DevMesh& m = mesh->dm;
   m.device = o.device;
   m.opt = o;
-  preprocess(X, N, T, tag, E, nmats, o.reorder != 0, o.coarse_box_nodes, m.h);
+  // host preprocessing, from the cache when this exact mesh was prepared before
+  uint64_t key = hash_bytes(0x6D756D6167ull, X, sizeof(double) * 3 * (size_t)std::max<int64_t>(N, 0));
+  key = hash_bytes(key, T, sizeof(int32_t) * 4 * (size_t)std::max<int64_t>(E, 0));
+  key = hash_bytes(key, tag, sizeof(int32_t) * (size_t)std::max<int64_t>(E, 0));
+  std::shared_ptr<PrepEntry> prep =
+      N > 0 && E > 0 ? prep_find(key, X, N, T, tag, E, o.reorder != 0, o.coarse_box_nodes) : nullptr;
+  if (prep) {
+    m.h = prep->h;
+    if ((int32_t)m.h.tags.size() > nmats)
+      throw std::runtime_error("materials file has " + std::to_string(nmats) + " rows for " +
+                               std::to_string(m.h.tags.size()) + " element tags");
+  } else {
+    preprocess(X, N, T, tag, E, nmats, o.reorder != 0, o.coarse_box_nodes, m.h);
+    prep = std::make_shared<PrepEntry>();
+    prep->hash = key;
+    prep->reorder = o.reorder != 0;
+    prep->coarse = o.coarse_box_nodes;
+    prep->X.assign(X, X + 3 * N);
+    prep->T.assign(T, T + 4 * E);
+    prep->tag.assign(tag, tag + E);
+    prep->h = m.h;
+    prep_store(prep);
+  }
   // PCG arrangement: fixed by the caller, else by size until mm_autotune times both; the
   // two-level preconditioner runs in the two-sync arrangement only
   m.pcg2 = o.pcg_variant == 2 ? 1 : o.pcg_variant == 1 ? 0 : (m.h.N >= kPcg2Nodes ? 1 : 0);
@@ -386,7 +475,7 @@ mm_status mm_mesh_create(const double* X, int64_t N, const int32_t* T, const int
     upload(m.etag, h.etag, m.stream);
     upload(m.dmats, m.mats, m.stream);
     assemble_operators(m);
-    build_coarse(m);
+    build_coarse(m, &prep->Ainv);
     // solver state: 12 three-vectors, 2 node vectors, 2 x Npad PCG records (4 doubles each);
     // the total is computed from the same list that carves the buffer
     const size_t np = h.Npad;
@@ -425,13 +514,13 @@ mm_status mm_mesh_create(const double* X, int64_t N, const int32_t* T, const int
     dalloc(m.red, (size_t)2 * kMaxRed * kMaxGrid);  // any grid the autotuner may choose
     dalloc(m.flags, 2);
     dalloc(m.resd, 2);
-    dalloc(m.resi, 8);
+    dalloc(m.resi, kResI);
     if (std::getenv("MUMAG_PROFILE")) {  // diagnostic per-CTA phase timers
       dalloc(m.prof, (size_t)kProfCols * kMaxGrid);  // any grid the autotuner may choose
       MM_CK(cudaMemsetAsync(m.prof, 0, sizeof(long long) * kProfCols * kMaxGrid, m.stream));
     }
     MM_CK(cudaHostAlloc(reinterpret_cast<void**>(&m.h_resd), 2 * sizeof(double), cudaHostAllocDefault));
-    MM_CK(cudaHostAlloc(reinterpret_cast<void**>(&m.h_resi), 8 * sizeof(long long), cudaHostAllocDefault));
+    MM_CK(cudaHostAlloc(reinterpret_cast<void**>(&m.h_resi), kResI * sizeof(long long), cudaHostAllocDefault));
     MM_CK(cudaHostAlloc(reinterpret_cast<void**>(&m.h_flags), 2 * sizeof(int), cudaHostAllocDefault));
     MM_CK(cudaStreamSynchronize(m.stream));
   } catch (...) {
@@ -640,6 +729,7 @@ mm_status mm_minimize(mm_mesh* mesh, double h, const mm_solver_params* sp, mm_st
     res->kernel_ns = m.h_resi[5];
     res->sync_ns = m.h_resi[6];
     res->barriers = m.h_resi[7];
+    res->learned_starts = m.h_resi[8];
     res->device_ms = m.last_launch_ms;
     res->status = st;
   }
@@ -678,6 +768,7 @@ mm_status mm_loop(mm_mesh* mesh, const mm_loop_params* lp, const mm_solver_param
     r.kernel_ns = m.h_resi[5];
     r.sync_ns = m.h_resi[6];
     r.barriers = m.h_resi[7];
+    r.learned_starts = m.h_resi[8];
     r.device_ms = m.last_launch_ms;
     r.status = st;
     if (st != MM_OK) {
@@ -784,7 +875,7 @@ mm_status batch_run(mm_batch* b, const double* h, const mm_solver_params* sp, co
   for (int q = 0; q < count; ++q) {
     DevMesh& m = b->meshes[q]->dm;
     MM_CK(cudaMemcpyAsync(m.h_resd, m.resd, 2 * sizeof(double), cudaMemcpyDeviceToHost, b->stream));
-    MM_CK(cudaMemcpyAsync(m.h_resi, m.resi, 8 * sizeof(long long), cudaMemcpyDeviceToHost, b->stream));
+    MM_CK(cudaMemcpyAsync(m.h_resi, m.resi, kResI * sizeof(long long), cudaMemcpyDeviceToHost, b->stream));
     MM_CK(cudaMemcpyAsync(m.h_flags, m.flags, 2 * sizeof(int), cudaMemcpyDeviceToHost, b->stream));
   }
   MM_CK(cudaStreamSynchronize(b->stream));
@@ -811,6 +902,7 @@ void fill_result(const DevMesh& m, mm_status st, mm_step_result& r) {
   r.kernel_ns = m.h_resi[5];
   r.sync_ns = m.h_resi[6];
   r.barriers = m.h_resi[7];
+  r.learned_starts = m.h_resi[8];
   r.device_ms = 0.0;
   r.status = st;
 }
@@ -1141,6 +1233,15 @@ mm_status mm_mesh_set_warm_start(mm_mesh* mesh, int32_t mode, const mm_model* mo
   }
   m.warm = mode;
   solver_configure(m);  // the learned start's network region changes the shared-memory plan
+  return MM_OK;
+  API_END
+}
+
+mm_status mm_mesh_set_learned_gate(mm_mesh* mesh, double ratio) {
+  API_BEGIN
+  check_mesh(mesh);
+  if (!(ratio >= 0.0) || !std::isfinite(ratio)) throw std::runtime_error("the gate ratio must be finite and >= 0");
+  mesh->dm.warm_gate = ratio;
   return MM_OK;
   API_END
 }

@@ -48,6 +48,7 @@ struct __align__(16) PcgRec32 {
   float r, w, s, invd;
 };
 
+constexpr int kResI = 9;       // integer results of a launch (SolveArgs::resi)
 constexpr int kProfCols = 12;  // per-CTA timers of SolveArgs::prof
 constexpr int kNumPlanes32 = kNumPlanes;  // FP32 copies of every plane (mixed precision)
 
@@ -78,6 +79,7 @@ struct SolveArgs {
   int pcg2;             // 1: two-sync PCG iteration (z gathered alone), 0: one-sync
   // Poisson warm start (MM_WARM_*): previous u, zero, or previous u + the learned correction
   int warm;
+  double warm_gate2;    // the learned start runs only when r.r > warm_gate2 * tol_u^2 b.b
   int32_t nreal;        // real (non-padding) rows
   MlpDev mlp;           // learned warm start: the model
   float* feat;          // [Npad][kMlpIn] node features of the learned start
@@ -94,6 +96,7 @@ struct SolveArgs {
   const int32_t* bslot; // [nc+1] box c's partial sums are slots [bslot[c], bslot[c+1])
   const int32_t* ctabox;  // [grid][3] first box, number of boxes and first slot of each CTA
   int co_off;           // dynamic shared-memory offset of the coarse vectors
+  int co_rows;          // > 0: each CTA keeps its rows of Ainv32 in shared memory (capacity)
   // training-sample recording (rec_cap > 0): at a hash-selected 1/rec_stride of the
   // (node, solve) pairs, the node's features at the warm start and, after the solve,
   // the target (u - u0) / sigma
@@ -131,7 +134,8 @@ struct SolveArgs {
   long long* prof;
   // results
   double* resd;     // [0] energy, [1] mh
-  long long* resi;  // [0] ncg iters, [1] evals, [2] pcg iters, [3] ls shrinks, [4] minv iters
+  long long* resi;  // [kResI]: ncg iters, evals, pcg iters, ls shrinks, minv iters, kernel ns,
+                    // sync ns, barriers, learned starts applied
 };
 
 enum { WARM_PREV = 0, WARM_ZERO = 1, WARM_LEARNED = 2 };
@@ -170,6 +174,7 @@ struct DevMesh {
   int bar_stall = 0;  // test hook (SolveArgs::bar_stall)
   // warm start and sample recording (SolveArgs)
   int warm = 0;
+  double warm_gate = 0.0;  // mm_mesh_set_learned_gate
   MlpDev mlp{};
   float *feat = nullptr, *du = nullptr;
   float *rs_feat = nullptr, *rs_tgt = nullptr;
@@ -208,6 +213,7 @@ struct DevMesh {
   int32_t* bslot = nullptr;
   int32_t* ctabox = nullptr;
   int co_off = -1;
+  int co_rows = 0;
 };
 
 // A batched persistent launch over several meshes: mesh q runs on CTAs

@@ -192,10 +192,10 @@ struct Ctx {
   const int64_t* soff;  // SELL offsets and widths of the CTA's slices (shared memory)
   const int32_t* sw;
   int64_t cbase;
-  long long evals = 0, pcg_iters = 0, minv_iters = 0, shrinks = 0;
+  long long evals = 0, pcg_iters = 0, minv_iters = 0, shrinks = 0, lstarts = 0;
   unsigned long long t_phase_start = 0, t_pcg_phase = 0;
   unsigned long long t_pcg = 0, t_minv = 0, t_eval = 0;  // profiling (thread 0): whole solves, M_inv, evaluations
-  unsigned long long t_cpub = 0, t_cgat = 0, t_csol = 0;  // profiling: coarse publish, gather, own solve
+  unsigned long long t_cpub = 0, t_cgat = 0, t_csol = 0;  // profiling: (unused), coarse update, (unused)
   double h;  // applied field of the current field step (mu0 H, T)
   // the tensor-core network of the learned start (tcsm = its shared-memory region, null when
   // the network runs on mma.sync), its TMEM columns and mbarrier phase
@@ -208,6 +208,7 @@ struct Ctx {
   // per slice of the CTA the (at most two) boxes its rows belong to with their partial sums
   double *cPs = nullptr, *cPr = nullptr, *cxc = nullptr, *csv = nullptr;
   double* cslv = nullptr;  // the box slots of the last exchange, staged
+  const float* crows = nullptr;  // the CTA's rows of Ac^-1 (FP32), staged; null: read from L2
   int* csb = nullptr;
   unsigned* cmk = nullptr;    // per slice, the lanes of its first and of its second box
   const int* cbsl = nullptr;  // the slot range of every box (a copy of SolveArgs::bslot)
@@ -694,7 +695,8 @@ __device__ __noinline__ bool pcg_solve(Ctx& c, const double* x) {
   const double sig = sqrt(zz / (double)a.nreal);
   const bool recording = a.rec_cap > 0 && sig > 0.0;
   if (recording) record_features(c, x, reinterpret_cast<const double*>(a.rec[0]), 1.0 / sig);
-  if (a.warm == WARM_LEARNED && sig > 0.0) {
+  if (a.warm == WARM_LEARNED && sig > 0.0 && rr > a.warm_gate2 * atol2) {
+    c.lstarts += 1;
     CHECK(learned_start<TC>(c, x, sig, gamma, rr));
     if (!(rr > atol2)) {
       if (recording) record_targets(c, sig);
@@ -869,8 +871,10 @@ __device__ __noinline__ bool pcg_solve_mixed(Ctx& c, const double* x) {
   const double sig = sqrt(zz / (double)a.nreal);
   const bool recording = rr > atol2 && a.max_pcg > 0 && a.rec_cap > 0 && sig > 0.0;
   if (recording) record_features(c, x, a.r64, 1.0 / sig);
-  if (rr > atol2 && a.max_pcg > 0 && a.warm == WARM_LEARNED && sig > 0.0)
+  if (rr > atol2 && a.max_pcg > 0 && a.warm == WARM_LEARNED && sig > 0.0 && rr > a.warm_gate2 * atol2) {
+    c.lstarts += 1;
     CHECK(learned_start_mixed<TC>(c, x, sig, rr, rin2, gin));
+  }
   for (int outer = 0; rr > atol2 && k < a.max_pcg && outer < 32; ++outer) {
     const double inner_tol2 = fmax(1e-10 * rin2, 0.25 * atol2);  // 1e-5 relative, or the outer target
     double gamma = gin, delta;
@@ -956,6 +960,68 @@ __device__ __noinline__ bool pcg_solve_mixed(Ctx& c, const double* x) {
   return true;
 }
 
+// The row-loop state of a CTA copied into a value that is never address-taken, so it stays in
+// registers: Ctx is passed by reference to non-inlined phases and lives in local memory,
+// where every global store would force its fields to be reloaded inside the hot loops.
+struct Rows {
+  int s0, s1, warp, nwarps, lane, cb0;
+  const int64_t* soff;
+  const int32_t* sw;
+  int64_t cbase;
+  const int32_t* scol;
+  const double* sS;
+  const float* sS32;
+  const unsigned* cmk;
+  const int* csb;
+  const double* cxc;
+  double* csv;
+};
+__device__ __forceinline__ Rows rows_of(const Ctx& c) {
+  return Rows{c.s0, c.s1, c.warp, c.nwarps, c.lane, c.cb0, c.soff, c.sw, c.cbase, c.scol,
+              c.sS, c.sS32, c.cmk, c.csb, c.cxc, c.csv};
+}
+#define FOR_ROWS_R(r)                                                    \
+  for (int s_ = (r).s0 + (r).warp; s_ < (r).s1; s_ += (r).nwarps) {     \
+    const int i = s_ * 32 + (r).lane;                                    \
+    const int64_t off_ = (r).soff[s_ - (r).s0] + (r).lane;               \
+    const int64_t loff_ = off_ - (r).cbase;                              \
+    const int w_ = (r).sw[s_ - (r).s0];                                  \
+    (void)loff_;
+
+// gather_row over the staged pattern given by its column array
+template <class VT, class ZT, class AT, int CH>
+__device__ __forceinline__ AT gather_row_r(const int32_t* scol, const VT* sval, int64_t loff, int w, const ZT* z) {
+  AT acc = 0;
+  int jc[CH];
+  VT vc[CH];
+#pragma unroll
+  for (int q = 0; q < CH; ++q) {
+    const bool in = q < w;
+    jc[q] = in ? scol[loff + 32 * (int64_t)q] : 0;
+    vc[q] = in ? sval[loff + 32 * (int64_t)q] : VT(0);
+  }
+  for (int k0 = 0; k0 < w; k0 += CH) {
+    int jn[CH];
+    VT vn[CH];
+#pragma unroll
+    for (int q = 0; q < CH; ++q) {
+      const int k = k0 + CH + q;
+      const bool in = k < w;
+      jn[q] = in ? scol[loff + 32 * (int64_t)k] : 0;
+      vn[q] = in ? sval[loff + 32 * (int64_t)k] : VT(0);
+    }
+#pragma unroll
+    for (int q = 0; q < CH; ++q)
+      if (k0 + q < w) acc += vc[q] * (AT)z[jc[q]];
+#pragma unroll
+    for (int q = 0; q < CH; ++q) {
+      jc[q] = jn[q];
+      vc[q] = vn[q];
+    }
+  }
+  return acc;
+}
+
 // ---------------------------------------------------------------------------------------
 // Two-level additive preconditioner of the Poisson PCG (no counterpart in the reference,
 // whose jax.scipy.sparse.linalg.cg at scripts/solvers.py:221-231 uses Jacobi):
@@ -967,11 +1033,14 @@ __device__ __noinline__ bool pcg_solve_mixed(Ctx& c, const double* x) {
 //
 // P^T r is carried by the same recurrence as r (P^T r <- P^T r - alpha P^T s,
 // P^T s <- P^T w + beta P^T s), so the only new exchange per iteration is the box sums of
-// w = S z: each CTA sums its rows per box (warp sums per slice, then slices in order) and
-// publishes one partial per box it holds rows of, in slots ordered CTA by CTA; after the
-// iteration's reduction every CTA adds up every box's slots in slot order (bit-identical in
-// all CTAs) and updates its copy of P^T s and P^T r.  Each CTA then needs xc only for its
-// own boxes: its rows of the dense Ac^-1 (L2-resident) times P^T r.
+// w = S z, and it rides on the iteration's grid reduction (grid_reduce_coarse): before the
+// barrier each CTA publishes one partial per box it holds rows of (warp sums per slice,
+// then the slices in order), in slots ordered CTA by CTA; after the barrier every CTA loads
+// all slots with the reduction's partials, adds up every box's slots in slot order
+// (bit-identical in all CTAs) and updates its copy of P^T s and P^T r (coarse_update).  Each
+// CTA then needs xc only for its own boxes: its rows of Ac^-1, kept in shared memory for
+// the whole launch (FP32) when they fit, times P^T r.  On meshes whose PCG working set sits
+// in L2 an iteration is latency-bound, so the exchange adds no memory round trip of its own.
 // ---------------------------------------------------------------------------------------
 __device__ __forceinline__ int warp_min_i(int v) {
   for (int o = 16; o > 0; o >>= 1) v = min(v, __shfl_xor_sync(0xffffffffu, v, o));
@@ -982,12 +1051,11 @@ __device__ __forceinline__ int warp_max_i(int v) {
   return v;
 }
 
-// Sums of v over the rows of slice t (CTA-local index) in each of the slice's boxes; called
-// by all 32 lanes of the warp (lane = row i of the slice).
-// The slice's lane masks (shared memory, made at launch start) say which rows belong to
-// which box, so the hot loops read no box ids from global memory.
-__device__ __forceinline__ void coarse_slice_sum(const Ctx& c, int t, int i, double v) {
-  (void)i;
+// Sums of v over the rows of slice t (CTA-local index) in each of the slice's (at most two)
+// boxes; called by all 32 lanes of the warp (lane = row of the slice).  The slice's lane
+// masks (shared memory, made at launch start) say which rows belong to which box, so the
+// hot loops read no box ids from global memory.
+__device__ __forceinline__ void coarse_slice_sum(const Ctx& c, int t, double v) {
   const unsigned bit = 1u << c.lane, ml = c.cmk[2 * t], mh = c.cmk[2 * t + 1];
   const double slo = warp_sum((ml & bit) ? v : 0.0);
   const double shi = mh ? warp_sum((mh & bit) ? v : 0.0) : 0.0;
@@ -997,49 +1065,108 @@ __device__ __forceinline__ void coarse_slice_sum(const Ctx& c, int t, int i, dou
   }
 }
 
+__device__ __forceinline__ void coarse_slice_sum(const Rows& r, int t, double v) {
+  const unsigned bit = 1u << r.lane, ml = r.cmk[2 * t], mh = r.cmk[2 * t + 1];
+  const double slo = warp_sum((ml & bit) ? v : 0.0);
+  const double shi = mh ? warp_sum((mh & bit) ? v : 0.0) : 0.0;
+  if (r.lane == 0) {
+    r.csv[2 * t] = slo;
+    r.csv[2 * t + 1] = shi;
+  }
+}
+__device__ __forceinline__ double coarse_xc(const Rows& r, int t) {
+  const unsigned bit = 1u << r.lane;
+  const int rb = (r.cmk[2 * t] & bit) ? r.csb[2 * t] : ((r.cmk[2 * t + 1] & bit) ? r.csb[2 * t + 1] : -1);
+  return rb >= 0 ? r.cxc[rb - r.cb0] : 0.0;
+}
+
 // The box of this lane's row in slice t, -1 for Dirichlet and padding rows.
 __device__ __forceinline__ int coarse_row_box(const Ctx& c, int t) {
   const unsigned bit = 1u << c.lane;
   return (c.cmk[2 * t] & bit) ? c.csb[2 * t] : ((c.cmk[2 * t + 1] & bit) ? c.csb[2 * t + 1] : -1);
 }
 
-// The CTA's partial sum of each of its boxes into its slots: a warp per box, lanes over
-// the CTA's slices, a fixed-order warp sum.  Must come before the grid reduction (or
-// barrier) that publishes them.
-__device__ __forceinline__ void coarse_publish(Ctx& c) {
-  const unsigned long long t0 = (c.sy.timing && threadIdx.x == 0) ? globaltimer() : 0ull;
-  __syncthreads();
-  const int ns = c.s1 - c.s0;
-  for (int q = c.warp; q < c.cnb; q += c.nwarps) {
-    const int box = c.cb0 + q;
-    double acc = 0.0;
-    for (int t = c.lane; t < ns; t += 32)
-      acc += c.csb[2 * t] == box ? c.csv[2 * t] : (c.csb[2 * t + 1] == box ? c.csv[2 * t + 1] : 0.0);
-    acc = warp_sum(acc);
-    if (c.lane == 0) c.a.bslots[c.cslot0 + q] = acc;
+// grid_reduce plus the box exchange: before the barrier the CTA's box partials (a warp per
+// box over the slices' sums, a fixed-order warp sum) go to its slots; after it every slot is
+// loaded into shared memory together with the reduction's partials.
+template <int K>
+__device__ __noinline__ bool grid_reduce_coarse(Ctx& c, double (&v)[K]) {
+  Sync& s = c.sy;
+  __shared__ double sh[32][kMaxRed];
+  __shared__ double res[kMaxRed];
+  const int lane = c.lane, warp = c.warp, nw = c.nwarps;
+  const unsigned long long tr0 = (s.timing && threadIdx.x == 0) ? globaltimer() : 0ull;
+#pragma unroll
+  for (int k = 0; k < K; ++k) {
+    const double w = warp_sum(v[k]);
+    if (lane == 0) sh[warp][k] = w;
   }
-  if (c.sy.timing && threadIdx.x == 0) c.t_cpub += globaltimer() - t0;
+  __syncthreads();  // the slices' sums (c.csv) are complete
+  {
+    const int ns = c.s1 - c.s0;
+    for (int q = warp; q < c.cnb; q += nw) {
+      const int box = c.cb0 + q;
+      double acc = 0.0;
+      for (int t = lane; t < ns; t += 32)
+        acc += c.csb[2 * t] == box ? c.csv[2 * t] : (c.csb[2 * t + 1] == box ? c.csv[2 * t + 1] : 0.0);
+      acc = warp_sum(acc);
+      if (lane == 0) c.a.bslots[c.cslot0 + q] = acc;
+    }
+  }
+  double* set = s.red + (size_t)s.slot * kMaxRed * s.nblk;
+  if (threadIdx.x < K) {
+    const int k = threadIdx.x;
+    double a = sh[0][k];
+    for (int w = 1; w < nw; ++w) a += sh[w][k];
+    set[(size_t)k * s.nblk + s.blk] = a;
+  }
+  const unsigned long long tr1 = (s.timing && threadIdx.x == 0) ? globaltimer() : 0ull;
+  if (!grid_barrier(s)) return false;
+  const unsigned long long tr2 = (s.timing && threadIdx.x == 0) ? globaltimer() : 0ull;
+  if (warp < K) {
+    const double* p = set + (size_t)warp * s.nblk;
+    double got[kMaxCtaPerLane];
+#pragma unroll
+    for (int t = 0; t < kMaxCtaPerLane; ++t) got[t] = (lane + 32 * t < s.nblk) ? __ldcg(p + lane + 32 * t) : 0.0;
+    double a = got[0];
+#pragma unroll
+    for (int t = 1; t < kMaxCtaPerLane; ++t) a += got[t];
+    a = warp_sum(a);
+    if (lane == 0) res[warp] = a;
+  }
+  {
+    const int nsl = c.cbsl[c.a.nc];
+    const int bd = blockDim.x;
+    for (int t0 = threadIdx.x; t0 < nsl; t0 += 4 * bd) {
+      double x[4];
+#pragma unroll
+      for (int u = 0; u < 4; ++u) x[u] = t0 + u * bd < nsl ? __ldcg(c.a.bslots + t0 + u * bd) : 0.0;
+#pragma unroll
+      for (int u = 0; u < 4; ++u)
+        if (t0 + u * bd < nsl) c.cslv[t0 + u * bd] = x[u];
+    }
+  }
+  __syncthreads();
+#pragma unroll
+  for (int k = 0; k < K; ++k) v[k] = res[k];
+  s.slot ^= 1;
+  if (s.timing && threadIdx.x == 0) {
+    const unsigned long long tr3 = globaltimer();
+    s.t_pre += tr1 - tr0;
+    s.t_bar += tr2 - tr1;
+    s.t_post += tr3 - tr2;
+  }
+  return true;
 }
 
-// After the barrier: every box's total (its slots in order) folded into the coarse vectors.
-// restart: Pr = total, Ps = 0 (a fresh residual); else Ps = total + beta Ps, Pr -= alpha Ps.
-// The slots are first copied to shared memory with four independent loads in flight per
-// thread, so the step costs about one L2 round trip.
-__device__ __forceinline__ void coarse_gather(Ctx& c, bool restart, double alpha, double beta) {
-  const unsigned long long tg0 = (c.sy.timing && threadIdx.x == 0) ? globaltimer() : 0ull;
+// After grid_reduce_coarse: every box's total (its slots in order) folded into the coarse
+// vectors -- restart: Pr = total, Ps = 0 (a fresh residual); else Ps = total + beta Ps,
+// Pr -= alpha Ps -- then xc = Ac^-1 Pr for the CTA's own boxes.
+__device__ __noinline__ void coarse_update(Ctx& c, bool restart, double alpha, double beta) {
   const SolveArgs& a = c.a;
-  const int nsl = c.cbsl[a.nc];
-  const int bd = blockDim.x;
-  for (int t0 = threadIdx.x; t0 < nsl; t0 += 4 * bd) {
-    double v[4];
-#pragma unroll
-    for (int u = 0; u < 4; ++u) v[u] = t0 + u * bd < nsl ? __ldcg(a.bslots + t0 + u * bd) : 0.0;
-#pragma unroll
-    for (int u = 0; u < 4; ++u)
-      if (t0 + u * bd < nsl) c.cslv[t0 + u * bd] = v[u];
-  }
-  __syncthreads();
-  for (int q = threadIdx.x; q < a.nc; q += bd) {
+  const unsigned long long t0 = (c.sy.timing && threadIdx.x == 0) ? globaltimer() : 0ull;
+  const int nc = a.nc, bd = blockDim.x;
+  for (int q = threadIdx.x; q < nc; q += bd) {
     const int t1 = c.cbsl[q + 1];
     double w = 0.0;
     for (int t = c.cbsl[q]; t < t1; ++t) w += c.cslv[t];
@@ -1053,55 +1180,27 @@ __device__ __forceinline__ void coarse_gather(Ctx& c, bool restart, double alpha
     }
   }
   __syncthreads();
-  if (c.sy.timing && threadIdx.x == 0) c.t_cgat += globaltimer() - tg0;
-}
-
-// xc = Ac^-1 Pr for the CTA's own boxes.  Up to kOwnBoxes boxes: every thread takes columns
-// j = tid, tid + blockDim, ... of all the boxes' rows at once (independent L2 loads in
-// flight), then a fixed-order block sum per box.  More boxes (small grids): a warp per box.
-constexpr int kOwnBoxes = 8;
-template <class AT>
-__device__ __forceinline__ void coarse_solve_own(Ctx& c, const AT* Ainv) {
-  __shared__ double red[32][kOwnBoxes];
-  const unsigned long long ts0 = (c.sy.timing && threadIdx.x == 0) ? globaltimer() : 0ull;
-  const int nc = c.a.nc, nb = c.cnb;
-  if (nb <= kOwnBoxes) {
-    double acc[kOwnBoxes];
-#pragma unroll
-    for (int b = 0; b < kOwnBoxes; ++b) acc[b] = 0.0;
-    const AT* rows = Ainv + (size_t)c.cb0 * nc;
-    for (int j = threadIdx.x; j < nc; j += blockDim.x) {
-      const double pr = c.cPr[j];
-      AT v[kOwnBoxes];
-#pragma unroll
-      for (int b = 0; b < kOwnBoxes; ++b) v[b] = b < nb ? __ldg(rows + (size_t)b * nc + j) : AT(0);
-#pragma unroll
-      for (int b = 0; b < kOwnBoxes; ++b) acc[b] += (double)v[b] * pr;
-    }
-#pragma unroll
-    for (int b = 0; b < kOwnBoxes; ++b) {
-      if (b >= nb) break;
-      const double w = warp_sum(acc[b]);
-      if (c.lane == 0) red[c.warp][b] = w;
-    }
-    __syncthreads();
-    if (threadIdx.x < nb) {
-      double t = 0.0;
-      for (int w = 0; w < c.nwarps; ++w) t += red[w][threadIdx.x];
-      c.cxc[c.cb0 + threadIdx.x] = t;
-    }
-  } else {
-    for (int q = c.warp; q < nb; q += c.nwarps) {
-      const int box = c.cb0 + q;
-      const AT* row = Ainv + (size_t)box * nc;
-      double acc = 0.0;
+  // own boxes: a warp per box, lanes along its row of Ac^-1 (shared memory when staged)
+  for (int q = c.warp; q < c.cnb; q += c.nwarps) {
+    double acc = 0.0;
+    if (c.crows) {
+      const float* row = c.crows + (size_t)q * nc;
+      for (int j = c.lane; j < nc; j += 32) acc += (double)row[j] * c.cPr[j];
+    } else {
+      const float* row = a.Ainv32 + (size_t)(c.cb0 + q) * nc;
       for (int j = c.lane; j < nc; j += 32) acc += (double)__ldg(row + j) * c.cPr[j];
-      acc = warp_sum(acc);
-      if (c.lane == 0) c.cxc[box] = acc;
     }
+    acc = warp_sum(acc);
+    if (c.lane == 0) c.cxc[q] = acc;
   }
   __syncthreads();
-  if (c.sy.timing && threadIdx.x == 0) c.t_csol += globaltimer() - ts0;
+  if (c.sy.timing && threadIdx.x == 0) c.t_cgat += globaltimer() - t0;
+}
+
+// xc of the box of this lane's row in slice t (0 for Dirichlet and padding rows).
+__device__ __forceinline__ double coarse_xc(const Ctx& c, int t) {
+  const int rb = coarse_row_box(c, t);
+  return rb >= 0 ? c.cxc[rb - c.cb0] : 0.0;
 }
 
 // Pr = P^T v for a residual v given per row by val(i) (after a warm start changed it).
@@ -1109,11 +1208,11 @@ template <class F>
 __device__ __noinline__ bool coarse_restrict(Ctx& c, F val) {
   FOR_ROWS(c)
   (void)w_;
-  coarse_slice_sum(c, s_ - c.s0, i, val(i));
+  coarse_slice_sum(c, s_ - c.s0, val(i));
   END_ROWS
-  coarse_publish(c);
-  CHECK(grid_barrier(c.sy));
-  coarse_gather(c, true, 0.0, 0.0);
+  double v[1] = {0.0};
+  CHECK(grid_reduce_coarse<1>(c, v));
+  coarse_update(c, true, 0.0, 0.0);
   return true;
 }
 
@@ -1126,20 +1225,21 @@ __device__ __noinline__ bool pcg_solve_coarse(Ctx& c, const double* x) {
   const double* Dk = plane(a, P_D);
   const int64_t ps = a.nent;
   const int n = a.Npad;
+  const Rows rw = rows_of(c);
   double* pl = reinterpret_cast<double*>(a.rec[0]);
   double* z = reinterpret_cast<double*>(a.rec[1]);
   double rr, bb, zz;
   const bool zero_start = a.warm == WARM_ZERO;
   {  // b = sum_k dk x_k, r0 = b - S u, and its box sums
     double pr2 = 0, pb = 0, pz = 0;
-    FOR_ROWS(c)
+    FOR_ROWS_R(rw)
     double b = 0, su = 0;
 #pragma unroll 4
     for (int k = 0; k < w_; ++k) {
       const int64_t e = ENTRY(k);
-      const int j = c.scol[LENTRY(k)];
+      const int j = rw.scol[LENTRY(k)];
       b += __ldg(Dk + e) * x[j] + __ldg(Dk + ps + e) * x[n + j] + __ldg(Dk + 2 * ps + e) * x[2 * n + j];
-      if (!zero_start) su += c.sS[LENTRY(k)] * a.u[j];
+      if (!zero_start) su += rw.sS[LENTRY(k)] * a.u[j];
     }
     if (zero_start) a.u[i] = 0.0;
     const double r = b - su;
@@ -1148,11 +1248,10 @@ __device__ __noinline__ bool pcg_solve_coarse(Ctx& c, const double* x) {
     pr2 += r * r;
     pb += b * b;
     if (i < a.nreal) pz += (r * invd) * (r * invd);
-    coarse_slice_sum(c, s_ - c.s0, i, r);
+    coarse_slice_sum(rw, s_ - rw.s0, r);
     END_ROWS
-    coarse_publish(c);
     double v[3] = {pr2, pb, pz};
-    CHECK(grid_reduce<3>(c.sy, v, 0u));
+    CHECK(grid_reduce_coarse<3>(c, v));
     rr = v[0];
     bb = v[1];
     zz = v[2];
@@ -1160,12 +1259,13 @@ __device__ __noinline__ bool pcg_solve_coarse(Ctx& c, const double* x) {
   const double atol2 = fmax(a.tol_u * a.tol_u * bb, 0.0);
   int k = 0;
   if (!(rr > atol2 && k < a.max_pcg)) return true;
-  coarse_gather(c, true, 0.0, 0.0);
+  coarse_update(c, true, 0.0, 0.0);
   const double sig = sqrt(zz / (double)a.nreal);
   const bool recording = a.rec_cap > 0 && sig > 0.0;
   if (recording) record_features(c, x, pl, 1.0 / sig);
-  if (a.warm == WARM_LEARNED && sig > 0.0) {
+  if (a.warm == WARM_LEARNED && sig > 0.0 && rr > a.warm_gate2 * atol2) {
     double gunused;
+    c.lstarts += 1;
     CHECK(learned_start<TC>(c, x, sig, gunused, rr));
     if (!(rr > atol2)) {
       if (recording) record_targets(c, sig);
@@ -1173,16 +1273,13 @@ __device__ __noinline__ bool pcg_solve_coarse(Ctx& c, const double* x) {
     }
     CHECK(coarse_restrict(c, [&](int i) { return pl[i]; }));
   }
-  // z0 = r0/diag + P xc, p = 0, gamma = r0.z0
   double gamma, delta;
-  coarse_solve_own(c, a.Ainv);
-  {
+  {  // z0 = r0/diag + P xc, p = 0, gamma = r0.z0
     double pg = 0;
-    FOR_ROWS(c)
+    FOR_ROWS_R(rw)
     (void)w_;
     const double r = pl[i], invd = pl[3 * n + i];
-    const int rb = coarse_row_box(c, s_ - c.s0);
-    const double z0 = r * invd + (rb >= 0 ? c.cxc[rb] : 0.0);
+    const double z0 = r * invd + coarse_xc(rw, s_ - rw.s0);
     z[i] = z0;
     a.pp[i] = 0.0;
     pg += r * z0;
@@ -1193,30 +1290,27 @@ __device__ __noinline__ bool pcg_solve_coarse(Ctx& c, const double* x) {
   }
   {  // w0 = S z0, delta = w0.z0, box sums of w0
     double pd = 0;
-    FOR_ROWS(c)
-    const double acc = gather_row<double, double, double, 8>(c, c.sS, loff_, w_, z);
+    FOR_ROWS_R(rw)
+    const double acc = gather_row_r<double, double, double, 8>(rw.scol, rw.sS, loff_, w_, z);
     rec_store_w(a.rec[0], i, n, acc);
     pd += acc * z[i];
-    coarse_slice_sum(c, s_ - c.s0, i, acc);
+    coarse_slice_sum(rw, s_ - rw.s0, acc);
     END_ROWS
-    coarse_publish(c);
     double v[1] = {pd};
-    CHECK(grid_reduce<1>(c.sy, v, 0u));
+    CHECK(grid_reduce_coarse<1>(c, v));
     delta = v[0];
   }
   double alpha = gamma / delta, beta = 0.0;
-  coarse_gather(c, false, alpha, beta);
+  coarse_update(c, false, alpha, beta);
   for (;;) {
     if (c.sy.timing && threadIdx.x == 0) c.t_phase_start = globaltimer();
-    coarse_solve_own(c, a.Ainv);
     double pg = 0, pd = 0, pr2 = 0;
-    FOR_ROWS(c)
+    FOR_ROWS_R(rw)
     (void)w_;
     const PcgRec q = rec_load(a.rec[0], i, n);
     const double sn = q.w + beta * q.s;
     const double r = q.r - alpha * sn;
-    const int rb = coarse_row_box(c, s_ - c.s0);
-    const double zn = r * q.invd + (rb >= 0 ? c.cxc[rb] : 0.0);
+    const double zn = r * q.invd + coarse_xc(rw, s_ - rw.s0);
     const double p = z[i] + beta * a.pp[i];
     a.pp[i] = p;
     a.u[i] = a.u[i] + alpha * p;
@@ -1227,16 +1321,15 @@ __device__ __noinline__ bool pcg_solve_coarse(Ctx& c, const double* x) {
     pr2 += r * r;
     END_ROWS
     CHECK(grid_barrier(c.sy));
-    FOR_ROWS(c)
-    const double acc = gather_row<double, double, double, 8>(c, c.sS, loff_, w_, z);
+    FOR_ROWS_R(rw)
+    const double acc = gather_row_r<double, double, double, 8>(rw.scol, rw.sS, loff_, w_, z);
     rec_store_w(a.rec[0], i, n, acc);
     pd += acc * z[i];
-    coarse_slice_sum(c, s_ - c.s0, i, acc);
+    coarse_slice_sum(rw, s_ - rw.s0, acc);
     END_ROWS
-    coarse_publish(c);
     double v[3] = {pg, pd, pr2};
     if (c.sy.timing && threadIdx.x == 0) c.t_pcg_phase += globaltimer() - c.t_phase_start;
-    CHECK(grid_reduce<3>(c.sy, v, 0u));
+    CHECK(grid_reduce_coarse<3>(c, v));
     ++k;
     rr = v[2];
     if (!(rr > atol2 && k < a.max_pcg)) break;
@@ -1244,7 +1337,7 @@ __device__ __noinline__ bool pcg_solve_coarse(Ctx& c, const double* x) {
     alpha = v[0] / (v[1] - bn * v[0] / alpha);
     beta = bn;
     gamma = v[0];
-    coarse_gather(c, false, alpha, beta);
+    coarse_update(c, false, alpha, beta);
   }
   c.pcg_iters += k;
   if (recording) record_targets(c, sig);
@@ -1257,23 +1350,24 @@ __device__ __noinline__ bool pcg_solve_coarse(Ctx& c, const double* x) {
 template <bool TC>
 __device__ __noinline__ bool pcg_solve_mixed_coarse(Ctx& c, const double* x) {
   const SolveArgs& a = c.a;
-  const float* Dk = a.vals32 + (size_t)P_D * a.nent;  // FP32 divergence planes, FP64 sums
+  const double* Dk = plane(a, P_D);
   const int64_t ps = a.nent;
   const int n = a.Npad;
+  const Rows rw = rows_of(c);
   PcgRec32* rc = a.rec32[0];
   float* z = reinterpret_cast<float*>(a.rec32[1]);
   double rr, bb, zz;
   const bool zero_start = a.warm == WARM_ZERO;
   {  // FP64 residual of the warm start, FP32 inner record, box sums of the FP32 residual
     double p0 = 0, p1 = 0, pz = 0;
-    FOR_ROWS(c)
+    FOR_ROWS_R(rw)
     double b = 0, su = 0;
 #pragma unroll 4
     for (int k = 0; k < w_; ++k) {
       const int64_t e = ENTRY(k);
-      const int j = c.scol[LENTRY(k)];
+      const int j = rw.scol[LENTRY(k)];
       b += __ldg(Dk + e) * x[j] + __ldg(Dk + ps + e) * x[n + j] + __ldg(Dk + 2 * ps + e) * x[2 * n + j];
-      if (!zero_start) su += c.sS[LENTRY(k)] * a.u[j];
+      if (!zero_start) su += rw.sS[LENTRY(k)] * a.u[j];
     }
     if (zero_start) a.u[i] = 0.0;
     const double r = b - su;
@@ -1284,11 +1378,10 @@ __device__ __noinline__ bool pcg_solve_mixed_coarse(Ctx& c, const double* x) {
     p0 += r * r;
     p1 += b * b;
     if (i < a.nreal) pz += (r * invd) * (r * invd);
-    coarse_slice_sum(c, s_ - c.s0, i, (double)rf);
+    coarse_slice_sum(rw, s_ - rw.s0, (double)rf);
     END_ROWS
-    coarse_publish(c);
     double v[3] = {p0, p1, pz};
-    CHECK(grid_reduce<3>(c.sy, v, 0u));
+    CHECK(grid_reduce_coarse<3>(c, v));
     rr = v[0];
     bb = v[1];
     zz = v[2];
@@ -1298,24 +1391,22 @@ __device__ __noinline__ bool pcg_solve_mixed_coarse(Ctx& c, const double* x) {
   const double sig = sqrt(zz / (double)a.nreal);
   const bool active = rr > atol2 && a.max_pcg > 0;
   const bool recording = active && a.rec_cap > 0 && sig > 0.0;
-  if (active) coarse_gather(c, true, 0.0, 0.0);
+  if (active) coarse_update(c, true, 0.0, 0.0);
   if (recording) record_features(c, x, a.r64, 1.0 / sig);
-  if (active && a.warm == WARM_LEARNED && sig > 0.0) {
+  if (active && a.warm == WARM_LEARNED && sig > 0.0 && rr > a.warm_gate2 * atol2) {
     double rin2, gin;
+    c.lstarts += 1;
     CHECK(learned_start_mixed<TC>(c, x, sig, rr, rin2, gin));
     if (rr > atol2) CHECK(coarse_restrict(c, [&](int i) { return (double)rc[i].r; }));
   }
   for (int outer = 0; rr > atol2 && k < a.max_pcg && outer < 32; ++outer) {
-    // z0 = rf/diag + P xc, p = e = 0; gamma = rf.z0, rin2 = rf.rf
     double gamma, rin2, delta;
-    coarse_solve_own(c, a.Ainv32);
-    {
+    {  // z0 = rf/diag + P xc, p = e = 0; gamma = rf.z0, rin2 = rf.rf
       double pg = 0, p2 = 0;
-      FOR_ROWS(c)
+      FOR_ROWS_R(rw)
       (void)w_;
       const PcgRec32 q = rc[i];
-      const int rb = coarse_row_box(c, s_ - c.s0);
-      const float z0 = q.r * q.invd + (rb >= 0 ? (float)c.cxc[rb] : 0.f);
+      const float z0 = q.r * q.invd + (float)coarse_xc(rw, s_ - rw.s0);
       z[i] = z0;
       a.pp32[i] = 0.f;
       a.e32[i] = 0.f;
@@ -1330,30 +1421,27 @@ __device__ __noinline__ bool pcg_solve_mixed_coarse(Ctx& c, const double* x) {
     const double inner_tol2 = fmax(1e-10 * rin2, 0.25 * atol2);  // 1e-5 relative, or the outer target
     {  // w0 = S32 z0, delta = w0.z0, box sums of w0
       double pd = 0;
-      FOR_ROWS(c)
-      const float acc = gather_row<float, float, float, kChunk32>(c, c.sS32, loff_, w_, z);
+      FOR_ROWS_R(rw)
+      const float acc = gather_row_r<float, float, float, kChunk32>(rw.scol, rw.sS32, loff_, w_, z);
       rc[i].w = acc;
       pd += (double)acc * (double)z[i];
-      coarse_slice_sum(c, s_ - c.s0, i, (double)acc);
+      coarse_slice_sum(rw, s_ - rw.s0, (double)acc);
       END_ROWS
-      coarse_publish(c);
       double v[1] = {pd};
-      CHECK(grid_reduce<1>(c.sy, v, 0u));
+      CHECK(grid_reduce_coarse<1>(c, v));
       delta = v[0];
     }
     double alpha = gamma / delta, beta = 0.0;
-    coarse_gather(c, false, alpha, beta);
+    coarse_update(c, false, alpha, beta);
     for (;;) {
-      coarse_solve_own(c, a.Ainv32);
       const float af = (float)alpha, bf = (float)beta;
       double pg = 0, pd = 0, pr2 = 0;
-      FOR_ROWS(c)
+      FOR_ROWS_R(rw)
       (void)w_;
       const PcgRec32 q = rc[i];
       const float sn = q.w + bf * q.s;
       const float r = q.r - af * sn;
-      const int rb = coarse_row_box(c, s_ - c.s0);
-      const float zn = r * q.invd + (rb >= 0 ? (float)c.cxc[rb] : 0.f);
+      const float zn = r * q.invd + (float)coarse_xc(rw, s_ - rw.s0);
       const float p = z[i] + bf * a.pp32[i];
       a.pp32[i] = p;
       a.e32[i] = a.e32[i] + af * p;
@@ -1363,43 +1451,41 @@ __device__ __noinline__ bool pcg_solve_mixed_coarse(Ctx& c, const double* x) {
       pr2 += (double)r * (double)r;
       END_ROWS
       CHECK(grid_barrier(c.sy));
-      FOR_ROWS(c)
-      const float acc = gather_row<float, float, float, kChunk32>(c, c.sS32, loff_, w_, z);
+      FOR_ROWS_R(rw)
+      const float acc = gather_row_r<float, float, float, kChunk32>(rw.scol, rw.sS32, loff_, w_, z);
       rc[i].w = acc;
       pd += (double)acc * (double)z[i];
-      coarse_slice_sum(c, s_ - c.s0, i, (double)acc);
+      coarse_slice_sum(rw, s_ - rw.s0, (double)acc);
       END_ROWS
-      coarse_publish(c);
       double v[3] = {pg, pd, pr2};
-      CHECK(grid_reduce<3>(c.sy, v, 0u));
+      CHECK(grid_reduce_coarse<3>(c, v));
       ++k;
       if (!(v[2] > inner_tol2 && k < a.max_pcg)) break;
       const double bn = v[0] / gamma;
       alpha = v[0] / (v[1] - bn * v[0] / alpha);
       beta = bn;
       gamma = v[0];
-      coarse_gather(c, false, alpha, beta);
+      coarse_update(c, false, alpha, beta);
     }
     {  // u += e, r -= S e in FP64; next inner record and its box sums
       double p0 = 0;
-      FOR_ROWS(c)
+      FOR_ROWS_R(rw)
       double se = 0;
 #pragma unroll 8
-      for (int k2 = 0; k2 < w_; ++k2) se += c.sS[LENTRY(k2)] * (double)a.e32[c.scol[LENTRY(k2)]];
+      for (int k2 = 0; k2 < w_; ++k2) se += rw.sS[LENTRY(k2)] * (double)a.e32[rw.scol[LENTRY(k2)]];
       a.u[i] = a.u[i] + (double)a.e32[i];
       const double r = a.r64[i] - se;
       a.r64[i] = r;
       const float rf = (float)r, inv = (float)__ldg(a.invdS + i);
       rc[i] = PcgRec32{rf, 0.f, 0.f, inv};
       p0 += r * r;
-      coarse_slice_sum(c, s_ - c.s0, i, (double)rf);
+      coarse_slice_sum(rw, s_ - rw.s0, (double)rf);
       END_ROWS
-      coarse_publish(c);
       double v[1] = {p0};
-      CHECK(grid_reduce<1>(c.sy, v, 0u));
+      CHECK(grid_reduce_coarse<1>(c, v));
       rr = v[0];
     }
-    if (rr > atol2 && k < a.max_pcg) coarse_gather(c, true, 0.0, 0.0);
+    if (rr > atol2 && k < a.max_pcg) coarse_update(c, true, 0.0, 0.0);
   }
   c.pcg_iters += k;
   if (recording) record_targets(c, sig);
@@ -1960,6 +2046,14 @@ __device__ __forceinline__ void solve_body(const SolveArgs& args, int nblk, int 
     c.cb0 = __ldg(args.ctabox + 3 * blk);
     c.cnb = __ldg(args.ctabox + 3 * blk + 1);
     c.cslot0 = __ldg(args.ctabox + 3 * blk + 2);
+    if (args.co_rows >= c.cnb && c.cnb > 0) {  // the CTA's rows of Ac^-1 for the whole launch
+      float* rows = reinterpret_cast<float*>(
+          (reinterpret_cast<uintptr_t>(bsl + args.nc + 1) + 15) & ~static_cast<uintptr_t>(15));
+      const float* src = args.Ainv32 + (size_t)c.cb0 * args.nc;
+      const int nrow = c.cnb * args.nc;
+      for (int t = threadIdx.x; t < nrow; t += blockDim.x) rows[t] = __ldg(src + t);
+      c.crows = rows;
+    }
     for (int t = c.warp; t < c.s1 - c.s0; t += c.nwarps) {
       const int rb = __ldg(args.rbox + (size_t)(c.s0 + t) * 32 + c.lane);
       const int lo = warp_min_i(rb >= 0 ? rb : INT_MAX), hi = warp_max_i(rb);
@@ -1999,6 +2093,7 @@ __device__ __forceinline__ void solve_body(const SolveArgs& args, int nblk, int 
     ok = minimize<TC>(c, f, mh, k);
   }
   if (ok && blk == 0 && threadIdx.x == 0) {
+    args.resi[8] = c.lstarts;
     args.resi[1] = c.evals;
     args.resi[2] = c.pcg_iters;
     args.resi[3] = c.shrinks;
@@ -2060,10 +2155,12 @@ struct StagePlan {
   size_t smem;
   int extra_off;  // offset of the extra region, -1 = none
   int co_off;     // offset of the coarse region, -1 = none
+  int co_rows;    // rows of Ac^-1 each CTA stages (the most boxes a CTA holds), 0 = none
 };
 // Regions: [staged entries][slice metadata][coarse vectors: Ps, Pr, xc (nc doubles each),
 // the staged box slots (nc + kMaxGrid doubles), per slice two partial sums, two box ids and
-// two lane masks, every box's first slot (nc + 1 ints)][tensor-core network]
+// two lane masks, every box's first slot (nc + 1 ints), the CTA's rows of Ac^-1 in FP32
+// when they fit][tensor-core network]
 StagePlan stage_plan(const DevMesh& m, int grid, size_t limit, size_t extra = 0, bool allow_stage = true,
                      int nc = 0) {
   int64_t emax = 0, smax = 0;
@@ -2079,13 +2176,35 @@ StagePlan stage_plan(const DevMesh& m, int grid, size_t limit, size_t extra = 0,
   const size_t need = (size_t)emax * (sizeof(double) + sizeof(int32_t) + (m.vals32 ? sizeof(float) : 0));
   StagePlan p;
   p.stage = (allow_stage && need + meta + 16 + coarse + (extra ? extra + 1024 : 0) <= limit) ? 1 : 0;
+  // the two-level preconditioner's rows of Ac^-1 per CTA, staged when they fit beside the rest
+  p.co_rows = 0;
+  size_t rows = 0;
+  if (nc > 0) {
+    int bmax = 0;
+    for (int b = 0; b < grid; ++b) {
+      const int64_t r0 = kSlice * ((m.h.nslices * b) / grid), r1 = kSlice * ((m.h.nslices * (b + 1)) / grid);
+      int lo = INT_MAX, hi = -1;
+      for (int64_t i = r0; i < r1; ++i)
+        if (m.h.rbox[i] >= 0) {
+          lo = std::min(lo, m.h.rbox[i]);
+          hi = std::max(hi, m.h.rbox[i]);
+        }
+      if (hi >= 0) bmax = std::max(bmax, hi - lo + 1);
+    }
+    const size_t want = (size_t)bmax * nc * sizeof(float) + 16;
+    const size_t used = (p.stage ? need : 0) + meta + 16 + coarse + (extra ? extra + 1024 : 0);
+    if (bmax > 0 && used + want <= limit) {
+      p.co_rows = bmax;
+      rows = want;
+    }
+  }
   p.stage_max = emax;
   p.meta_max = smax;
   p.smem = (p.stage ? ((need + 15) & ~(size_t)15) : 0) + meta;
   p.co_off = -1;
   if (coarse) {
     p.co_off = (int)((p.smem + 15) & ~(size_t)15);
-    p.smem = (size_t)p.co_off + coarse;
+    p.smem = (size_t)p.co_off + coarse + rows;
   }
   p.extra_off = -1;
   if (extra) {  // the tensor-core network's region, 1024-byte aligned, after the metadata
@@ -2177,6 +2296,7 @@ void solver_configure(DevMesh& m) {
   m.smem = sp.smem;
   m.tc_off = sp.extra_off;
   m.co_off = sp.co_off;
+  m.co_rows = sp.co_rows;
   // The attribute is per kernel, shared by every mesh: raise it to the device limit once
   // (occupancy follows each launch's actual request).
   const int dsm = (int)(prop.sharedMemPerBlockOptin - 16 * 1024);
@@ -2329,8 +2449,10 @@ SolveArgs solver_args(const DevMesh& m, int mode, double h, const mm_solver_para
   a.bslot = m.bslot;
   a.ctabox = m.ctabox;
   a.co_off = m.co_off;
+  a.co_rows = m.co_rows;
   a.bar_stall = m.bar_stall;
   a.warm = m.warm;
+  a.warm_gate2 = m.warm_gate * m.warm_gate;
   a.nreal = (int32_t)m.h.N;
   a.mlp = m.mlp;
   a.feat = m.feat;
@@ -2371,7 +2493,7 @@ SolveArgs solver_args(const DevMesh& m, int mode, double h, const mm_solver_para
 cudaError_t launch_prep(DevMesh& m, cudaStream_t st) {
   cudaError_t e = cudaMemsetAsync(m.bar, 0, sizeof(unsigned long long), st);
   if (e == cudaSuccess) e = cudaMemsetAsync(m.flags, 0, 2 * sizeof(int), st);
-  if (e == cudaSuccess) e = cudaMemsetAsync(m.resi, 0, 8 * sizeof(long long), st);
+  if (e == cudaSuccess) e = cudaMemsetAsync(m.resi, 0, kResI * sizeof(long long), st);
   return e;
 }
 

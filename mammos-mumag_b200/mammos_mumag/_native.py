@@ -74,6 +74,7 @@ EXPORTED = (
     "mm_mesh_read_samples",
     "mm_debug_stall_barriers",
     "mm_mesh_get_coarse",
+    "mm_mesh_set_learned_gate",
 )
 WARM_PREVIOUS, WARM_ZERO, WARM_LEARNED = 0, 1, 2
 MLP_FEATURES = 16
@@ -126,6 +127,7 @@ class StepResult(C.Structure):
         ("barriers", C.c_int64),
         ("device_ms", C.c_double),
         ("status", C.c_int),
+        ("learned_starts", C.c_int64),
     ]
 
     def as_dict(self):
@@ -255,6 +257,7 @@ def load():
         "mm_mesh_read_samples": (C.c_int, [C.c_void_p, _F, _F, _I32, C.c_int64, _I64]),
         "mm_debug_stall_barriers": (C.c_int, [C.c_void_p, C.c_int32]),
         "mm_mesh_get_coarse": (C.c_int, [C.c_void_p, _I32, _I32]),
+        "mm_mesh_set_learned_gate": (C.c_int, [C.c_void_p, C.c_double]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -399,6 +402,11 @@ class Mesh:
         WARM_LEARNED (``model`` must stay alive while the mesh uses it)."""
         check(load().mm_mesh_set_warm_start(self._h, int(mode), model._h if model is not None else None))
         self._warm_model = model
+
+    def set_learned_gate(self, ratio: float):
+        """Run the learned start only on solves whose initial residual exceeds ``ratio`` times
+        the stop tolerance (0 or 1: every solve)."""
+        check(load().mm_mesh_set_learned_gate(self._h, float(ratio)))
 
     def record_samples(self, capacity: int, stride: int = 1, seed: int = 0):
         """Record (features, target) pairs of 1/stride of the (node, solve) pairs from now on."""
