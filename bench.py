@@ -1,32 +1,43 @@
 """Benchmark of the hysteresis hot path: field steps per second on the B200 path.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
-                    [--workload multigrain|single|large|batch]
+                    [--workload large|multigrain|single|batch]
 
-A step is one full field sweep of the workload (the reference's loop, scripts/loop.py:71-142,
-run to the last field value).  The default workload is the multigrain cube: 80 nm edge,
-32^3 cells x 6 tets (196,608 tets, 35,937 nodes), 8 seeded Voronoi grains with easy axes in
-a 15 degree cone, a 2 nm grain-boundary phase (A=2e-12 J/m, K1=0, Js=0.5 T), field along z
-tilted 1 degree toward x, +8 T -> -8 T in 0.1 T steps (161 field steps), FP64.  Inputs are
+The default workload is the large multigrain cube: 200 nm edge, 80^3 cells x 6 tets
+(3,072,000 tets, 531,441 nodes), 27 seeded Voronoi grains with easy axes in a 20 degree cone,
+a 2 nm grain-boundary phase (A=2e-12 J/m, K1=0, Js=0.5 T), field along z from +8 T to -8 T in
+0.05 T steps (321 field steps, the reference's loop, scripts/loop.py:71-124).  Inputs are
 seeded synthetic data of those shapes.
 
-``value`` is whole-job field steps/s of the path the metric names -- mixed precision with
-the learned warm start (``config.path`` = learned_mixed; the plain FP64 path for the
-single-grain workload or with ``--no-learned``) -- with the mesh operators resident in HBM
-(device time from CUDA events on the library's stream); ``variants`` holds the plain FP64,
-mixed and learned+mixed sweeps of the same run with their PCG iterations per solve and
-Hc/Mr against FP64.  ``e2e`` is the headline path through the public API from host buffers
-(mesh build + state upload + sweep + result read-back), ``cpu_baseline`` the CPU oracle on
-a bounded sample.  The network of the learned warm start is trained at set-up (untimed) on
-plain loops of other seeds of the same mesh family.  Multi-GPU runs are independent replicas (one sweep per rank,
-no collective on the data path).  ``--impl reference`` times the CPU oracle alone (the
-reference's algorithm restated; its own JAX/escript stack is not installable here).
+Each path ("variant") first runs the whole sweep once, one field step per launch, untimed:
+that gives its coercive field Hc and remanence Mr, its per-step counters and the state
+(m, u) before every field step of a window of consecutive field steps around the switching
+field (located on the plain FP64 sweep: the steps where the most work is).  A timed "step" is
+then one field step of that window, started from its saved state (the state restored before
+each step), cycling through the window; ``value`` is field steps per second of the path the
+metric names -- mixed precision with the learned warm start, here with the two-level Poisson
+preconditioner (``config.path``) -- with the operators resident in HBM (device time from CUDA
+events on the library's stream, the L2 flushed before each step).  ``variants`` holds every
+path of the same run: the plain FP64 path (the reference's method: the denominator), mixed
+precision, mixed with the two-level preconditioner, and the learned start with and without
+its residual gate, each with the window rate, the whole-sweep rate, PCG iterations per solve,
+Hc/Mr and their deviation from the FP64 path (and from the FP64 oracle's sweep where one is
+committed, tests/golden/sweep_*.npz).  ``e2e`` is the headline path through the public API
+from pinned host buffers: the mesh built once (a preprocessing-cache hit), then per step the
+state uploaded, the field step run and the state read back.  ``cpu_baseline`` is the NumPy
+oracle on a bounded sample of the same workload (field step 1 from the initial state), timed
+in a separate process on the host cores meanwhile, beside the GPU paths' rates on that same
+field step.  Multi-GPU runs are independent replicas (one per rank, no collective on the data
+path).  ``--impl reference`` times the CPU oracle alone on the same workload (the reference's
+algorithm restated; its own JAX/escript stack is not installable here).
 """
 
 from __future__ import annotations
 
 import argparse
+import collections
 import json
+import math
 import os
 import pathlib
 import statistics
@@ -45,90 +56,99 @@ import numpy as np  # noqa: E402
 METRIC = "field steps/s + PCG iters/solve: learned+mixed vs plain FP64 GPU at |ΔHc|<1%"
 UNIT = "field steps/s"
 L2_FLUSH_BYTES = 256 << 20
-# DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) per algorithmic byte of one
-# k_solve field-step launch, from one ncu capture of each workload and path
-# (python -m mammos_mumag.perfcase field-step ...): the multigrain FP64 launch moved
-# 133.8 MB for 5,422 MB of algorithmic bytes, the multigrain learned+mixed launch (network
-# on tcgen05) 406.5 MB for 4,128 MB, the large mesh's FP64 launch 178.3 GB for 162.8 GB.
-# The bench scales the ratio to its own average launch (traffic grows with the work
-# counters the algorithmic bytes are computed from).
-TRAFFIC_PER_ALGORITHMIC_BYTE = {("multigrain", "fp64"): 133.8 / 5422.4,
-                                ("multigrain", "learned_mixed"): 406.5 / 4128.4,
-                                ("large", "fp64"): 178.3 / 162.8}
+DBL_MAX = 1.7976931348623157e308
+# DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) per algorithmic byte of one k_solve
+# field-step launch, from one ncu capture (profiles/k_solve_large_mixed_coarse_traffic.md): field
+# step 2 of the large mesh on the mixed path with the two-level preconditioner (the headline's
+# kernel; its gated learned start ran on none of that step's solves) moved 28.74 GB of DRAM
+# traffic for 40.515 GB of algorithmic bytes (the FP32 Poisson operator stays in L2).  The bench
+# scales the ratio to its own average launch (traffic grows with the work counters the
+# algorithmic bytes are computed from).
+TRAFFIC_PER_ALGORITHMIC_BYTE = {("large", "learned_mixed_coarse"): 28.741132032 / 40.515,
+                                ("large", "mixed_coarse"): 28.741132032 / 40.515}
+
+# Seeded synthetic workloads: mesh (synthetic.multigrain / single_grain arguments), field
+# tilt from z toward x (degrees), sweep (hstart, hfinal, hstep, mstep, mfinal), aggregate
+# size of the two-level preconditioner, length of the timed window (field steps), the oracle
+# sweep committed for it (tests/golden), description.
+WORKLOADS = {
+    "large": dict(
+        mesh=dict(kind="multigrain", n=80, L=200.0, grains=27, cone_deg=20.0, gb=2.0), tilt=0.0,
+        sweep=(8.0, -8.0, -0.05, 0.4, -2.0), coarse=512, window=12, oracle=None, train_seeds=2,
+        train_steps=20,
+        desc="large multigrain 200 nm, 80^3 x 6 tets (3,072,000 tets, 531,441 nodes), 27 Voronoi grains "
+             "(20 deg cone) + 2 nm grain-boundary phase, field along z, +8 -> -8 T in 0.05 T steps "
+             "(321 field steps)"),
+    "multigrain": dict(
+        mesh=dict(kind="multigrain", n=32, L=80.0, grains=8, cone_deg=15.0, gb=2.0), tilt=1.0,
+        sweep=(8.0, -8.0, -0.1, 0.4, -2.0), coarse=256, window=12, oracle="sweep_multigrain.npz",
+        train_seeds=4, train_steps=0,
+        desc="multigrain 80 nm, 32^3 x 6 tets (196,608 tets, 35,937 nodes), 8 Voronoi grains "
+             "(15 deg cone) + 2 nm grain-boundary phase, field 1 deg off z, +8 -> -8 T in 0.1 T "
+             "steps (161 field steps)"),
+    "single": dict(
+        mesh=dict(kind="single_grain", n=16, L=20.0), tilt=0.0,
+        sweep=(8.0, -8.0, -0.2, 0.4, -2.0), coarse=64, window=8, oracle="sweep_single.npz",
+        train_seeds=0, train_steps=0,
+        desc="single grain 20 nm, 16^3 x 6 tets (24,576 tets, 4,913 nodes), Js=1.61 T, "
+             "A=7.7e-12 J/m, K1=4.3e6 J/m^3, +8 -> -8 T in 0.2 T steps (81 field steps)"),
+}
 
 
-def batch_workload(count: int = 64, seed: int = 0):
-    """64 independent loops on seeded meshes of uneven size: structured grids of 12..40 cells
-    per edge (h = 1.25 nm), 6 tets per cell, 1..27 Voronoi grains with easy axes in a cone of
-    up to 30 degrees, the single-grain material, a 2 nm grain-boundary phase."""
+def workload(name: str, seed: int = 0):
+    """(X, T, tag, krn, m0, hdir) of a workload, from its seed."""
     from mammos_mumag import synthetic
 
-    rng = np.random.default_rng(seed)
-    out = []
-    for q in range(count):
-        n = int(rng.integers(12, 41))
-        grains = int(rng.integers(1, 28))
-        cone = float(rng.uniform(0.0, 30.0))
-        out.append(synthetic.multigrain(n=n, L=1.25 * n, grains=grains, cone_deg=cone, gb=2.0 if grains > 1 else 0.0,
-                                        seed=seed * 1000 + q))
-    return out
+    w = WORKLOADS[name]
+    mesh = dict(w["mesh"])
+    kind = mesh.pop("kind")
+    X, T, tag, krn, m0 = getattr(synthetic, kind)(seed=seed, **mesh)
+    d = math.radians(w["tilt"])
+    return X, T, tag, krn, m0, [math.sin(d), 0.0, math.cos(d)]
 
 
-def workload(name: str, seed: int):
-    from mammos_mumag import synthetic
-
-    if name == "large":
-        X, T, tag, krn, m0 = synthetic.multigrain(n=80, L=200.0, grains=27, cone_deg=20.0, gb=2.0, seed=seed)
-        hdir = [0.0, 0.0, 1.0]
-        sweep = dict(hstart=8.0, hfinal=-8.0, hstep=-0.05, mstep=0.4, mfinal=-2.0, max_steps=20)
-        desc = ("large multigrain 200 nm, 80^3 x 6 tets (3,072,000 tets, 531,441 nodes), 27 Voronoi grains "
-                "(20 deg cone) + 2 nm grain-boundary phase, +8 T in 0.05 T steps, first 20 field steps of 321")
-        return X, T, tag, krn, m0, hdir, sweep, desc
-    if name == "single":
-        X, T, tag, krn, m0 = synthetic.single_grain(16, 20.0, seed=seed)
-        hdir = [0.0, 0.0, 1.0]
-        sweep = dict(hstart=8.0, hfinal=-8.0, hstep=-0.2, mstep=0.4, mfinal=-2.0)
-        desc = ("single grain 20 nm, 16^3 x 6 tets (24,576 tets, 4,913 nodes), Js=1.61 T, "
-                "A=7.7e-12 J/m, K1=4.3e6 J/m^3, +8 -> -8 T in 0.2 T steps (81 field steps)")
-    else:
-        X, T, tag, krn, m0 = synthetic.multigrain(n=32, L=80.0, grains=8, cone_deg=15.0, gb=2.0, seed=seed)
-        d = np.radians(1.0)
-        hdir = [float(np.sin(d)), 0.0, float(np.cos(d))]
-        sweep = dict(hstart=8.0, hfinal=-8.0, hstep=-0.1, mstep=0.4, mfinal=-2.0)
-        desc = ("multigrain 80 nm, 32^3 x 6 tets (196,608 tets, 35,937 nodes), 8 Voronoi grains "
-                "(15 deg cone) + 2 nm grain-boundary phase, field 1 deg off z, +8 -> -8 T in 0.1 T "
-                "steps (161 field steps)")
-    return X, T, tag, krn, m0, hdir, sweep, desc
+def headline_of(name: str) -> str:
+    return "learned_mixed_coarse" if WORKLOADS[name]["train_seeds"] > 0 else "mixed_coarse"
 
 
-def hc_mr(rows):
-    """Coercive field and remanence of the sweep's rows (``mammos_mumag.hysteresis``)."""
-    from mammos_mumag.hysteresis import coercivity_remanence
+def config_of(name: str, world: int) -> dict:
+    """The run's configuration: static, so the reference arm prints the same dictionary."""
+    w = WORKLOADS[name]
+    head = headline_of(name)
+    return {
+        "workload": w["desc"],
+        "step": (f"one field step of a {w['window']}-step window around the switching field, from its "
+                 "saved state (restored before each step)"),
+        "path": head,
+        "precision": "mixed (FP32 operator planes and inner PCG, FP64 refinement, reductions, energies)",
+        "preconditioner": f"two-level additive (Jacobi + {w['coarse']}-node box aggregates); FP64 path: Jacobi",
+        "warm_start": "learned (residual-gated)" if head.startswith("learned") else "previous u (reference)",
+        "parallelism": f"replicas x{world}",
+        "l2": "256 MB buffer written before every timed step (L2 flush)",
+    }
 
-    return coercivity_remanence(rows)
 
-
-def algorithmic_bytes(steps, Z: int, N: int, s: int = 8, s_pcg: int | None = None) -> float:
+def algorithmic_bytes(steps, Z: int, N: int, mixed: bool, coarse: bool) -> float:
     """Compulsory bytes of the persistent field-step kernel, summed over its work counters.
 
-    Z = unpadded node-pair entries of the SELL pattern, N = nodes, s = value bytes of the
-    energy / NCG / M_inv work, s_pcg = value bytes of the Poisson PCG iterations (4 when they
-    run on FP32 planes, mixed precision; default s).
-    Per Poisson PCG iteration: one S SpMV Z(s+4) + 4(N+1) + 2Ns and the fused vector
-    update 9Ns.  Per energy evaluation outside the PCG: divergence + initial residual
-    Z(4s+4) + 5Ns, exchange/anisotropy/gradient gathers Z(10s+4) + 14Ns, the normalised
-    trial point 9Ns.  Per M_inv iteration: the C SpMV Z(7s+4) + 6Ns and ~8 three-vector
-    passes 24Ns.  Per NCG iteration: ~12 three-vector passes 36Ns.
+    Z = unpadded node-pair entries, N = nodes; operator values in FP32 (4 B) for the mixed
+    path, FP64 (8 B) otherwise; vectors FP64 except the PCG's FP32 inner vectors.
+    Per Poisson PCG iteration: the S SpMV Z(s+4) + 4(N+1) + 2Ns and the vector update 9Ns
+    (+ Ns for the stored z with the two-level preconditioner).  Per energy evaluation outside
+    the PCG: divergence and initial residual Z(3s+8+4) + 5N*8, exchange/anisotropy/gradient
+    gathers Z(10s+4) + 14N*8, the normalised trial point 9N*8.  Per M_inv iteration: the C SpMV
+    Z(7s+4) + 30N*8.  Per NCG iteration: ~12 three-vector passes 36N*8.  The mixed path's
+    refinement passes are not counted (a lower bound).
     """
-    sp = s if s_pcg is None else s_pcg
+    s = 4 if mixed else 8
     pcg = sum(st["pcg_iters"] for st in steps)
     ev = sum(st["evals"] for st in steps)
     mi = sum(st["minv_iters"] for st in steps)
     ncg = sum(st["ncg_iters"] for st in steps)
-    b = pcg * (Z * (sp + 4) + 4 * (N + 1) + 2 * N * sp + 9 * N * sp)
-    b += ev * (Z * (4 * s + 4) + 5 * N * s + Z * (10 * s + 4) + 14 * N * s + 9 * N * s)
-    b += mi * (Z * (7 * s + 4) + 30 * N * s)
-    b += ncg * 36 * N * s
+    b = pcg * (Z * (s + 4) + 4 * (N + 1) + 2 * N * s + 9 * N * s + (N * s if coarse else 0))
+    b += ev * (Z * (3 * s + 12) + 5 * N * 8 + Z * (10 * s + 4) + 14 * N * 8 + 9 * N * 8)
+    b += mi * (Z * (7 * s + 4) + 30 * N * 8)
+    b += ncg * 36 * N * 8
     return float(b)
 
 
@@ -175,21 +195,6 @@ class ClockSampler:
                 "reasons": reasons, "samples": len(self.rows)}
 
 
-def cpu_sample(name: str, n_field_steps: int, seed: int = 0):
-    """The CPU oracle (NumPy/SciPy restatement of the reference's loop) on the first
-    ``n_field_steps`` field steps of the workload.  Returns (field steps/s, seconds, threads)."""
-    import oracle as O
-
-    X, T, tag, krn, m0, hdir, sweep, _ = workload(name, seed)
-    P = O.Problem(X, T, tag, krn)
-    par = dict(hdir=hdir, tol_fun=1e-10, tol_u=1e-10, precond_iter=10, hmag_on=1, m=[0, 0, 1.0], **sweep)
-    par.pop("max_steps", None)
-    t = time.perf_counter()
-    rows, _ = O.run_loop(P, par, m0=m0, max_steps=n_field_steps)
-    dt = time.perf_counter() - t
-    return len(rows) / dt, dt, len(rows)
-
-
 def dist_setup():
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -221,85 +226,330 @@ def dist_barrier(world: int):
         dist.barrier()
 
 
-_REF_CACHE = {}
+def batch_workload(count: int = 64, seed: int = 0):
+    """64 independent loops on seeded meshes of uneven size: structured grids of 12..40 cells
+    per edge (h = 1.25 nm), 6 tets per cell, 1..27 Voronoi grains with easy axes in a cone of
+    up to 30 degrees, the single-grain material, a 2 nm grain-boundary phase."""
+    from mammos_mumag import synthetic
+
+    rng = np.random.default_rng(seed)
+    out = []
+    for q in range(count):
+        n = int(rng.integers(12, 41))
+        grains = int(rng.integers(1, 28))
+        cone = float(rng.uniform(0.0, 30.0))
+        out.append(synthetic.multigrain(n=n, L=1.25 * n, grains=grains, cone_deg=cone, gb=2.0 if grains > 1 else 0.0,
+                                        seed=seed * 1000 + q))
+    return out
 
 
-def _ref_sample(job):
-    """One bounded sample of the CPU reference path in a worker process: the first
-    ``n_fs`` field steps of the workload's sweep.  The oracle's operators are built once
-    per process (cached), so repeated samples time the loop alone."""
+_ORACLE = {}
+
+
+def oracle_step(name: str):
+    """One bounded sample of the reference's algorithm on the host: field step 1 of the
+    workload's sweep from its initial state (u = 0), by the NumPy/SciPy oracle (the
+    reference's scripts/loop.py restated), single-threaded.  The oracle's operators are built
+    once per process (untimed).  Returns (seconds, evaluations, PCG iterations)."""
     import oracle as O
 
-    name, n_fs = job
-    if name not in _REF_CACHE:
-        X, T, tag, krn, m0, hdir, sweep, _ = workload(name, 0)
-        par = dict(hdir=hdir, tol_fun=1e-10, tol_u=1e-10, precond_iter=10, hmag_on=1, m=[0, 0, 1.0], **sweep)
-        par.pop("max_steps", None)
-        _REF_CACHE[name] = (O.Problem(X, T, tag, krn), par, m0)
-    P, par, m0 = _REF_CACHE[name]
+    if name not in _ORACLE:
+        X, T, tag, krn, m0, hdir = workload(name, 0)
+        _ORACLE[name] = (O.Problem(X, T, tag, krn), m0, hdir)
+    P, m0, hdir = _ORACLE[name]
+    hstart, hfinal, hstep, mstep, mfinal = WORKLOADS[name]["sweep"]
+    par = dict(hdir=hdir, hstart=hstart, hfinal=hfinal, hstep=hstep, mstep=mstep, mfinal=mfinal,
+               tol_fun=1e-10, tol_u=1e-10, precond_iter=10, hmag_on=1, m=[0.0, 0.0, 1.0])
     t = time.perf_counter()
-    rows, _ = O.run_loop(P, par, m0=m0, max_steps=n_fs)
-    return len(rows), time.perf_counter() - t
+    _, st = O.run_loop(P, par, m0=m0, max_steps=1)
+    return time.perf_counter() - t, st[0].evals, st[0].pcg_iters
+
+
+def _oracle_job(name):
+    return oracle_step(name)
+
+
+def _cpu_baseline_proc(name, q):
+    """cpu_baseline in a separate (spawned) process, alongside the GPU work."""
+    for k in ("OMP_NUM_THREADS", "OPENBLAS_NUM_THREADS", "MKL_NUM_THREADS"):
+        os.environ[k] = "1"
+    try:
+        dt, ev, pcg = oracle_step(name)
+        q.put({"seconds": dt, "evals": ev, "pcg_iters": pcg})
+    except Exception as e:  # reported, not fatal
+        q.put({"error": repr(e)})
+
+
+def host_cores() -> int:
+    try:
+        return len(os.sched_getaffinity(0))
+    except AttributeError:
+        return os.cpu_count() or 1
 
 
 def run_reference(args, world, rank):
     """The reference's algorithm on the host cores: the oracle port (the reference's own
-    esys-escript/JAX stack is not installable here), every step a bounded sample of the
-    workload.  One sweep is sequential and the port's sparse kernels (scipy.sparse) are
-    single-threaded, so the configured workload -- one sweep -- uses one host core
-    (``--ref-procs 1``, the default); ``--ref-procs N`` (0 = one per usable core) runs N
-    independent replicas of the sample in parallel processes and reports their summed
-    throughput instead."""
+    esys-escript/JAX stack is not installable here), on the same workload and configuration
+    as the GPU arm.  A step is one bounded sample of that workload -- field step 1 of its
+    sweep from the initial state, single-threaded (one sweep is sequential and the port's
+    sparse kernels are single-threaded).  The samples run in P spawned processes at once so
+    the run ends within minutes on the large mesh, whose field step takes tens of seconds
+    here; value = 1 / mean sample time, the rate of one sweep (the concurrent samples share
+    memory bandwidth, so it is if anything low).  Under torchrun rank 0 alone runs."""
     if rank != 0:
         return 0
     import multiprocessing as mp
 
-    n_fs = 4
+    cores = host_cores()
+    avail = None
     try:
-        cores = len(os.sched_getaffinity(0))
-    except AttributeError:
-        cores = os.cpu_count() or 1
-    procs = max(1, cores if args.ref_procs <= 0 else min(cores, args.ref_procs))
+        import psutil
+
+        avail = psutil.virtual_memory().available
+    except Exception:
+        pass
+    per_proc = {"large": 8 << 30, "multigrain": 1 << 30, "single": 1 << 28}[args.workload]
+    procs = max(1, min(8, cores, args.steps + args.warmup,
+                       int(avail // per_proc) if avail else 8))
+    if args.ref_procs > 0:
+        procs = min(procs, args.ref_procs)
     for k in ("OMP_NUM_THREADS", "OPENBLAS_NUM_THREADS", "MKL_NUM_THREADS"):
         os.environ[k] = "1"
-    jobs = [(args.workload, n_fs)] * procs
     with mp.get_context("spawn").Pool(procs) as pool:
-        for _ in range(max(1, args.warmup)):
-            pool.map(_ref_sample, jobs, chunksize=1)
-        tot_t, tot_n = 0.0, 0
-        for _ in range(args.steps):
-            t0 = time.perf_counter()
-            res = pool.map(_ref_sample, jobs, chunksize=1)
-            tot_t += time.perf_counter() - t0
-            tot_n += sum(n for n, _ in res)
-    v = tot_n / tot_t
-    _, _, _, _, _, _, _, desc = workload(args.workload, 0)
-    sample = (f"first {n_fs} field steps of the sweep, NumPy/SciPy oracle, single thread" if procs == 1 else
-              f"first {n_fs} field steps of the sweep per replica, {procs} single-threaded NumPy/SciPy oracle "
-              f"replicas in parallel per step")
+        pool.map(_oracle_job, [args.workload] * max(args.warmup, procs), chunksize=1)
+        t0 = time.perf_counter()
+        res = pool.map(_oracle_job, [args.workload] * args.steps, chunksize=1)
+        wall = time.perf_counter() - t0
+    secs = [r[0] for r in res]
+    v = len(secs) / sum(secs)
+    sample = (f"field step 1 of the sweep from the initial state (u = 0) per step, NumPy/SciPy oracle, "
+              f"single-threaded, {procs} samples at a time in separate processes; value = 1 / mean sample "
+              f"time ({statistics.mean(secs):.1f} s; {res[0][1]} energy evaluations, {res[0][2]} PCG iterations)")
     line = {
         "impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * tot_t / args.steps,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * statistics.mean(secs),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": desc + f"; each step = the first {n_fs} field steps"
-                   + (f", {procs} replicas" if procs > 1 else ""),
-                   "precision": "fp64"},
-        "cpu_baseline": {"value": v, "unit": UNIT, "cores": procs, "kind": "port", "sample": sample},
+        "config": config_of(args.workload, world),
+        "cpu_baseline": {"value": v, "unit": UNIT, "cores": procs, "host_cores": cores, "kind": "port",
+                         "sample": sample},
         "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "wall_s": wall,
     }
     print(json.dumps(line), flush=True)
     return 0
 
 
-def loop_spec(name: str):
-    """The workload's mesh family and sweep as a ``learned.LoopSpec`` (training loops for the
-    learned warm start run on other seeds of the same family)."""
+def run_sweep(M, m0, sweep, sp, window=0, keep=None):
+    """The reference's field loop (scripts/loop.py:71-124: cumulative field, mfinal stop,
+    snapshot counter) one field step per launch, untimed.  Keeps the state (m, u, field)
+    before the steps in ``keep``; with ``keep`` None it locates the switching step (the
+    first whose mh is <= 0) and keeps the ``window`` steps around it.  Returns (rows, step
+    dicts, kept states, first window step)."""
+    hstart, hfinal, hstep, mstep, mfinal = sweep
+    nmax = int(abs(hfinal - hstart) / abs(hstep)) + 1
+    M.set_state(m0, None, m0)
+    rows, steps, states = [], [], {}
+    recent = collections.deque(maxlen=window // 2 + 1) if keep is None else None
+    want = set(keep) if keep is not None else set()
+    j0 = None
+    mh = last = DBL_MAX
+    counter, h = 0, hstart
+    for idx in range(nmax):
+        if not mh > mfinal:
+            break
+        if recent is not None or idx in want:
+            m, u, _ = M.get_state()
+            if idx in want:
+                states[idx] = (m, u, h)
+            if recent is not None:
+                recent.append((idx, m, u, h))
+        r = M.minimize(h, sp)
+        if r["status"] != 0:
+            raise RuntimeError(f"field step {idx} returned status {r['status']}")
+        mh = r["mh"]
+        if (last - mh) > mstep:
+            counter += 1
+            last = mh
+        rows.append([counter, h, mh, r["energy"]])
+        steps.append(r)
+        if recent is not None and mh <= 0.0:  # switching: the window is half before, half after
+            j0 = max(0, idx - window // 2)
+            for j, m, u, hj in recent:
+                if j >= j0:
+                    states[j] = (m, u, hj)
+            want = set(range(idx + 1, j0 + window))
+            recent = None
+        h = h + hstep
+    rows = np.array(rows)
+    if keep is None and j0 is None:  # no switching within the sweep: the last steps
+        raise RuntimeError("the sweep does not switch; no window to time")
+    return rows, steps, states, j0
+
+
+def time_window(M, states, order, sp, m0, flush, warmup, steps, world):
+    """W untimed, then K timed field steps cycling through ``order``, each from its saved
+    state, the L2 flushed before each, device time from CUDA events on the library's stream.
+    Returns (ms over ranks, step dicts)."""
+    import torch
+
+    def one(t, timed):
+        m, u, h = states[order[t % len(order)]]
+        M.set_state(m, u, m0)
+        if timed:
+            flush.fill_(1.0)  # L2 flush (256 MB > 126 MB L2)
+            torch.cuda.synchronize()
+            M.timer_start()
+        r = M.minimize(h, sp)
+        return (M.timer_stop() if timed else 0.0), r
+
+    for t in range(warmup):
+        one(t, False)
+    dist_barrier(world)
+    torch.cuda.synchronize()
+    total, out = 0.0, []
+    for t in range(steps):
+        ms, r = one(t, True)
+        total += ms
+        out.append(r)
+    torch.cuda.synchronize()
+    dist_barrier(world)
+    return dist_max(total, world), out
+
+
+def train_model(name, rank, local):
+    """The learned start's network, trained at set-up (untimed) on plain loops of other seeds
+    of the workload's mesh family."""
     from mammos_mumag import learned
 
-    if name == "large":
-        return learned.LoopSpec(n=80, L=200.0, grains=27, cone_deg=20.0, gb=2.0, hstep=-0.05, tilt_deg=0.0,
-                                max_steps=20)
-    return learned.LoopSpec(n=32, L=80.0, grains=8, cone_deg=15.0, gb=2.0, hstep=-0.1, tilt_deg=1.0)
+    w = WORKLOADS[name]
+    mesh = w["mesh"]
+    hs = w["sweep"]
+    spec = learned.LoopSpec(n=mesh["n"], L=mesh["L"], grains=mesh["grains"], cone_deg=mesh["cone_deg"],
+                            gb=mesh["gb"], hstart=hs[0], hfinal=hs[1], hstep=hs[2], tilt_deg=w["tilt"],
+                            max_steps=w["train_steps"])
+    t0 = time.perf_counter()
+    feats, targets = learned.collect([1000 + 10 * rank + q for q in range(w["train_seeds"])], spec,
+                                     samples=50000, device=local)
+    t1 = time.perf_counter()
+    model, loss = learned.train(feats, targets, epochs=30, device=local)
+    info = {"samples": int(len(targets)), "training_meshes": w["train_seeds"], "collect_s": t1 - t0,
+            "train_s": time.perf_counter() - t1, "loss_rel": loss}
+    return model, info
+
+
+def variant_table(name, gate):
+    """(variant, precision, aggregate nodes, learned gate or None); the first is the plain
+    FP64 path (the reference's method, the denominator)."""
+    from mammos_mumag import _native
+
+    cb = WORKLOADS[name]["coarse"]
+    out = [("fp64", _native.PREC_FP64, 0, None), ("mixed", _native.PREC_MIXED, 0, None),
+           ("mixed_coarse", _native.PREC_MIXED, cb, None)]
+    if WORKLOADS[name]["train_seeds"] > 0:
+        out.append(("learned_mixed_coarse", _native.PREC_MIXED, cb, gate))
+    return out
+
+
+def hc_mr(rows):
+    from mammos_mumag.hysteresis import coercivity_remanence
+
+    return coercivity_remanence(rows)
+
+
+def rel(a, b):
+    return abs(a - b) / abs(b) if np.isfinite(a) and np.isfinite(b) and b != 0 else None
+
+
+def run_b200(args, world, rank, local):
+    import multiprocessing as mp
+
+    import torch
+
+    from mammos_mumag import _native
+
+    if _native.device_count() < 1:
+        raise RuntimeError("no sm_100 GPU visible")
+    torch.cuda.set_device(local)
+    name = args.workload
+    w = WORKLOADS[name]
+    X, T, tag, krn, m0, hdir = workload(name, 0)
+    sp = _native.solver_params(hdir=hdir)
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=f"cuda:{local}")
+    head = headline_of(name)
+    # the CPU oracle's sample, in its own process while the GPU works (rank 0, one GPU)
+    cpu_q = cpu_p = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        ctx = mp.get_context("spawn")
+        cpu_q = ctx.Queue()
+        cpu_p = ctx.Process(target=_cpu_baseline_proc, args=(name, cpu_q), daemon=True)
+        cpu_p.start()
+    model, train_info = (None, None)
+    if w["train_seeds"] > 0:
+        model, train_info = train_model(name, rank, local)
+
+    def make_mesh(prec, cb, gate):
+        msh = _native.Mesh(X, T, tag, krn, device=local, precision=prec, coarse_box_nodes=cb)
+        if gate is not None:
+            msh.set_warm_start(_native.WARM_LEARNED, model)
+            msh.set_learned_gate(gate)
+        msh.set_state(m0, None, m0)
+        msh.autotune(sp)  # launch shape (set-up, untimed)
+        return msh
+
+    variants, runs = {}, {}
+    j0, order = None, None
+    for vname, prec, cb, gate in variant_table(name, args.learned_gate):
+        msh = make_mesh(prec, cb, gate)
+        info = msh.info()
+        keep = None if j0 is None else order
+        rows, steps, states, jw = run_sweep(msh, m0, w["sweep"], sp, window=w["window"], keep=keep)
+        if j0 is None:  # the plain FP64 sweep locates the window
+            j0 = jw
+            order = [j for j in range(j0, j0 + w["window"]) if j in states]
+        clk = ClockSampler(local) if vname == head else None
+        if clk:
+            clk.__enter__()
+        try:
+            ms, tsteps = time_window(msh, states, order, sp, m0, flush, args.warmup, args.steps, world)
+        finally:
+            if clk:
+                clk.__exit__(None, None, None)
+        # the restored steps repeat the sweep's own steps (deterministic kernels: identical energies)
+        restored = max(abs(r["energy"] - rows[order[t % len(order)]][3]) / abs(rows[order[t % len(order)]][3])
+                       for t, r in enumerate(tsteps))
+        hc, mr = hc_mr(rows)
+        ev = sum(s["evals"] for s in tsteps)
+        sev = sum(s["evals"] for s in steps)
+        variants[vname] = {
+            "value": len(tsteps) * world / (ms * 1e-3),
+            "pcg_iters_per_solve": sum(s["pcg_iters"] for s in tsteps) / max(1, ev),
+            "sweep_value": len(steps) / (1e-3 * sum(s["device_ms"] for s in steps)),
+            "sweep_pcg_iters_per_solve": sum(s["pcg_iters"] for s in steps) / max(1, sev),
+            "sweep_steps": len(steps),
+            "hc_T": hc, "mr_T": mr,
+            "learned_starts_per_solve": (sum(s["learned_starts"] for s in steps) / max(1, sev)
+                                         if gate is not None else None),
+            "learned_gate": gate,
+            "grid_ctas": info["grid_ctas"], "kernel_ctas_per_sm": info["kernel_ctas_per_sm"],
+            "pcg_variant": info["pcg_variant"], "coarse_boxes": info["coarse_boxes"],
+            "restored_energy_dev": restored,
+        }
+        runs[vname] = dict(ms=ms, tsteps=tsteps, steps=steps, rows=rows, info=info, clk=clk, states=states,
+                           prec=prec, cb=cb, gate=gate)
+        if vname == head and gate is not None:
+            # the same window with the learned start on every solve (no gate), on this path's states
+            msh.set_learned_gate(0.0)
+            ms_u, ts_u = time_window(msh, states, order, sp, m0, flush, args.warmup, args.steps, world)
+            evu = sum(s["evals"] for s in ts_u)
+            variants[vname + "_ungated"] = {
+                "value": len(ts_u) * world / (ms_u * 1e-3),
+                "pcg_iters_per_solve": sum(s["pcg_iters"] for s in ts_u) / max(1, evu),
+                "learned_starts_per_solve": sum(s["learned_starts"] for s in ts_u) / max(1, evu),
+                "note": "window only, from the gated path's saved states",
+            }
+        msh.close()
+    return finish_b200(args, world, rank, local, name, variants, runs, head, j0, order, model, train_info,
+                       cpu_q, cpu_p, sp, m0, X, T, tag, krn, flush)
 
 
 def run_batch(args, world, rank, local):
@@ -385,109 +635,38 @@ def run_batch(args, world, rank, local):
     return 0
 
 
-def run_b200(args, world, rank, local):
+def finish_b200(args, world, rank, local, name, variants, runs, head, j0, order, model, train_info, cpu_q, cpu_p,
+                sp, m0, X, T, tag, krn, flush):
     import torch
 
-    from mammos_mumag import _native, learned
+    from mammos_mumag import _native
 
-    if _native.device_count() < 1:
-        raise RuntimeError("no sm_100 GPU visible")
-    torch.cuda.set_device(local)
-    X, T, tag, krn, m0, hdir, sweep, desc = workload(args.workload, seed=rank)
-    sp = _native.solver_params(hdir=hdir)
-    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=f"cuda:{local}")
-    nfs_expected = int(abs(sweep["hfinal"] - sweep["hstart"]) / abs(sweep["hstep"])) + 1
-    if sweep.get("max_steps"):
-        nfs_expected = min(nfs_expected, sweep["max_steps"])
-    sw = (sweep["hstart"], sweep["hfinal"], sweep["hstep"], sweep["mstep"], sweep["mfinal"])
-    mx = sweep.get("max_steps", 0)
-    use_learned = args.workload != "single" and not args.no_learned
-    headline = "learned_mixed" if use_learned else "fp64"
-
-    # the learned warm start's network: trained once at set-up (untimed) on plain loops of
-    # other seeds of the workload's mesh family
-    model, train_info = None, None
-    if use_learned:
-        spec = loop_spec(args.workload)
-        nseed = 2 if args.workload == "large" else 4
-        t0 = time.perf_counter()
-        feats, targets = learned.collect([1000 + 10 * rank + q for q in range(nseed)], spec, samples=50000,
-                                         device=local)
-        t1 = time.perf_counter()
-        model, loss = learned.train(feats, targets, epochs=30, device=local)
-        train_info = {"samples": int(len(targets)), "training_meshes": nseed, "collect_s": t1 - t0,
-                      "train_s": time.perf_counter() - t1, "loss_rel": loss}
-
-    def make_mesh(prec, warm):
-        msh = _native.Mesh(X, T, tag, krn, device=local, precision=prec)
-        if warm == _native.WARM_LEARNED:
-            msh.set_warm_start(warm, model)
-        msh.set_state(m0, None, m0)
-        msh.autotune(sp)  # launch shape (set-up, untimed)
-        return msh
-
-    def timed(msh, clk_index=None):
-        """W untimed sweeps, then K sweeps timed with CUDA events on the library's stream,
-        the L2 flushed before each.  Returns (ms over ranks, field steps, step dicts, rows)."""
-        for _ in range(args.warmup):
-            msh.set_state(m0, None, m0)
-            msh.loop(*sw, sp, max_steps=mx)
-        total_ms, nfs, steps_all, rows = 0.0, 0, [], None
-        dist_barrier(world)
-        torch.cuda.synchronize()
-        for _ in range(args.steps):
-            flush.fill_(1.0)  # L2 flush between timed sweeps (256 MB > 126 MB L2)
-            torch.cuda.synchronize()
-            msh.set_state(m0, None, m0)
-            msh.timer_start()
-            rows, steps = msh.loop(*sw, sp, max_steps=mx)
-            total_ms += msh.timer_stop()
-            nfs += len(rows)
-            steps_all += steps
-        torch.cuda.synchronize()
-        dist_barrier(world)
-        return dist_max(total_ms, world), nfs, steps_all, rows
-
-    paths = {"fp64": (_native.PREC_FP64, _native.WARM_PREVIOUS)}
-    if not args.no_mixed:
-        paths["mixed"] = (_native.PREC_MIXED, _native.WARM_PREVIOUS)
-    if use_learned:
-        paths["learned_mixed"] = (_native.PREC_MIXED, _native.WARM_LEARNED)
-    variants, raw = {}, {}
-    clk = None
-    for name, (prec, warm) in paths.items():
-        msh = make_mesh(prec, warm)
-        info = msh.info()
-        if name == headline:
-            with ClockSampler(local) as clk:
-                res = timed(msh)
-        else:
-            res = timed(msh)
-        msh.close()
-        t_ms, nfs, st, rows = res
-        evals = sum(x["evals"] for x in st)
-        hc, mr = hc_mr(rows)
-        raw[name] = (t_ms, nfs, st, rows, info)
-        variants[name] = {"value": nfs * world / (t_ms * 1e-3),
-                          "pcg_iters_per_solve": sum(x["pcg_iters"] for x in st) / max(1, evals),
-                          "hc_T": hc, "mr_T": mr, "grid_ctas": info["grid_ctas"], "pcg_variant": info["pcg_variant"]}
+    w = WORKLOADS[name]
     ref = variants["fp64"]
-    for name, v in variants.items():
-        if name == "fp64":
+    oracle_hc = oracle_mr = None
+    if w["oracle"]:
+        f = np.load(ROOT / "tests" / "golden" / w["oracle"])
+        oracle_hc, oracle_mr = float(f["hc"]), float(f["mr"])
+    for vname, v in variants.items():
+        if vname != "fp64":
+            v["speedup_vs_fp64"] = v["value"] / ref["value"]
+            v["pcg_per_solve_vs_fp64"] = v["pcg_iters_per_solve"] / ref["pcg_iters_per_solve"]
+        if "hc_T" not in v:
             continue
-        v["speedup_vs_fp64"] = v["value"] / ref["value"]
-        v["pcg_per_solve_vs_fp64"] = v["pcg_iters_per_solve"] / ref["pcg_iters_per_solve"]
-        v["dHc_rel"] = (abs(v["hc_T"] - ref["hc_T"]) / ref["hc_T"]
-                        if np.isfinite(ref["hc_T"]) and np.isfinite(v["hc_T"]) else None)
-        v["dMr_rel"] = (abs(v["mr_T"] - ref["mr_T"]) / abs(ref["mr_T"])
-                        if np.isfinite(ref["mr_T"]) and np.isfinite(v["mr_T"]) else None)
-    t_max, nfs, steps_all, rows, info = raw[headline]
-    value = variants[headline]["value"]
-    launches = len(steps_all)
-    kernel_ms = sum(st["device_ms"] for st in steps_all)
-    Z, N = info["nnz"], info["nodes"]
-    s_pcg = 4 if headline != "fp64" else 8
-    ab = algorithmic_bytes(steps_all, Z, N, s_pcg=s_pcg)
+        if vname != "fp64":
+            v["sweep_speedup_vs_fp64"] = v["sweep_value"] / ref["sweep_value"]
+            v["dHc_rel"] = rel(v["hc_T"], ref["hc_T"])
+            v["dMr_rel"] = rel(v["mr_T"], ref["mr_T"])
+        if oracle_hc is not None:
+            v["dHc_rel_oracle"] = rel(v["hc_T"], oracle_hc)
+            v["dMr_rel_oracle"] = rel(v["mr_T"], oracle_mr)
+    hr = runs[head]
+    value = variants[head]["value"]
+    tsteps = hr["tsteps"]
+    launches = len(tsteps)
+    kernel_ms = sum(s["device_ms"] for s in tsteps)
+    Z, N = hr["info"]["nnz"], hr["info"]["nodes"]
+    ab = algorithmic_bytes(tsteps, Z, N, mixed=hr["prec"] == _native.PREC_MIXED, coarse=hr["cb"] > 0)
     achieved = ab / (kernel_ms * 1e-3) / 1e9  # GB/s over the kernel's own launch durations
     peaks = {}
     try:
@@ -495,72 +674,79 @@ def run_b200(args, world, rank, local):
     except Exception:
         pass
     peak = float(peaks.get("hbm_gbs", 6650.0))
-    ratio = TRAFFIC_PER_ALGORITHMIC_BYTE.get((args.workload, headline))
+    ratio = TRAFFIC_PER_ALGORITHMIC_BYTE.get((name, head))
     traffic = ratio * ab / launches if ratio is not None else None
-    prec_h, warm_h = paths[headline]
-    # e2e: the public API from host buffers (pinned), every step: mesh build + upload,
-    # warm-start set-up, state upload, sweep, result read-back
-    pin = {k: torch.from_numpy(np.ascontiguousarray(v)).pin_memory() for k, v in
-           (("X", X), ("T", np.asarray(T, np.int32)), ("tag", np.asarray(tag, np.int32)), ("m0", m0))}
-    h2d = sum(t.numel() * t.element_size() for t in pin.values()) + 48 * len(krn)
-    e2e_t, e2e_n = 0.0, 0
-    for _ in range(args.steps):
-        torch.cuda.synchronize()
-        t0 = time.perf_counter()
-        with _native.Mesh(pin["X"].numpy(), pin["T"].numpy(), pin["tag"].numpy(), krn, device=local,
-                          precision=prec_h) as mm:
-            if warm_h == _native.WARM_LEARNED:
-                mm.set_warm_start(warm_h, model)
-            mm.set_state(pin["m0"].numpy(), None, pin["m0"].numpy())
-            mm.autotune(sp)  # cached for this mesh shape: no timing runs after the first
-            r2, _ = mm.loop(*sw, sp, max_steps=mx)
-            mfin, _, _ = mm.get_state()
-        e2e_t += time.perf_counter() - t0
-        e2e_n += len(r2)
-    d2h = 32 * nfs_expected + mfin.nbytes
+    # e2e: the public API from pinned host buffers -- the mesh built once (the preprocessing
+    # cache hits: X, T, tag are hashed and compared), then per step the state uploaded, the
+    # field step run and the state read back
+    pin = lambda a: torch.from_numpy(np.ascontiguousarray(a)).pin_memory().numpy()  # noqa: E731
+    pX, pT, ptag, pm0 = pin(X), pin(np.asarray(T, np.int32)), pin(np.asarray(tag, np.int32)), pin(m0)
+    pstates = {j: (pin(m), pin(u), h) for j, (m, u, h) in hr["states"].items()}
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    with _native.Mesh(pX, pT, ptag, krn, device=local, precision=hr["prec"], coarse_box_nodes=hr["cb"]) as mm:
+        if hr["gate"] is not None:
+            mm.set_warm_start(_native.WARM_LEARNED, model)
+            mm.set_learned_gate(hr["gate"])
+        mm.set_state(pm0, None, pm0)
+        mm.autotune(sp)  # cached for this mesh shape: no timing runs
+        for t in range(args.steps):
+            m, u, h = pstates[order[t % len(order)]]
+            mm.set_state(m, u, pm0)
+            mm.minimize(h, sp)
+            mout, uout, gout = mm.get_state()
+    e2e_t = time.perf_counter() - t0
     e2e_t = dist_max(e2e_t, world)
-    if rank == 0:
-        cpu = None
-        if world == 1 and args.workload != "large":
-            v, dt, n = cpu_sample(args.workload, 12)
-            cpu = {"value": v, "unit": UNIT, "cores": 1, "kind": "port",
-                   "sample": f"first {n} field steps of the sweep ({dt:.1f} s), NumPy/SciPy oracle, single thread"}
-        evals = sum(st["evals"] for st in steps_all)
-        pcg = sum(st["pcg_iters"] for st in steps_all)
-        line = {
-            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": t_max / args.steps, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f64" if headline == "fp64" else "f32+f64",
-            "data": "synthetic",
-            "config": {"workload": desc, "path": headline,
-                       "precision": "fp64" if prec_h == _native.PREC_FP64 else
-                       "mixed (FP32 operator planes and inner PCG, FP64 refinement, reductions, energies)",
-                       "warm_start": "learned" if warm_h == _native.WARM_LEARNED else "previous u (reference)",
-                       "parallelism": f"replicas x{world}",
-                       "l2": "256 MB buffer written between timed sweeps (L2 flush)",
-                       "grid_ctas": info["grid_ctas"], "block_threads": info["block_threads"],
-                       "pcg_variant": info["pcg_variant"]},
-            "pcg_iters_per_solve": pcg / max(1, evals),
-            "variants": variants,
-            "learned_training": train_info,
-            "field_steps_per_sweep": nfs // args.steps,
-            "hc_T": variants[headline]["hc_T"], "mr_T": variants[headline]["mr_T"],
-            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                         "frac": achieved / peak, "traffic": traffic,
-                         "traffic_source": ("DRAM bytes per algorithmic byte of one ncu-captured field-step "
-                                            "launch of this path, scaled to the average launch")
-                         if traffic is not None else None,
-                         "kernel": f"k_solve (persistent field step, {headline})",
-                         "algorithmic_bytes_per_launch": ab / launches,
-                         "avg_launch_ms": kernel_ms / launches,
-                         "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)" if peaks else "fallback"},
-            "cpu_baseline": cpu,
-            "e2e": {"value": e2e_n * world / e2e_t, "unit": UNIT, "h2d_bytes_per_step": int(h2d),
-                    "d2h_bytes_per_step": int(d2h)},
-            "gpu_launches": launches,
-            "clocks": clk.summary() if clk is not None else None,
-        }
-        print(json.dumps(line), flush=True)
+    h2d = 8 * (3 * N + N + 3 * N) + (pX.nbytes + pT.nbytes + ptag.nbytes + 48 * len(krn)) / args.steps
+    d2h = 8 * (3 * N + N + 3 * N) + 128
+    if rank != 0:
+        return 0
+    cpu = None
+    if cpu_p is not None:
+        cpu_p.join(timeout=1800)
+        res = cpu_q.get(timeout=5) if not cpu_q.empty() else {"error": "no result"}
+        if "seconds" in res:
+            same = {k: 1e3 / runs[k]["steps"][0]["device_ms"] for k in ("fp64", head)}
+            cpu = {"value": 1.0 / res["seconds"], "unit": UNIT, "cores": 1, "host_cores": host_cores(), "kind": "port",
+                   "sample": (f"field step 1 of the sweep from the initial state (u = 0), NumPy/SciPy oracle, "
+                              f"single thread, {res['seconds']:.1f} s ({res['evals']} energy evaluations, "
+                              f"{res['pcg_iters']} PCG iterations), run in a separate process during the GPU work"),
+                   "gpu_same_sample": {k: {"value": v, "ratio_to_cpu": v * res["seconds"]} for k, v in same.items()}}
+        else:
+            cpu = {"value": None, "unit": UNIT, "cores": 1, "kind": "port", "error": res.get("error")}
+    clk = hr["clk"]
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": hr["ms"] / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic",
+        "config": config_of(name, world),
+        "window": {"first_step": j0, "steps": len(order),
+                   "fields_T": [hr["states"][order[0]][2], hr["states"][order[-1]][2]],
+                   "located_by": "the plain FP64 sweep's first field step with mh <= 0, half the window before it"},
+        "pcg_iters_per_solve": variants[head]["pcg_iters_per_solve"],
+        "speedup_vs_fp64": variants[head]["speedup_vs_fp64"],
+        "hc_T": variants[head]["hc_T"], "mr_T": variants[head]["mr_T"],
+        "dHc_rel": variants[head].get("dHc_rel"), "dMr_rel": variants[head].get("dMr_rel"),
+        "variants": variants,
+        "learned_training": train_info,
+        "launch": {"grid_ctas": hr["info"]["grid_ctas"], "block_threads": hr["info"]["block_threads"],
+                   "kernel_ctas_per_sm": hr["info"]["kernel_ctas_per_sm"]},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "traffic": traffic,
+                     "traffic_source": ("DRAM bytes per algorithmic byte of one ncu-captured field-step launch of "
+                                        "this path, scaled to the average launch") if traffic is not None else None,
+                     "kernel": f"k_solve (persistent field step, {head})",
+                     "algorithmic_bytes_per_launch": ab / launches, "avg_launch_ms": kernel_ms / launches,
+                     "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)" if peaks else "fallback"},
+        "cpu_baseline": cpu,
+        "e2e": {"value": args.steps * world / e2e_t, "unit": UNIT, "h2d_bytes_per_step": int(h2d),
+                "d2h_bytes_per_step": int(d2h),
+                "includes": "mesh build (preprocessing-cache hit) once, then per step state upload, field step, "
+                            "state read-back"},
+        "gpu_launches": launches,
+        "clocks": clk.summary() if clk is not None else None,
+    }
+    print(json.dumps(line), flush=True)
     if model is not None:
         model.close()
     return 0
@@ -569,20 +755,22 @@ def run_b200(args, world, rank, local):
 def main():
     ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=3)
-    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
-    ap.add_argument("--workload", choices=["multigrain", "single", "large", "batch"], default="multigrain")
-    ap.add_argument("--no-mixed", action="store_true", help="skip the mixed-precision variant")
-    ap.add_argument("--ref-procs", type=int, default=1,
-                    help="reference arm: independent replica processes (0: one per usable host core); the "
-                         "default 1 times the workload as configured, one sweep")
-    ap.add_argument("--no-learned", action="store_true",
-                    help="skip the learned warm start (headline = the plain FP64 path)")
+    ap.add_argument("--workload", choices=["large", "multigrain", "single", "batch"], default="large")
+    ap.add_argument("--learned-gate", type=float, default=1e8,
+                    help="the learned start runs only on solves whose initial residual exceeds this many "
+                         "times the stop tolerance (0: every solve)")
+    ap.add_argument("--ref-procs", type=int, default=0,
+                    help="reference arm: at most this many concurrent sample processes (0: up to 8)")
+    ap.add_argument("--no-cpu", action="store_true", help="skip the cpu_baseline sample")
     args = ap.parse_args()
     world, rank, local = dist_setup()
     try:
         if args.impl == "reference":
+            if args.workload == "batch":
+                raise SystemExit("the reference arm times the single-sweep workloads")
             return run_reference(args, world, rank)
         if args.workload == "batch":
             return run_batch(args, world, rank, local)
