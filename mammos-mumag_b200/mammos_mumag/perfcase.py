@@ -2,7 +2,7 @@
 
     python -m mammos_mumag.perfcase field-step [--workload multigrain|large] [--precision fp64|mixed]
                                                [--grid N] [--ctas-per-sm 2|3] [--pcg-variant 1|2]
-                                               [--learned]
+                                               [--coarse BOX_NODES] [--learned]
     python -m mammos_mumag.perfcase mlp-train [--samples N] [--epochs E]
     python -m mammos_mumag.perfcase mlp-predict [--rows N]
 
@@ -58,7 +58,7 @@ def field_step(args) -> int:
         feats, targets = learned.collect([1], spec, samples=20000, evals_per_step=10)
         model, _ = learned.train(feats, targets, epochs=5)
     with _native.Mesh(X, T, tag, krn, precision=prec, grid_ctas=args.grid, ctas_per_sm=args.ctas_per_sm,
-                      pcg_variant=args.pcg_variant) as M:
+                      pcg_variant=args.pcg_variant, coarse_box_nodes=args.coarse) as M:
         if model is not None:
             M.set_warm_start(_native.WARM_LEARNED, model)
         M.set_state(m0, None, m0)
@@ -69,6 +69,7 @@ def field_step(args) -> int:
           f"(build {info['kernel_ctas_per_sm']} CTAs/SM, PCG arrangement {info['pcg_variant']}): "
           f"{r['device_ms']:.3f} ms, PCG iterations {r['pcg_iters']}, evaluations {r['evals']}, "
           f"M_inv iterations {r['minv_iters']}, NCG iterations {r['ncg_iters']}"
+          + (f", two-level preconditioner ({info['coarse_boxes']} boxes)" if info["coarse_boxes"] else "")
           + (", learned warm start" if model is not None else ""))
     if model is not None:
         model.close()
@@ -105,6 +106,8 @@ def main(argv=None) -> int:
     fs.add_argument("--grid", type=int, default=0, help="CTAs (0: the size-based default)")
     fs.add_argument("--ctas-per-sm", type=int, choices=[0, 2, 3], default=0)
     fs.add_argument("--pcg-variant", type=int, choices=[0, 1, 2], default=0)
+    fs.add_argument("--coarse", type=int, default=0,
+                    help="two-level Poisson preconditioner with boxes of about this many nodes (0: Jacobi)")
     fs.add_argument("--learned", action="store_true", help="learned warm start (trains a network first)")
     mt = sub.add_parser("mlp-train")
     mt.add_argument("--samples", type=int, default=16384)
