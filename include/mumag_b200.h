@@ -206,6 +206,16 @@ mm_status mm_set_state(mm_mesh* mesh, const double* m, const double* u, const do
 /* Read the state back; any pointer may be NULL. gfull [3N] is the last full gradient. */
 mm_status mm_get_state(mm_mesh* mesh, double* m, double* u, double* gfull);
 
+/* Device-resident forms of mm_set_state / mm_get_state: the same arrays and layouts
+ * (interleaved m [3N] and mbar [3N], u [N], gfull [3N], mesh-file order), but as pointers to
+ * memory on the mesh's device, so a caller whose state already lives on the GPU (as the
+ * reference's total_eg takes JAX device arrays, scripts/energies.py:67-99) avoids the host
+ * round trip.  The permutation to the device layout runs on the mesh's stream; both calls
+ * return when it has finished.  A non-finite input is refused with MM_BAD_INPUT (the state
+ * is then undefined: set it again). */
+mm_status mm_set_state_device(mm_mesh* mesh, const double* m, const double* u, const double* mbar);
+mm_status mm_get_state_device(mm_mesh* mesh, double* m, double* u, double* gfull);
+
 /* One energy + gradient evaluation, total_eg (scripts/energies.py:67-99), at the state's
  * m with the state's u as PCG warm start; u and gfull in the state are updated.
  * Outputs (NULL allowed): *energy, gproj [3N] = m x (g x m), *pcg_iters. */

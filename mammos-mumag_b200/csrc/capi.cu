@@ -79,6 +79,45 @@ void d2h(std::vector<double>& h, const double* d, size_t n, cudaStream_t st) {
   MM_CK(cudaStreamSynchronize(st));
 }
 
+// Device-resident state transfers: the reference's layout (interleaved m [3N], u [N], mesh-file
+// order) to the device layout (component planes, device row order) and back, one thread per
+// node.  A non-finite input value raises *bad (the host form refuses it the same way).
+__global__ void k_state_in(const double* __restrict__ m, const double* __restrict__ u,
+                           const double* __restrict__ mb, const int32_t* __restrict__ iperm, int64_t N, int64_t np,
+                           double* x, double* ud, double* mbd, int* bad) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < N; i += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t j = iperm[i];
+    for (int q = 0; q < 3; ++q) {
+      const double v = m[3 * i + q], w = mb ? mb[3 * i + q] : v;
+      if (!isfinite(v) || !isfinite(w)) *bad = 1;
+      x[q * np + j] = v;
+      mbd[q * np + j] = w;
+    }
+    const double uv = u ? u[i] : 0.0;
+    if (!isfinite(uv)) *bad = 1;
+    ud[j] = uv;
+  }
+}
+__global__ void k_state_out(const double* __restrict__ x, const double* __restrict__ ud,
+                            const double* __restrict__ gf, const int32_t* __restrict__ iperm, int64_t N, int64_t np,
+                            double* m, double* u, double* g) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < N; i += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t j = iperm[i];
+    for (int q = 0; q < 3; ++q) {
+      if (m) m[3 * i + q] = x[q * np + j];
+      if (g) g[3 * i + q] = gf[q * np + j];
+    }
+    if (u) u[i] = ud[j];
+  }
+}
+
+void ensure_iperm(DevMesh& m) {
+  if (m.d_iperm) return;
+  dalloc(m.d_iperm, m.h.N);
+  dalloc(m.d_bad, 1);
+  upload(m.d_iperm, m.h.iperm, m.stream);
+}
+
 void release(DevMesh& m) {
   if (m.device >= 0) cudaSetDevice(m.device);
   dfree(m.sl_off);
@@ -117,6 +156,8 @@ void release(DevMesh& m) {
   dfree(m.bslots);
   dfree(m.bslot);
   dfree(m.ctabox);
+  dfree(m.d_iperm);
+  dfree(m.d_bad);
   if (m.h_resd) cudaFreeHost(m.h_resd);
   if (m.h_resi) cudaFreeHost(m.h_resi);
   if (m.h_flags) cudaFreeHost(m.h_flags);
@@ -646,6 +687,43 @@ mm_status mm_set_state(mm_mesh* mesh, const double* mv, const double* uv, const 
   }
   MM_CK(cudaMemcpyAsync(m.u, tu.data(), sizeof(double) * np, cudaMemcpyHostToDevice, m.stream));
   MM_CK(cudaMemsetAsync(m.gf, 0, sizeof(double) * 3 * np, m.stream));
+  MM_CK(cudaStreamSynchronize(m.stream));
+  return MM_OK;
+  API_END
+}
+
+mm_status mm_set_state_device(mm_mesh* mesh, const double* mv, const double* uv, const double* mbar) {
+  API_BEGIN
+  check_mesh(mesh);
+  if (!mv) throw std::runtime_error("m is NULL");
+  DevMesh& m = mesh->dm;
+  const size_t np = m.h.Npad;
+  MM_CK(cudaSetDevice(m.device));
+  ensure_iperm(m);
+  MM_CK(cudaMemsetAsync(m.x, 0, sizeof(double) * 3 * np, m.stream));
+  MM_CK(cudaMemsetAsync(m.mbar, 0, sizeof(double) * 3 * np, m.stream));
+  MM_CK(cudaMemsetAsync(m.u, 0, sizeof(double) * np, m.stream));
+  MM_CK(cudaMemsetAsync(m.gf, 0, sizeof(double) * 3 * np, m.stream));
+  MM_CK(cudaMemsetAsync(m.d_bad, 0, sizeof(int), m.stream));
+  const int grid = (int)std::min<int64_t>((m.h.N + 255) / 256, 1184);
+  k_state_in<<<grid, 256, 0, m.stream>>>(mv, uv, mbar, m.d_iperm, m.h.N, (int64_t)np, m.x, m.u, m.mbar, m.d_bad);
+  MM_CK(cudaGetLastError());
+  MM_CK(cudaMemcpyAsync(m.h_flags, m.d_bad, sizeof(int), cudaMemcpyDeviceToHost, m.stream));
+  MM_CK(cudaStreamSynchronize(m.stream));
+  if (m.h_flags[0]) throw std::runtime_error("non-finite magnetisation or potential");
+  return MM_OK;
+  API_END
+}
+
+mm_status mm_get_state_device(mm_mesh* mesh, double* mv, double* uv, double* gfull) {
+  API_BEGIN
+  check_mesh(mesh);
+  DevMesh& m = mesh->dm;
+  MM_CK(cudaSetDevice(m.device));
+  ensure_iperm(m);
+  const int grid = (int)std::min<int64_t>((m.h.N + 255) / 256, 1184);
+  k_state_out<<<grid, 256, 0, m.stream>>>(m.x, m.u, m.gf, m.d_iperm, m.h.N, (int64_t)m.h.Npad, mv, uv, gfull);
+  MM_CK(cudaGetLastError());
   MM_CK(cudaStreamSynchronize(m.stream));
   return MM_OK;
   API_END

@@ -212,6 +212,8 @@ struct DevMesh {
   double* bslots = nullptr;
   int32_t* bslot = nullptr;
   int32_t* ctabox = nullptr;
+  int32_t* d_iperm = nullptr;  // iperm on the device (device-resident state transfers)
+  int* d_bad = nullptr;
   int co_off = -1;
   int co_rows = 0;
 };

@@ -988,6 +988,10 @@ __device__ __forceinline__ Rows rows_of(const Ctx& c) {
     const int w_ = (r).sw[s_ - (r).s0];                                  \
     (void)loff_;
 
+// Entries a row gather fetches per round trip in the two-level solves: a whole row of the
+// structured meshes (about 15 entries) at once, since these iterations are latency-bound.
+constexpr int kChunkCoarse = 16;
+
 // gather_row over the staged pattern given by its column array
 template <class VT, class ZT, class AT, int CH>
 __device__ __forceinline__ AT gather_row_r(const int32_t* scol, const VT* sval, int64_t loff, int w, const ZT* z) {
@@ -1291,7 +1295,7 @@ __device__ __noinline__ bool pcg_solve_coarse(Ctx& c, const double* x) {
   {  // w0 = S z0, delta = w0.z0, box sums of w0
     double pd = 0;
     FOR_ROWS_R(rw)
-    const double acc = gather_row_r<double, double, double, 8>(rw.scol, rw.sS, loff_, w_, z);
+    const double acc = gather_row_r<double, double, double, kChunkCoarse>(rw.scol, rw.sS, loff_, w_, z);
     rec_store_w(a.rec[0], i, n, acc);
     pd += acc * z[i];
     coarse_slice_sum(rw, s_ - rw.s0, acc);
@@ -1322,7 +1326,7 @@ __device__ __noinline__ bool pcg_solve_coarse(Ctx& c, const double* x) {
     END_ROWS
     CHECK(grid_barrier(c.sy));
     FOR_ROWS_R(rw)
-    const double acc = gather_row_r<double, double, double, 8>(rw.scol, rw.sS, loff_, w_, z);
+    const double acc = gather_row_r<double, double, double, kChunkCoarse>(rw.scol, rw.sS, loff_, w_, z);
     rec_store_w(a.rec[0], i, n, acc);
     pd += acc * z[i];
     coarse_slice_sum(rw, s_ - rw.s0, acc);
@@ -1422,7 +1426,7 @@ __device__ __noinline__ bool pcg_solve_mixed_coarse(Ctx& c, const double* x) {
     {  // w0 = S32 z0, delta = w0.z0, box sums of w0
       double pd = 0;
       FOR_ROWS_R(rw)
-      const float acc = gather_row_r<float, float, float, kChunk32>(rw.scol, rw.sS32, loff_, w_, z);
+      const float acc = gather_row_r<float, float, float, kChunkCoarse>(rw.scol, rw.sS32, loff_, w_, z);
       rc[i].w = acc;
       pd += (double)acc * (double)z[i];
       coarse_slice_sum(rw, s_ - rw.s0, (double)acc);
@@ -1434,6 +1438,7 @@ __device__ __noinline__ bool pcg_solve_mixed_coarse(Ctx& c, const double* x) {
     double alpha = gamma / delta, beta = 0.0;
     coarse_update(c, false, alpha, beta);
     for (;;) {
+      if (c.sy.timing && threadIdx.x == 0) c.t_phase_start = globaltimer();
       const float af = (float)alpha, bf = (float)beta;
       double pg = 0, pd = 0, pr2 = 0;
       FOR_ROWS_R(rw)
@@ -1452,12 +1457,13 @@ __device__ __noinline__ bool pcg_solve_mixed_coarse(Ctx& c, const double* x) {
       END_ROWS
       CHECK(grid_barrier(c.sy));
       FOR_ROWS_R(rw)
-      const float acc = gather_row_r<float, float, float, kChunk32>(rw.scol, rw.sS32, loff_, w_, z);
+      const float acc = gather_row_r<float, float, float, kChunkCoarse>(rw.scol, rw.sS32, loff_, w_, z);
       rc[i].w = acc;
       pd += (double)acc * (double)z[i];
       coarse_slice_sum(rw, s_ - rw.s0, (double)acc);
       END_ROWS
       double v[3] = {pg, pd, pr2};
+      if (c.sy.timing && threadIdx.x == 0) c.t_pcg_phase += globaltimer() - c.t_phase_start;
       CHECK(grid_reduce_coarse<3>(c, v));
       ++k;
       if (!(v[2] > inner_tol2 && k < a.max_pcg)) break;

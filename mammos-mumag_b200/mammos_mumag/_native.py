@@ -75,6 +75,8 @@ EXPORTED = (
     "mm_debug_stall_barriers",
     "mm_mesh_get_coarse",
     "mm_mesh_set_learned_gate",
+    "mm_set_state_device",
+    "mm_get_state_device",
 )
 WARM_PREVIOUS, WARM_ZERO, WARM_LEARNED = 0, 1, 2
 MLP_FEATURES = 16
@@ -258,6 +260,8 @@ def load():
         "mm_debug_stall_barriers": (C.c_int, [C.c_void_p, C.c_int32]),
         "mm_mesh_get_coarse": (C.c_int, [C.c_void_p, _I32, _I32]),
         "mm_mesh_set_learned_gate": (C.c_int, [C.c_void_p, C.c_double]),
+        "mm_set_state_device": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
+        "mm_get_state_device": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -493,6 +497,17 @@ class Mesh:
         if m.size != 3 * self.N or (u is not None and u.size != self.N) or (mbar is not None and mbar.size != 3 * self.N):
             raise ValueError("state arrays have the wrong size")
         check(load().mm_set_state(self._h, _dp(m), _dp(u), _dp(mbar)))
+
+    def set_state_device(self, m_ptr: int, u_ptr: int = 0, mbar_ptr: int = 0):
+        """``set_state`` from device memory: pointers (integers, 0 = NULL) to float64 arrays on
+        the mesh's device in the reference's layout (m, mbar [3N] interleaved, u [N])."""
+        check(load().mm_set_state_device(self._h, C.c_void_p(m_ptr or None), C.c_void_p(u_ptr or None),
+                                         C.c_void_p(mbar_ptr or None)))
+
+    def get_state_device(self, m_ptr: int = 0, u_ptr: int = 0, g_ptr: int = 0):
+        """``get_state`` into device memory (pointers as in ``set_state_device``; 0 = skip)."""
+        check(load().mm_get_state_device(self._h, C.c_void_p(m_ptr or None), C.c_void_p(u_ptr or None),
+                                         C.c_void_p(g_ptr or None)))
 
     def get_state(self):
         m = np.empty(3 * self.N)
