@@ -1,15 +1,11 @@
 // Training and stand-alone inference of the warm-start MLP (mlp.cuh), plus its C ABI.
 //
 // One training step on a batch of B samples (B a multiple of 16):
-//   k_fwd    per warp, 16 samples: normalised features -> three GELU layers (pre-activations
-//            Z kept in FP32, activations stored transposed in BF16 for the weight gradients)
-//            -> head y; loss 1/B sum (y - t/out_scale)^2 and dL/dy
-//   k_bwd    per warp, 16 samples: dZ3 = dy w4 . gelu'(Z3), dZ2 = (dZ3 W3) . gelu'(Z2),
-//            dZ1 = (dZ2 W2) . gelu'(Z1) on the tensor cores (B operands W^T), dZ stored
-//            transposed in BF16; dw4, db4 by warp reductions
-//   k_wgrad  dW = dZ^T H on the tensor cores (K = the batch), one 16x8 tile per warp
-//   k_bsum   db = column sums of dZ
-//   k_adam   Adam on FP32 master weights, then BF16 copies and transposes
+//   k_train_tc  the gradient on the 5th-generation tensor cores (mlp_train_tc.cuh): one CTA
+//               per 128-row tile, forward with the pre-activations kept in TMEM, backward
+//               products dZ W and weight gradients dZ^T H as tcgen05 MMAs, loss
+//               1/B sum (y - t/out_scale)^2
+//   k_adam      Adam on FP32 master weights, then BF16 copies and transposes (k_publish)
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
@@ -24,6 +20,7 @@
 
 #include "device_mesh.h"
 #include "mlp.cuh"
+#include "mlp_train_tc.cuh"
 #include "umma.cuh"
 
 namespace mumag {
@@ -39,194 +36,12 @@ constexpr int kOffW4 = kOffB3 + kMlpHidden;                 // [128]
 constexpr int kOffB4 = kOffW4 + kMlpHidden;                 // [1]
 constexpr int kNumParams = kOffB4 + 1;
 
+// A tensor-core product of the training kernel did not complete within its wait limit.
+struct TrainTimeout : std::runtime_error {
+  TrainTimeout() : std::runtime_error("the tensor-core training kernel timed out waiting for its products") {}
+};
+
 namespace {
-
-__global__ void k_fwd(MlpDev M, const float* __restrict__ feat, const float* __restrict__ target, int B,
-                      float* Z1, float* Z2, float* Z3, __nv_bfloat16* H0t, __nv_bfloat16* H1t, __nv_bfloat16* H2t,
-                      __nv_bfloat16* H3t, float* dy, float* loss) {
-  const int lane = threadIdx.x & 31;
-  const int tile = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  if (tile * 16 >= B) return;
-  const int r0 = tile * 16, g = lane >> 2, t = lane & 3;
-  auto F = [&](int row, int col) { return feat[(size_t)(r0 + row) * kMlpIn + col]; };
-  uint32_t a0[1][4];
-  feature_frag(M, lane, F, a0);
-  // store the normalised input transposed (its BF16 values are what layer 1 consumed)
-  auto store_t = [&](__nv_bfloat16* Ht, const uint32_t(&a)[4], int ks) {
-    const __nv_bfloat162 v0 = *reinterpret_cast<const __nv_bfloat162*>(&a[0]);
-    const __nv_bfloat162 v1 = *reinterpret_cast<const __nv_bfloat162*>(&a[1]);
-    const __nv_bfloat162 v2 = *reinterpret_cast<const __nv_bfloat162*>(&a[2]);
-    const __nv_bfloat162 v3 = *reinterpret_cast<const __nv_bfloat162*>(&a[3]);
-    const int c = ks * 16 + 2 * t;
-    Ht[(size_t)c * B + r0 + g] = v0.x;
-    Ht[(size_t)(c + 1) * B + r0 + g] = v0.y;
-    Ht[(size_t)c * B + r0 + g + 8] = v1.x;
-    Ht[(size_t)(c + 1) * B + r0 + g + 8] = v1.y;
-    Ht[(size_t)(c + 8) * B + r0 + g] = v2.x;
-    Ht[(size_t)(c + 9) * B + r0 + g] = v2.y;
-    Ht[(size_t)(c + 8) * B + r0 + g + 8] = v3.x;
-    Ht[(size_t)(c + 9) * B + r0 + g + 8] = v3.y;
-  };
-  store_t(H0t, a0[0], 0);
-  auto store_z = [&](float* Z, const float (*z)[4]) {
-    for (int nt = 0; nt < 16; ++nt) {
-      const int c = nt * 8 + 2 * t;
-      *reinterpret_cast<float2*>(Z + (size_t)(r0 + g) * kMlpHidden + c) = make_float2(z[nt][0], z[nt][1]);
-      *reinterpret_cast<float2*>(Z + (size_t)(r0 + g + 8) * kMlpHidden + c) = make_float2(z[nt][2], z[nt][3]);
-    }
-  };
-  uint32_t h1[8][4], h2[8][4];
-  float z[16][4];
-  mlp_layer<1>(a0, M.W1, M.b1, lane, h1, z);
-  store_z(Z1, z);
-  for (int ks = 0; ks < 8; ++ks) store_t(H1t, h1[ks], ks);
-  mlp_layer<8>(h1, M.W2, M.b2, lane, h2, z);
-  store_z(Z2, z);
-  for (int ks = 0; ks < 8; ++ks) store_t(H2t, h2[ks], ks);
-  mlp_layer<8>(h2, M.W3, M.b3, lane, h1, z);
-  store_z(Z3, z);
-  for (int ks = 0; ks < 8; ++ks) store_t(H3t, h1[ks], ks);
-  float ylo, yhi;
-  mlp_head(h1, M.w4, __ldg(M.b4), lane, ylo, yhi);
-  if (t == 0) {
-    const float elo = ylo - target[r0 + g] / M.out_scale, ehi = yhi - target[r0 + g + 8] / M.out_scale;
-    dy[r0 + g] = 2.f * elo / B;
-    dy[r0 + g + 8] = 2.f * ehi / B;
-    atomicAdd(loss, (elo * elo + ehi * ehi) / B);
-  }
-}
-
-// dZ of one layer from dH in C layout: dz = dh * gelu'(Z); stored transposed (BF16) and
-// returned as k16 A fragments for the next product
-__device__ __forceinline__ void dz_from_dh(float (*dh)[4], const float* Z, int B, int r0, int lane,
-                                           __nv_bfloat16* dZt, uint32_t (&a)[8][4]) {
-  const int g = lane >> 2, t = lane & 3;
-#pragma unroll
-  for (int nt = 0; nt < 16; ++nt) {
-    const int c = nt * 8 + 2 * t;
-    const float2 zl = *reinterpret_cast<const float2*>(Z + (size_t)(r0 + g) * kMlpHidden + c);
-    const float2 zh = *reinterpret_cast<const float2*>(Z + (size_t)(r0 + g + 8) * kMlpHidden + c);
-    dh[nt][0] *= gelu_grad_f(zl.x);
-    dh[nt][1] *= gelu_grad_f(zl.y);
-    dh[nt][2] *= gelu_grad_f(zh.x);
-    dh[nt][3] *= gelu_grad_f(zh.y);
-  }
-#pragma unroll
-  for (int p = 0; p < 8; ++p) {
-    a[p][0] = pack_bf16(dh[2 * p][0], dh[2 * p][1]);
-    a[p][1] = pack_bf16(dh[2 * p][2], dh[2 * p][3]);
-    a[p][2] = pack_bf16(dh[2 * p + 1][0], dh[2 * p + 1][1]);
-    a[p][3] = pack_bf16(dh[2 * p + 1][2], dh[2 * p + 1][3]);
-    const __nv_bfloat162 v0 = *reinterpret_cast<const __nv_bfloat162*>(&a[p][0]);
-    const __nv_bfloat162 v1 = *reinterpret_cast<const __nv_bfloat162*>(&a[p][1]);
-    const __nv_bfloat162 v2 = *reinterpret_cast<const __nv_bfloat162*>(&a[p][2]);
-    const __nv_bfloat162 v3 = *reinterpret_cast<const __nv_bfloat162*>(&a[p][3]);
-    const int c = p * 16 + 2 * t;
-    dZt[(size_t)c * B + r0 + g] = v0.x;
-    dZt[(size_t)(c + 1) * B + r0 + g] = v0.y;
-    dZt[(size_t)c * B + r0 + g + 8] = v1.x;
-    dZt[(size_t)(c + 1) * B + r0 + g + 8] = v1.y;
-    dZt[(size_t)(c + 8) * B + r0 + g] = v2.x;
-    dZt[(size_t)(c + 9) * B + r0 + g] = v2.y;
-    dZt[(size_t)(c + 8) * B + r0 + g + 8] = v3.x;
-    dZt[(size_t)(c + 9) * B + r0 + g + 8] = v3.y;
-  }
-}
-
-// dH = dZ . W (W [out][in]), B operand W^T stored [in][out]
-__device__ __forceinline__ void back_product(const uint32_t (&a)[8][4], const __nv_bfloat16* Wt, int lane,
-                                             float (*dh)[4]) {
-#pragma unroll
-  for (int nt = 0; nt < 16; ++nt) {
-    dh[nt][0] = dh[nt][1] = dh[nt][2] = dh[nt][3] = 0.f;
-#pragma unroll
-    for (int ks = 0; ks < 8; ++ks) {
-      uint32_t b0, b1;
-      load_b_frag(Wt, kMlpHidden, nt, ks, lane, b0, b1);
-      mma_bf16_16816(dh[nt], a[ks], b0, b1);
-    }
-  }
-}
-
-__global__ void k_bwd(MlpDev M, const __nv_bfloat16* W2t, const __nv_bfloat16* W3t, int B, const float* Z1,
-                      const float* Z2, const float* Z3, const __nv_bfloat16* H3t, const float* dy,
-                      __nv_bfloat16* dZ1t, __nv_bfloat16* dZ2t, __nv_bfloat16* dZ3t, float* gw4, float* gb4) {
-  const int lane = threadIdx.x & 31;
-  const int tile = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  if (tile * 16 >= B) return;
-  const int r0 = tile * 16, g = lane >> 2, t = lane & 3;
-  const float dlo = dy[r0 + g], dhi = dy[r0 + g + 8];
-  float dh[16][4];
-#pragma unroll
-  for (int nt = 0; nt < 16; ++nt) {
-    const int c = nt * 8 + 2 * t;
-    const float w0 = M.w4[c], w1 = M.w4[c + 1];
-    dh[nt][0] = dlo * w0;
-    dh[nt][1] = dlo * w1;
-    dh[nt][2] = dhi * w0;
-    dh[nt][3] = dhi * w1;
-    // dw4 partials: sum over the 16 rows of dy * H3
-    float p0 = dlo * __bfloat162float(H3t[(size_t)c * B + r0 + g]) + dhi * __bfloat162float(H3t[(size_t)c * B + r0 + g + 8]);
-    float p1 = dlo * __bfloat162float(H3t[(size_t)(c + 1) * B + r0 + g]) +
-               dhi * __bfloat162float(H3t[(size_t)(c + 1) * B + r0 + g + 8]);
-    for (int o = 4; o < 32; o <<= 1) {
-      p0 += __shfl_xor_sync(0xffffffffu, p0, o);
-      p1 += __shfl_xor_sync(0xffffffffu, p1, o);
-    }
-    if (g == 0) {
-      atomicAdd(gw4 + c, p0);
-      atomicAdd(gw4 + c + 1, p1);
-    }
-  }
-  if (lane == 0) {
-    float s = 0.f;
-    for (int r = 0; r < 16; ++r) s += dy[r0 + r];
-    atomicAdd(gb4, s);
-  }
-  uint32_t a[8][4];
-  dz_from_dh(dh, Z3, B, r0, lane, dZ3t, a);
-  back_product(a, W3t, lane, dh);
-  dz_from_dh(dh, Z2, B, r0, lane, dZ2t, a);
-  back_product(a, W2t, lane, dh);
-  dz_from_dh(dh, Z1, B, r0, lane, dZ1t, a);
-}
-
-// dW[m][n] = sum_b At[m][b] Bt[n][b]  (At [M][K], Bt [N][K] rows of length K = batch)
-__global__ void k_wgrad(const __nv_bfloat16* At, const __nv_bfloat16* Bt, int M, int N, int K, float* dW) {
-  const int lane = threadIdx.x & 31;
-  const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  const int ntn = N / 8;
-  if (w >= (M / 16) * ntn) return;
-  const int mt = w / ntn, nt = w % ntn;
-  const int g = lane >> 2, t = lane & 3;
-  float acc[4] = {0.f, 0.f, 0.f, 0.f};
-  for (int ks = 0; ks < K / 16; ++ks) {
-    uint32_t a[4];
-    const __nv_bfloat16* p = At + (size_t)(mt * 16 + g) * K + ks * 16 + 2 * t;
-    a[0] = *reinterpret_cast<const unsigned int*>(p);
-    a[1] = *reinterpret_cast<const unsigned int*>(p + (size_t)8 * K);
-    a[2] = *reinterpret_cast<const unsigned int*>(p + 8);
-    a[3] = *reinterpret_cast<const unsigned int*>(p + (size_t)8 * K + 8);
-    uint32_t b0, b1;
-    load_b_frag(Bt, K, nt, ks, lane, b0, b1);
-    mma_bf16_16816(acc, a, b0, b1);
-  }
-  const int r = mt * 16 + g, c = nt * 8 + 2 * t;
-  dW[(size_t)r * N + c] = acc[0];
-  dW[(size_t)r * N + c + 1] = acc[1];
-  dW[(size_t)(r + 8) * N + c] = acc[2];
-  dW[(size_t)(r + 8) * N + c + 1] = acc[3];
-}
-
-__global__ void k_bsum(const __nv_bfloat16* dZt, int B, float* db) {  // one warp per output neuron
-  const int lane = threadIdx.x & 31;
-  const int j = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  if (j >= kMlpHidden) return;
-  float s = 0.f;
-  for (int b = lane; b < B; b += 32) s += __bfloat162float(dZt[(size_t)j * B + b]);
-  for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-  if (lane == 0) db[j] = s;
-}
 
 __global__ void k_adam(float* p, const float* gr, float* m1, float* m2, int n, float lr, float b1, float b2, float eps,
                        float c1, float c2) {
@@ -334,62 +149,49 @@ void dal(T*& p, size_t n) {
   MM_CK(cudaMalloc(reinterpret_cast<void**>(&p), sizeof(T) * (n ? n : 1)));
 }
 
-// Activations and gradients of one batch of B rows, allocated once per call.
+// Per-call buffers of the training kernels: the loss accumulator and the error flag of the
+// bounded tensor-core waits.
 struct Scratch {
   int B = 0;
-  float *Z1 = nullptr, *Z2 = nullptr, *Z3 = nullptr, *dy = nullptr, *loss = nullptr;
-  __nv_bfloat16 *H0t = nullptr, *H1t = nullptr, *H2t = nullptr, *H3t = nullptr;
-  __nv_bfloat16 *dZ1t = nullptr, *dZ2t = nullptr, *dZ3t = nullptr;
+  float* loss = nullptr;
+  int* err = nullptr;
   explicit Scratch(int b) : B(b) {
-    const size_t H = kMlpHidden;
-    dal(Z1, H * B);
-    dal(Z2, H * B);
-    dal(Z3, H * B);
-    dal(dy, B);
     dal(loss, 1);
-    dal(H0t, (size_t)kMlpInPad * B);
-    dal(H1t, H * B);
-    dal(H2t, H * B);
-    dal(H3t, H * B);
-    dal(dZ1t, H * B);
-    dal(dZ2t, H * B);
-    dal(dZ3t, H * B);
+    dal(err, 1);
+    MM_CK(cudaMemset(err, 0, sizeof(int)));
   }
   ~Scratch() {
-    for (void* q : {(void*)Z1, (void*)Z2, (void*)Z3, (void*)dy, (void*)loss, (void*)H0t, (void*)H1t, (void*)H2t,
-                    (void*)H3t, (void*)dZ1t, (void*)dZ2t, (void*)dZ3t})
-      if (q) cudaFree(q);
+    if (loss) cudaFree(loss);
+    if (err) cudaFree(err);
   }
   Scratch(const Scratch&) = delete;
   Scratch& operator=(const Scratch&) = delete;
 };
 
-// Gradient of the batch loss (mean squared error in units of out_scale) into md.g; the
-// loss is added to sc.loss.  All on md.stream, no host synchronisation.
+// Gradient of the batch loss (mean squared error in units of out_scale) into md.g on the
+// tensor cores (k_train_tc, one CTA per 128 rows); the loss is added to sc.loss.  All on
+// md.stream, no host synchronisation.
 void grad_batch(Model& md, Scratch& sc, const float* dfeat, const float* dtarget) {
   cudaStream_t st = md.stream;
   const int B = sc.B;
+  static bool attr_set[64] = {};
+  if (md.device < 64 && !attr_set[md.device]) {
+    MM_CK(cudaFuncSetAttribute(k_train_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmTrain));
+    attr_set[md.device] = true;
+  }
   MM_CK(cudaMemsetAsync(md.g, 0, sizeof(float) * kNumParams, st));
-  const MlpDev M = md.view();
-  const int warps = B / 16, tpb = 128;
-  k_fwd<<<(warps * 32 + tpb - 1) / tpb, tpb, 0, st>>>(M, dfeat, dtarget, B, sc.Z1, sc.Z2, sc.Z3, sc.H0t, sc.H1t, sc.H2t,
-                                                     sc.H3t, sc.dy, sc.loss);
+  k_train_tc<<<(B + kTcRows - 1) / kTcRows, kTcThreads, kSmTrain, st>>>(
+      md.view(), md.W2t, md.W3t, dfeat, dtarget, B, md.g, kOffW1, kOffB1, kOffW2, kOffB2, kOffW3, kOffB3, kOffW4,
+      kOffB4, sc.loss, sc.err);
   MM_CK(cudaGetLastError());
-  k_bwd<<<(warps * 32 + tpb - 1) / tpb, tpb, 0, st>>>(M, md.W2t, md.W3t, B, sc.Z1, sc.Z2, sc.Z3, sc.H3t, sc.dy, sc.dZ1t,
-                                                     sc.dZ2t, sc.dZ3t, md.g + kOffW4, md.g + kOffB4);
-  MM_CK(cudaGetLastError());
-  auto wg = [&](const __nv_bfloat16* At, const __nv_bfloat16* Bt, int Mr, int N, float* dW) {
-    const int tiles = (Mr / 16) * (N / 8);
-    k_wgrad<<<(tiles * 32 + 127) / 128, 128, 0, st>>>(At, Bt, Mr, N, B, dW);
-    MM_CK(cudaGetLastError());
-  };
-  wg(sc.dZ3t, sc.H2t, kMlpHidden, kMlpHidden, md.g + kOffW3);
-  wg(sc.dZ2t, sc.H1t, kMlpHidden, kMlpHidden, md.g + kOffW2);
-  wg(sc.dZ1t, sc.H0t, kMlpHidden, kMlpInPad, md.g + kOffW1);
-  k_bsum<<<(kMlpHidden * 32) / 128, 128, 0, st>>>(sc.dZ3t, B, md.g + kOffB3);
-  k_bsum<<<(kMlpHidden * 32) / 128, 128, 0, st>>>(sc.dZ2t, B, md.g + kOffB2);
-  k_bsum<<<(kMlpHidden * 32) / 128, 128, 0, st>>>(sc.dZ1t, B, md.g + kOffB1);
-  MM_CK(cudaGetLastError());
+}
+
+// The training kernels' bounded waits: a product that did not complete is reported.
+void check_train(Scratch& sc, cudaStream_t st) {
+  int e = 0;
+  MM_CK(cudaMemcpyAsync(&e, sc.err, sizeof(int), cudaMemcpyDeviceToHost, st));
+  MM_CK(cudaStreamSynchronize(st));
+  if (e) throw TrainTimeout();
 }
 
 void check_samples(const float* f, const float* t, int64_t n) {
@@ -435,6 +237,9 @@ using namespace mumag;
   }                                             \
   catch (const mumag::CudaFailure& e) {         \
     return mfail(MM_CUDA_ERROR, e.what());      \
+  }                                             \
+  catch (const mumag::TrainTimeout& e) {        \
+    return mfail(MM_TIMEOUT, e.what());         \
   }                                             \
   catch (const std::bad_alloc&) {               \
     return mfail(MM_BAD_INPUT, "host allocation failed"); \
@@ -606,6 +411,7 @@ mm_status mm_model_grad(mm_model* mo, const float* feats, const float* target, i
   MM_CK(cudaMemcpyAsync(&l, sc.loss, sizeof(float), cudaMemcpyDeviceToHost, md.stream));
   if (grads) MM_CK(cudaMemcpyAsync(grads, md.g, sizeof(float) * kNumParams, cudaMemcpyDeviceToHost, md.stream));
   MM_CK(cudaStreamSynchronize(md.stream));
+  check_train(sc, md.stream);
   if (loss) *loss = l;
   return MM_OK;
   MAPI_END
@@ -649,6 +455,7 @@ mm_status mm_model_train(mm_model* mo, const float* feats, const float* target, 
     float l = 0.f;
     MM_CK(cudaMemcpyAsync(&l, sc.loss, sizeof(float), cudaMemcpyDeviceToHost, md.stream));
     MM_CK(cudaStreamSynchronize(md.stream));
+    check_train(sc, md.stream);
     last = l / (float)nb;
     if (!std::isfinite(last)) throw std::runtime_error("training diverged (non-finite loss)");
   }
