@@ -235,9 +235,10 @@ struct Ctx {
 
 __device__ __forceinline__ const double* plane(const SolveArgs& a, int p) { return a.vals + (size_t)p * a.nent; }
 
-// C v at row i (exchange scalar + anisotropy blocks), v a 3-vector
-template <class VT>
-__device__ __forceinline__ void apply_C_row_t(const Ctx& c, const VT* Aex, const VT* K, const double* v, int64_t off,
+// C v at row i (exchange scalar + anisotropy blocks), v a 3-vector; VT = operator value
+// type, XT = vector type (FP64 products and sums in every case)
+template <class VT, class XT = double>
+__device__ __forceinline__ void apply_C_row_t(const Ctx& c, const VT* Aex, const VT* K, const XT* v, int64_t off,
                                               int64_t loff, int w, double o[3]) {
   const SolveArgs& a = c.a;
   const int64_t ps = a.nent;
@@ -247,7 +248,7 @@ __device__ __forceinline__ void apply_C_row_t(const Ctx& c, const VT* Aex, const
   for (int k = 0; k < w; ++k) {
     const int64_t e = off + 32 * (int64_t)k;
     const int j = c.scol[loff + 32 * (int64_t)k];
-    const double v0 = v[j], v1 = v[n + j], v2 = v[2 * n + j];
+    const double v0 = (double)v[j], v1 = (double)v[n + j], v2 = (double)v[2 * n + j];
     const double ax = (double)__ldg(Aex + e);
     const double k0 = (double)__ldg(K + e), k1 = (double)__ldg(K + ps + e), k2 = (double)__ldg(K + 2 * ps + e);
     const double k3 = (double)__ldg(K + 3 * ps + e), k4 = (double)__ldg(K + 4 * ps + e), k5 = (double)__ldg(K + 5 * ps + e);
@@ -776,6 +777,14 @@ __device__ __noinline__ bool pcg_solve(Ctx& c, const double* x) {
 // refinement: r = b - S u in FP64 -> inner FP32 solve S e = r to 1e-5 relative -> u += e,
 // r -= S e in FP64 -> repeat until the FP64 residual meets the reference's test
 // r.r <= tol_u^2 b.b.  The inner iterations are counted as PCG iterations.
+// An FP32 inner solve stops at 1e-5 of its starting residual or at 0.9 of the outer
+// residual target, whichever is larger (squared norms here).  The FP32 recurrence residual
+// tracks the FP64 one to about 1e-7 of the inner right-hand side, far inside the 10 % margin,
+// so one refinement pass normally meets the outer test.  Measured with the two-level
+// preconditioner on an 80 nm multigrain switching step: 41.2 iterations per solve to 0.9 of
+// the target, 43.3 to 0.5 of it, 40.8 to the target itself.
+constexpr double kInnerTarget2 = 0.81;
+
 struct CGNext32 {
   float s, r, z;
 };
@@ -876,7 +885,7 @@ __device__ __noinline__ bool pcg_solve_mixed(Ctx& c, const double* x) {
     CHECK(learned_start_mixed<TC>(c, x, sig, rr, rin2, gin));
   }
   for (int outer = 0; rr > atol2 && k < a.max_pcg && outer < 32; ++outer) {
-    const double inner_tol2 = fmax(1e-10 * rin2, 0.25 * atol2);  // 1e-5 relative, or the outer target
+    const double inner_tol2 = fmax(1e-10 * rin2, kInnerTarget2 * atol2);  // 1e-5 relative, or near the outer target
     double gamma = gin, delta;
     {  // w0 = S32 z0; reset the inner vectors
       double pd = 0;
@@ -1422,7 +1431,7 @@ __device__ __noinline__ bool pcg_solve_mixed_coarse(Ctx& c, const double* x) {
       gamma = v[0];
       rin2 = v[1];
     }
-    const double inner_tol2 = fmax(1e-10 * rin2, 0.25 * atol2);  // 1e-5 relative, or the outer target
+    const double inner_tol2 = fmax(1e-10 * rin2, kInnerTarget2 * atol2);  // 1e-5 relative, or near the outer target
     {  // w0 = S32 z0, delta = w0.z0, box sums of w0
       double pd = 0;
       FOR_ROWS_R(rw)
@@ -1612,38 +1621,55 @@ __device__ bool step_normalize(Ctx& c, double* xout, const double* x, double alp
 // M_inv, scripts/loop.py:40-55 -> truncated_cg_diag_precond_jit, scripts/solvers.py:7-131
 // A v = mbar x ((C v) x mbar) - (mbar . gf) v,  D = exchange diagonal
 // ---------------------------------------------------------------------------------------
-__device__ __forceinline__ void apply_A_row(const Ctx& c, const double* mb, const double* v, int i,
-                                            int64_t off, int64_t loff, int w, double o[3]) {
+// A v at row i; v in FP64 (FP64 path) or FP32 (mixed precision, with the FP32 C planes)
+template <class XT>
+__device__ __forceinline__ void apply_A_row(const Ctx& c, const double* mb, const XT* v, int i, int64_t off,
+                                            int64_t loff, int w, double o[3]) {
   const SolveArgs& a = c.a;
   const int n = a.Npad;
   double cv[3];
-  if (a.mixed)
-    apply_C_row_t<float>(c, a.vals32 + (size_t)P_AEX * a.nent, a.vals32 + (size_t)P_K * a.nent, v, off, loff, w, cv);
+  if constexpr (sizeof(XT) == 4)
+    apply_C_row_t<float, XT>(c, a.vals32 + (size_t)P_AEX * a.nent, a.vals32 + (size_t)P_K * a.nent, v, off, loff, w,
+                             cv);
+  else if (a.mixed)
+    apply_C_row_t<float, XT>(c, a.vals32 + (size_t)P_AEX * a.nent, a.vals32 + (size_t)P_K * a.nent, v, off, loff, w,
+                             cv);
   else
-    apply_C_row(c, v, off, loff, w, cv);
+    apply_C_row_t<double, XT>(c, plane(a, P_AEX), plane(a, P_K), v, off, loff, w, cv);
   const double m[3] = {mb[i], mb[n + i], mb[2 * n + i]};
   const double md = m[0] * a.gf[i] + m[1] * a.gf[n + i] + m[2] * a.gf[2 * n + i];
   double pr[3];
   project(m, cv, pr);
-  o[0] = pr[0] - md * v[i];
-  o[1] = pr[1] - md * v[n + i];
-  o[2] = pr[2] - md * v[2 * n + i];
+  o[0] = pr[0] - md * (double)v[i];
+  o[1] = pr[1] - md * (double)v[n + i];
+  o[2] = pr[2] - md * (double)v[2 * n + i];
 }
 
+template <class XT>
 __device__ bool minv_body(Ctx& c, const double* g, const double* mb, double* zout);
 
-// zout = M_inv(g): p with A p ~ g, or g itself when p stays zero.
+// zout = M_inv(g): p with A p ~ g, or g itself when p stays zero.  The mixed path runs the
+// truncated CG's vectors (r, z, d, B d) in FP32 -- the search directions of M_inv -- with
+// FP64 arithmetic, FP64 sums and the FP64 result p.
 __device__ bool minv(Ctx& c, const double* g, const double* mb, double* zout) {
   const bool tm = c.sy.timing && threadIdx.x == 0;
   const unsigned long long t0 = tm ? globaltimer() : 0ull;
-  const bool ok = minv_body(c, g, mb, zout);
+  const bool ok = c.a.mixed ? minv_body<float>(c, g, mb, zout) : minv_body<double>(c, g, mb, zout);
   if (tm) c.t_minv += globaltimer() - t0;
   return ok;
 }
 
+// XT: the vector type of r, z, d and B d (their FP64 buffers hold the FP32 vectors in their
+// first half on the mixed path).  Every update is computed in FP64 from the stored values
+// and rounded once when stored; the sums use the stored values.
+template <class XT>
 __device__ bool minv_body(Ctx& c, const double* g, const double* mb, double* zout) {
   const SolveArgs& a = c.a;
   const int n = a.Npad;
+  XT* const tr = reinterpret_cast<XT*>(a.tr);
+  XT* const tz = reinterpret_cast<XT*>(a.tz);
+  XT* const td = reinterpret_cast<XT*>(a.td);
+  XT* const tB = reinterpret_cast<XT*>(a.tBd);
   if (a.precond_iter <= 0) {
     FOR_ROWS(c)
     (void)off_;
@@ -1660,11 +1686,11 @@ __device__ bool minv_body(Ctx& c, const double* g, const double* mb, double* zou
   const double Di = __ldg(a.Dex + i);
   for (int q = 0; q < 3; ++q) {
     const double gi = g[q * n + i];
-    const double r = -gi;
-    const double z = r / Di;
-    a.tr[q * n + i] = r;
-    a.tz[q * n + i] = z;
-    a.td[q * n + i] = -z;
+    const XT r = (XT)(-gi);
+    const XT z = (XT)((double)r / Di);
+    tr[q * n + i] = r;
+    tz[q * n + i] = z;
+    td[q * n + i] = -z;
     zout[q * n + i] = 0.0;
     gg += gi * gi;
   }
@@ -1682,11 +1708,12 @@ __device__ bool minv_body(Ctx& c, const double* g, const double* mb, double* zou
     double pd = 0, prz = 0;
     FOR_ROWS(c)
     double o[3];
-    apply_A_row(c, mb, a.td, i, off_, loff_, w_, o);
+    apply_A_row<XT>(c, mb, td, i, off_, loff_, w_, o);
     for (int q = 0; q < 3; ++q) {
-      a.tBd[q * n + i] = o[q];
-      pd += a.td[q * n + i] * o[q];
-      prz += a.tr[q * n + i] * a.tz[q * n + i];
+      const XT b = (XT)o[q];
+      tB[q * n + i] = b;
+      pd += (double)td[q * n + i] * (double)b;
+      prz += (double)tr[q * n + i] * (double)tz[q * n + i];
     }
     END_ROWS
     double v[2] = {pd, prz};
@@ -1708,13 +1735,13 @@ __device__ bool minv_body(Ctx& c, const double* g, const double* mb, double* zou
     const double Di = __ldg(a.Dex + i);
     for (int q = 0; q < 3; ++q) {
       const int idx = q * n + i;
-      zout[idx] = zout[idx] + alpha * a.td[idx];
-      const double r = a.tr[idx] + alpha * a.tBd[idx];
-      const double z = r / Di;
-      a.tr[idx] = r;
-      a.tz[idx] = z;
-      prn += r * r;
-      przn += r * z;
+      zout[idx] = zout[idx] + alpha * (double)td[idx];
+      const XT r = (XT)((double)tr[idx] + alpha * (double)tB[idx]);
+      const XT z = (XT)((double)r / Di);
+      tr[idx] = r;
+      tz[idx] = z;
+      prn += (double)r * (double)r;
+      przn += (double)r * (double)z;
     }
     END_ROWS
     double v[2] = {prn, przn};
@@ -1727,14 +1754,14 @@ __device__ bool minv_body(Ctx& c, const double* g, const double* mb, double* zou
     double pd = 0;
     FOR_ROWS(c)
     double o[3];
-    apply_A_row(c, mb, a.tz, i, off_, loff_, w_, o);
+    apply_A_row<XT>(c, mb, tz, i, off_, loff_, w_, o);
     for (int q = 0; q < 3; ++q) {
       const int idx = q * n + i;
-      const double dn = -a.tz[idx] + beta * a.td[idx];
-      const double bn = -o[q] + beta * a.tBd[idx];
-      a.td[idx] = dn;
-      a.tBd[idx] = bn;
-      pd += dn * bn;
+      const XT dn = (XT)(-(double)tz[idx] + beta * (double)td[idx]);
+      const XT bn = (XT)(-o[q] + beta * (double)tB[idx]);
+      td[idx] = dn;
+      tB[idx] = bn;
+      pd += (double)dn * (double)bn;
     }
     END_ROWS
     double v2[1] = {pd};

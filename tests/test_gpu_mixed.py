@@ -1,6 +1,7 @@
 """Mixed precision (MM_PREC_MIXED): FP32 copies of every operator plane (Poisson, exchange,
 anisotropy, divergence, gradient) read with FP64 vectors and FP64 sums, FP32 inner PCG
-iterations, FP64 residual refinement, reductions and stop tests.
+iterations, FP64 residual refinement, reductions and stop tests; M_inv's truncated CG keeps
+its vectors (r, z, d, B d) in FP32 with FP64 arithmetic and sums.
 
 Bars: energies and fields of one evaluation within the FP32 rounding of the operator values
 (the FP32 planes define a slightly perturbed but consistent energy: 2-4e-8 relative on these
