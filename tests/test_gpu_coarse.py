@@ -69,14 +69,16 @@ def test_coarse_field_step_matches_jacobi(grains):
     assert b["pcg_iters"] / b["evals"] < a["pcg_iters"] / a["evals"]
 
 
-def test_coarse_launch_shapes_and_staging_agree(grains):
+@pytest.mark.parametrize("precision", [_native.PREC_FP64, _native.PREC_MIXED])
+def test_coarse_launch_shapes_and_staging_agree(grains, precision):
     """The box sums follow the CTA partition, so other grids round differently: energies agree
     to 1e-10; staged and streamed operators give identical results on one grid."""
     X, T, tag, krn, m0 = grains
     sp = _native.solver_params(hdir=[0.0, 0.0, 1.0])
     out = []
     for grid, stage in ((0, 1), (0, 0), (37, 1), (5, 1)):
-        with _native.Mesh(X, T, tag, krn, coarse_box_nodes=64, grid_ctas=grid, stage_operators=stage) as M:
+        with _native.Mesh(X, T, tag, krn, precision=precision, coarse_box_nodes=64, grid_ctas=grid,
+                          stage_operators=stage) as M:
             M.set_state(m0, None, m0)
             E, gp, it = M.energy_grad(0.3, sp)
             out.append((E, gp, it))
