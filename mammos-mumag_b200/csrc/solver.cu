@@ -1326,6 +1326,15 @@ __device__ __noinline__ void coarse_update(Ctx& c, bool restart, double alpha, d
     if (c.crows) {
       const float* row = c.crows + (size_t)q * nc;
       for (int j = c.lane; j < nc; j += 32) acc += (double)row[j] * c.cPr[j];
+    } else if ((nc & 3) == 0) {  // from L2, 16-byte loads all in flight at once
+      const float4* row = reinterpret_cast<const float4*>(a.Ainv32 + (size_t)(c.cb0 + q) * nc);
+      const int n4 = nc >> 2;
+#pragma unroll 8
+      for (int j = c.lane; j < n4; j += 32) {
+        const float4 r = __ldg(row + j);
+        const double* pr = c.cPr + 4 * j;
+        acc += (double)r.x * pr[0] + (double)r.y * pr[1] + (double)r.z * pr[2] + (double)r.w * pr[3];
+      }
     } else {
       const float* row = a.Ainv32 + (size_t)(c.cb0 + q) * nc;
       for (int j = c.lane; j < nc; j += 32) acc += (double)__ldg(row + j) * c.cPr[j];
@@ -2178,10 +2187,10 @@ __device__ __forceinline__ void solve_body(const SolveArgs& args, int nblk, int 
     double* base = reinterpret_cast<double*>(smem + args.co_off);
     c.cPs = base;
     c.cPr = base + args.nc;
-    c.cxc = base + 2 * args.nc;
-    c.cslv = base + 3 * args.nc;
+    c.cslv = base + 2 * args.nc;
     c.csv = c.cslv + args.nc + kMaxGrid;
-    c.csb = reinterpret_cast<int*>(c.csv + 2 * args.meta_max);
+    c.cxc = c.csv + 2 * args.meta_max;
+    c.csb = reinterpret_cast<int*>(c.cxc + args.co_nb);
     c.cmk = reinterpret_cast<unsigned*>(c.csb + 2 * args.meta_max);
     int* bsl = reinterpret_cast<int*>(c.cmk + 2 * args.meta_max);
     for (int q = threadIdx.x; q <= args.nc; q += blockDim.x) bsl[q] = __ldg(args.bslot + q);
@@ -2299,13 +2308,16 @@ struct StagePlan {
   int extra_off;  // offset of the extra region, -1 = none
   int co_off;     // offset of the coarse region, -1 = none
   int co_rows;    // rows of Ac^-1 each CTA stages (the most boxes a CTA holds), 0 = none
+  int co_nb;      // the most boxes a CTA holds rows of (the size of its xc)
 };
-// Regions: [staged entries][slice metadata][coarse vectors: Ps, Pr, xc (nc doubles each),
-// the staged box slots (nc + kMaxGrid doubles), per slice two partial sums, two box ids and
-// two lane masks, every box's first slot (nc + 1 ints), the CTA's rows of Ac^-1 in FP32
-// when they fit][tensor-core network]
+// Regions: [staged entries][slice metadata][coarse vectors: Ps, Pr (nc doubles each), the
+// staged box slots (nc + kMaxGrid doubles), per slice two partial sums, xc of the CTA's boxes,
+// per slice two box ids and two lane masks, every box's first slot (nc + 1 ints), the CTA's
+// rows of Ac^-1 in FP32 when they fit and `stage_rows`][tensor-core network].  Shared memory
+// is taken from the SM's L1 cache, so the rows are staged only for the two-CTA build: three
+// resident CTAs with their rows would leave L1 too small for the gathers.
 StagePlan stage_plan(const DevMesh& m, int grid, size_t limit, size_t extra = 0, bool allow_stage = true,
-                     int nc = 0) {
+                     int nc = 0, bool stage_rows = true) {
   int64_t emax = 0, smax = 0;
   for (int b = 0; b < grid; ++b) {
     const int64_t s0 = (m.h.nslices * b) / grid, s1 = (m.h.nslices * (b + 1)) / grid;
@@ -2313,17 +2325,8 @@ StagePlan stage_plan(const DevMesh& m, int grid, size_t limit, size_t extra = 0,
     smax = std::max(smax, s1 - s0);
   }
   const size_t meta = (size_t)smax * (sizeof(int64_t) + sizeof(int32_t));
-  const size_t coarse = nc > 0 ? (size_t)(4 * nc + kMaxGrid + 2 * smax) * sizeof(double) +
-                                     (size_t)(4 * smax + nc + 1) * sizeof(int) + 16
-                               : 0;
-  const size_t need = (size_t)emax * (sizeof(double) + sizeof(int32_t) + (m.vals32 ? sizeof(float) : 0));
-  StagePlan p;
-  p.stage = (allow_stage && need + meta + 16 + coarse + (extra ? extra + 1024 : 0) <= limit) ? 1 : 0;
-  // the two-level preconditioner's rows of Ac^-1 per CTA, staged when they fit beside the rest
-  p.co_rows = 0;
-  size_t rows = 0;
-  if (nc > 0) {
-    int bmax = 0;
+  int bmax = 0;  // the most boxes one CTA holds rows of
+  if (nc > 0)
     for (int b = 0; b < grid; ++b) {
       const int64_t r0 = kSlice * ((m.h.nslices * b) / grid), r1 = kSlice * ((m.h.nslices * (b + 1)) / grid);
       int lo = INT_MAX, hi = -1;
@@ -2334,6 +2337,17 @@ StagePlan stage_plan(const DevMesh& m, int grid, size_t limit, size_t extra = 0,
         }
       if (hi >= 0) bmax = std::max(bmax, hi - lo + 1);
     }
+  const size_t coarse = nc > 0 ? (size_t)(3 * nc + kMaxGrid + 2 * smax + bmax) * sizeof(double) +
+                                     (size_t)(4 * smax + nc + 1) * sizeof(int) + 16
+                               : 0;
+  const size_t need = (size_t)emax * (sizeof(double) + sizeof(int32_t) + (m.vals32 ? sizeof(float) : 0));
+  StagePlan p;
+  p.stage = (allow_stage && need + meta + 16 + coarse + (extra ? extra + 1024 : 0) <= limit) ? 1 : 0;
+  // the two-level preconditioner's rows of Ac^-1 per CTA, staged when they fit beside the rest
+  p.co_rows = 0;
+  p.co_nb = bmax;
+  size_t rows = 0;
+  if (nc > 0 && stage_rows) {
     const size_t want = (size_t)bmax * nc * sizeof(float) + 16;
     const size_t used = (p.stage ? need : 0) + meta + 16 + coarse + (extra ? extra + 1024 : 0);
     if (bmax > 0 && used + want <= limit) {
@@ -2432,7 +2446,8 @@ void solver_configure(DevMesh& m) {
   // share SMs, would lose residency to the region and keep the network on mma.sync.
   const size_t extra =
       (m.warm == WARM_LEARNED && block == kTcThreads && grid <= prop.multiProcessorCount) ? (size_t)kSmTc : 0;
-  const StagePlan sp = stage_plan(m, grid, limit, extra, m.opt.stage_operators != 0, m.nc);
+  if (m.kernel_mb != 2 && m.kernel_mb != 3) m.kernel_mb = 2;
+  const StagePlan sp = stage_plan(m, grid, limit, extra, m.opt.stage_operators != 0, m.nc, m.kernel_mb == 2);
   m.stage = sp.stage;
   m.stage_max = sp.stage_max;
   m.meta_max = sp.meta_max;
@@ -2440,6 +2455,7 @@ void solver_configure(DevMesh& m) {
   m.tc_off = sp.extra_off;
   m.co_off = sp.co_off;
   m.co_rows = sp.co_rows;
+  m.co_nb = sp.co_nb;
   // The attribute is per kernel, shared by every mesh: raise it to the device limit once
   // (occupancy follows each launch's actual request).
   const int dsm = (int)(prop.sharedMemPerBlockOptin - 16 * 1024);
@@ -2447,7 +2463,6 @@ void solver_configure(DevMesh& m) {
       cudaFuncSetAttribute(k_solve<3, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, dsm) != cudaSuccess ||
       cudaFuncSetAttribute(k_solve<2, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, dsm) != cudaSuccess)
     throw std::runtime_error("cannot reserve shared memory for the solver kernel");
-  if (m.kernel_mb != 2 && m.kernel_mb != 3) m.kernel_mb = 2;
   int occ = 0;
   if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, solve_kernel(m), block, m.smem) != cudaSuccess || occ < 1)
     throw std::runtime_error("persistent solver kernel cannot be resident with " + std::to_string(block) +
@@ -2593,6 +2608,7 @@ SolveArgs solver_args(const DevMesh& m, int mode, double h, const mm_solver_para
   a.ctabox = m.ctabox;
   a.co_off = m.co_off;
   a.co_rows = m.co_rows;
+  a.co_nb = m.co_nb;
   a.bar_stall = m.bar_stall;
   a.warm = m.warm;
   a.warm_gate2 = m.warm_gate * m.warm_gate;

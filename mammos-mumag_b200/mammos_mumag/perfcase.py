@@ -9,6 +9,8 @@
     python -m mammos_mumag.perfcase phase-timers [--workload multigrain|large] [--precision fp64|mixed]
                                                  [--grid N] [--ctas-per-sm 2|3] [--pcg-variant 1|2]
                                                  [--coarse BOX_NODES] [--from-step K] [--steps S]
+    python -m mammos_mumag.perfcase minv [--workload multigrain|large] [--precision fp64|mixed]
+                                         [--grid N] [--ctas-per-sm 2|3] [--coarse BOX_NODES]
     python -m mammos_mumag.perfcase mlp-train [--samples N] [--epochs E]
     python -m mammos_mumag.perfcase mlp-predict [--rows N]
 
@@ -32,6 +34,11 @@ this case before the mesh is built) over S field steps of the workload's sweep f
 step K (the steps before K run first, untimed): device time, work counters and the mean per
 CTA of the PCG row phases, the reductions (before, waiting at and after the grid barrier),
 the coarse update, whole Poisson solves, M_inv and the evaluations.
+
+``minv``: the same mesh and launch shape; one field step from the seeded initial state, one
+energy evaluation at a field 1 T lower, then the M_inv preconditioner (``mm_apply_minv``, one
+``k_solve`` launch each, truncated CG of up to 10 iterations) applied three times to that
+evaluation's gradient: launches 3 to 5 are M_inv alone.
 
 ``mlp-predict``: the network on N seeded feature rows (``k_predict``), twice.
 
@@ -167,6 +174,26 @@ def phase_timers(args) -> int:
     return 0
 
 
+def minv(args) -> int:
+    X, T, tag, krn, m0, hdir, h0 = _workload_mesh(args)
+    prec = _native.PREC_MIXED if args.precision == "mixed" else _native.PREC_FP64
+    sp = _native.solver_params(hdir=hdir)
+    with _native.Mesh(X, T, tag, krn, precision=prec, grid_ctas=args.grid, ctas_per_sm=args.ctas_per_sm,
+                      pcg_variant=args.pcg_variant, coarse_box_nodes=args.coarse) as M:
+        M.set_state(m0, None, m0)
+        M.minimize(h0, sp)
+        _, g, _ = M.energy_grad(h0 - 1.0, sp)
+        for _ in range(3):
+            M.timer_start()
+            _, iters = M.apply_minv(g, sp)
+            ms = M.timer_stop()
+        info = M.info()
+    print(f"minv: {args.workload} {args.precision} grid {info['grid_ctas']} x {info['block_threads']} "
+          f"(build {info['kernel_ctas_per_sm']} CTAs/SM): {iters} truncated-CG iterations, {ms:.3f} ms with the "
+          f"vector transfers")
+    return 0
+
+
 def mlp_train(args) -> int:
     rng = np.random.default_rng(0)
     feats = rng.standard_normal((args.samples, _native.MLP_FEATURES)).astype(np.float32)
@@ -218,6 +245,14 @@ def main(argv=None) -> int:
                     help="two-level Poisson preconditioner with boxes of about this many nodes (0: Jacobi)")
     pt.add_argument("--from-step", type=int, default=211)
     pt.add_argument("--steps", type=int, default=6)
+    mi = sub.add_parser("minv")
+    mi.add_argument("--workload", choices=["multigrain", "large"], default="large")
+    mi.add_argument("--precision", choices=["fp64", "mixed"], default="mixed")
+    mi.add_argument("--grid", type=int, default=0, help="CTAs (0: the size-based default)")
+    mi.add_argument("--ctas-per-sm", type=int, choices=[0, 2, 3], default=0)
+    mi.add_argument("--pcg-variant", type=int, choices=[0, 1, 2], default=0)
+    mi.add_argument("--coarse", type=int, default=0,
+                    help="two-level Poisson preconditioner with boxes of about this many nodes (0: Jacobi)")
     mt = sub.add_parser("mlp-train")
     mt.add_argument("--samples", type=int, default=16384)
     mt.add_argument("--epochs", type=int, default=2)
@@ -225,7 +260,7 @@ def main(argv=None) -> int:
     mp.add_argument("--rows", type=int, default=531441)
     args = ap.parse_args(argv)
     return {"field-step": field_step, "poisson-solve": poisson_solve, "phase-timers": phase_timers,
-            "mlp-train": mlp_train, "mlp-predict": mlp_predict}[args.case](args)
+            "minv": minv, "mlp-train": mlp_train, "mlp-predict": mlp_predict}[args.case](args)
 
 
 if __name__ == "__main__":
