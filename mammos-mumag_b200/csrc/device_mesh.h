@@ -97,7 +97,6 @@ struct SolveArgs {
   const int32_t* ctabox;  // [grid][3] first box, number of boxes and first slot of each CTA
   int co_off;           // dynamic shared-memory offset of the coarse vectors
   int co_rows;          // > 0: each CTA keeps its rows of Ainv32 in shared memory (capacity)
-  int co_nb;            // the most boxes a CTA holds rows of (its xc in shared memory)
   // training-sample recording (rec_cap > 0): at a hash-selected 1/rec_stride of the
   // (node, solve) pairs, the node's features at the warm start and, after the solve,
   // the target (u - u0) / sigma
@@ -217,7 +216,6 @@ struct DevMesh {
   int* d_bad = nullptr;
   int co_off = -1;
   int co_rows = 0;
-  int co_nb = 0;
 };
 
 // A batched persistent launch over several meshes: mesh q runs on CTAs

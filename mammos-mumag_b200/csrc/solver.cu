@@ -120,20 +120,12 @@ __device__ __forceinline__ double warp_max(double v) {
   return v;
 }
 
-// The per-warp partials and the totals of a grid reduction, one copy per CTA that every
-// reduction uses (each reduction instantiation declaring its own would add ~2 KB of static
-// shared memory per instantiation, and shared memory taken from the SM's 256 KB is L1 cache
-// lost).  Reductions never overlap: the partials are read before the __syncthreads of the
-// reduction's grid barrier, the totals before the next reduction's barrier.
-__shared__ double red_sh[32][kMaxRed];
-__shared__ double red_res[kMaxRed];
-
 // Deterministic grid reduction of K values (bit k of maxmask: max instead of sum); also a
 // grid barrier.  On return v[] holds totals identical in every thread of every CTA.
 template <int K>
 __device__ __noinline__ bool grid_reduce(Sync& s, double (&v)[K], unsigned maxmask) {
-  double(&sh)[32][kMaxRed] = red_sh;
-  double(&res)[kMaxRed] = red_res;
+  __shared__ double sh[32][kMaxRed];
+  __shared__ double res[kMaxRed];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
   const unsigned long long tr0 = (s.timing && threadIdx.x == 0) ? globaltimer() : 0ull;
 #pragma unroll
@@ -243,171 +235,36 @@ struct Ctx {
 
 __device__ __forceinline__ const double* plane(const SolveArgs& a, int p) { return a.vals + (size_t)p * a.nent; }
 
-// Loads of streamed operator data (values and columns read once per pass) that do not
-// allocate in L1, so L1 keeps the gathered vectors (neighbouring rows' entries of z, v, x, u),
-// which are reused across a warp's rows.  Global memory only.
-__device__ __forceinline__ float ldna(const float* p) {
-  float v;
-  asm("ld.global.nc.L1::no_allocate.f32 %0, [%1];" : "=f"(v) : "l"(p));
-  return v;
-}
-__device__ __forceinline__ double ldna(const double* p) {
-  double v;
-  asm("ld.global.nc.L1::no_allocate.f64 %0, [%1];" : "=d"(v) : "l"(p));
-  return v;
-}
-__device__ __forceinline__ int32_t ldna(const int32_t* p) {
-  int32_t v;
-  asm("ld.global.nc.L1::no_allocate.b32 %0, [%1];" : "=r"(v) : "l"(p));
-  return v;
-}
-// ldna when NA (the pointer is global memory), a plain load otherwise (it may be shared memory)
-template <bool NA, class T>
-__device__ __forceinline__ T ldop(const T* p) {
-  if constexpr (NA)
-    return ldna(p);
-  else
-    return *p;
-}
-
-// Entries per memory round trip of the C-operator row gathers: the next chunk's columns are
-// loaded while the current chunk gathers v and loads its 7 operator values, so a chunk costs
-// one round trip instead of two (column, then v).  Results do not depend on the chunk size:
-// every entry is added in entry order.
-#ifndef MUMAG_CCHUNK32
-#define MUMAG_CCHUNK32 4
-#endif
-#ifndef MUMAG_CCHUNK64
-#define MUMAG_CCHUNK64 2
-#endif
-
 // C v at row i (exchange scalar + anisotropy blocks), v a 3-vector; VT = operator value
 // type, XT = vector type (FP64 products and sums in every case)
-template <class VT, class XT = double, int CH = (sizeof(VT) == 4 ? MUMAG_CCHUNK32 : MUMAG_CCHUNK64)>
+template <class VT, class XT = double>
 __device__ __forceinline__ void apply_C_row_t(const Ctx& c, const VT* Aex, const VT* K, const XT* v, int64_t off,
                                               int64_t loff, int w, double o[3]) {
   const SolveArgs& a = c.a;
   const int64_t ps = a.nent;
   const int n = a.Npad;
   double o0 = 0, o1 = 0, o2 = 0;
-  int jc[CH];
-#pragma unroll
-  for (int q = 0; q < CH; ++q) jc[q] = q < w ? c.scol[loff + 32 * (int64_t)q] : 0;
-  for (int k0 = 0; k0 < w; k0 += CH) {
-    int jn[CH];
-#pragma unroll
-    for (int q = 0; q < CH; ++q) {
-      const int k = k0 + CH + q;
-      jn[q] = k < w ? c.scol[loff + 32 * (int64_t)k] : 0;
-    }
-#pragma unroll
-    for (int q = 0; q < CH; ++q) {
-      if (k0 + q < w) {
-        const int64_t e = off + 32 * (int64_t)(k0 + q);
-        const int j = jc[q];
-        const double v0 = (double)v[j], v1 = (double)v[n + j], v2 = (double)v[2 * n + j];
-        const double ax = (double)ldna(Aex + e);
-        const double k0v = (double)ldna(K + e), k1 = (double)ldna(K + ps + e), k2 = (double)ldna(K + 2 * ps + e);
-        const double k3 = (double)ldna(K + 3 * ps + e), k4 = (double)ldna(K + 4 * ps + e),
-                     k5 = (double)ldna(K + 5 * ps + e);
-        o0 += ax * v0 + (k0v * v0 + k1 * v1 + k2 * v2);
-        o1 += ax * v1 + (k1 * v0 + k3 * v1 + k4 * v2);
-        o2 += ax * v2 + (k2 * v0 + k4 * v1 + k5 * v2);
-      }
-    }
-#pragma unroll
-    for (int q = 0; q < CH; ++q) jc[q] = jn[q];
+#pragma unroll 4
+  for (int k = 0; k < w; ++k) {
+    const int64_t e = off + 32 * (int64_t)k;
+    const int j = c.scol[loff + 32 * (int64_t)k];
+    const double v0 = (double)v[j], v1 = (double)v[n + j], v2 = (double)v[2 * n + j];
+    const double ax = (double)__ldg(Aex + e);
+    const double k0 = (double)__ldg(K + e), k1 = (double)__ldg(K + ps + e), k2 = (double)__ldg(K + 2 * ps + e);
+    const double k3 = (double)__ldg(K + 3 * ps + e), k4 = (double)__ldg(K + 4 * ps + e), k5 = (double)__ldg(K + 5 * ps + e);
+    o0 += ax * v0 + (k0 * v0 + k1 * v1 + k2 * v2);
+    o1 += ax * v1 + (k1 * v0 + k3 * v1 + k4 * v2);
+    o2 += ax * v2 + (k2 * v0 + k4 * v1 + k5 * v2);
   }
   o[0] = o0;
   o[1] = o1;
   o[2] = o2;
 }
 
-// The two gathers of an energy evaluation at row i in one pass over the row's entries: C x
-// (exchange + anisotropy) and, with the magnetostatic term on, G u (the three gradient planes
-// applied to the potential).  Same per-entry arithmetic and order as two separate passes;
-// one column load and one round trip per chunk of CH entries serve both.
-template <class VT, int CH = (sizeof(VT) == 4 ? MUMAG_CCHUNK32 : MUMAG_CCHUNK64)>
-__device__ __forceinline__ void eval_row_t(const Ctx& c, const VT* Aex, const VT* K, const VT* G, const double* x,
-                                           const double* u, bool hmag, int64_t off, int64_t loff, int w, double gc[3],
-                                           double gh[3]) {
-  const int64_t ps = c.a.nent;
-  const int n = c.a.Npad;
-  double o0 = 0, o1 = 0, o2 = 0, h0 = 0, h1 = 0, h2 = 0;
-  int jc[CH];
-#pragma unroll
-  for (int q = 0; q < CH; ++q) jc[q] = q < w ? c.scol[loff + 32 * (int64_t)q] : 0;
-  for (int k0 = 0; k0 < w; k0 += CH) {
-    int jn[CH];
-#pragma unroll
-    for (int q = 0; q < CH; ++q) {
-      const int k = k0 + CH + q;
-      jn[q] = k < w ? c.scol[loff + 32 * (int64_t)k] : 0;
-    }
-#pragma unroll
-    for (int q = 0; q < CH; ++q) {
-      if (k0 + q < w) {
-        const int64_t e = off + 32 * (int64_t)(k0 + q);
-        const int j = jc[q];
-        const double v0 = x[j], v1 = x[n + j], v2 = x[2 * n + j];
-        const double ax = (double)ldna(Aex + e);
-        const double k0v = (double)ldna(K + e), k1 = (double)ldna(K + ps + e), k2 = (double)ldna(K + 2 * ps + e);
-        const double k3 = (double)ldna(K + 3 * ps + e), k4 = (double)ldna(K + 4 * ps + e),
-                     k5 = (double)ldna(K + 5 * ps + e);
-        o0 += ax * v0 + (k0v * v0 + k1 * v1 + k2 * v2);
-        o1 += ax * v1 + (k1 * v0 + k3 * v1 + k4 * v2);
-        o2 += ax * v2 + (k2 * v0 + k4 * v1 + k5 * v2);
-        if (hmag) {
-          const double uj = u[j];
-          h0 += (double)ldna(G + e) * uj;
-          h1 += (double)ldna(G + ps + e) * uj;
-          h2 += (double)ldna(G + 2 * ps + e) * uj;
-        }
-      }
-    }
-#pragma unroll
-    for (int q = 0; q < CH; ++q) jc[q] = jn[q];
-  }
-  gc[0] = o0;
-  gc[1] = o1;
-  gc[2] = o2;
-  gh[0] = h0;
-  gh[1] = h1;
-  gh[2] = h2;
-}
-
-// The right-hand side of the Poisson solve at row i, b = sum_k dk x_k, and S u of the warm
-// start (skipped on a zero start), in one chunked pass over the row's entries (entry order).
-template <class DT, int CH = (sizeof(DT) == 4 ? MUMAG_CCHUNK32 : MUMAG_CCHUNK64)>
-__device__ __forceinline__ void rhs_row(const int32_t* scol, const double* sS, const DT* Dk, int64_t ps, const double* x,
-                                        const double* u, int n, bool zero_start, int64_t off, int64_t loff, int w,
-                                        double& b, double& su) {
-  double bb = 0, s = 0;
-  int jc[CH];
-#pragma unroll
-  for (int q = 0; q < CH; ++q) jc[q] = q < w ? scol[loff + 32 * (int64_t)q] : 0;
-  for (int k0 = 0; k0 < w; k0 += CH) {
-    int jn[CH];
-#pragma unroll
-    for (int q = 0; q < CH; ++q) {
-      const int k = k0 + CH + q;
-      jn[q] = k < w ? scol[loff + 32 * (int64_t)k] : 0;
-    }
-#pragma unroll
-    for (int q = 0; q < CH; ++q) {
-      if (k0 + q < w) {
-        const int64_t e = off + 32 * (int64_t)(k0 + q);
-        const int j = jc[q];
-        bb += (double)ldna(Dk + e) * x[j] + (double)ldna(Dk + ps + e) * x[n + j] +
-              (double)ldna(Dk + 2 * ps + e) * x[2 * n + j];
-        if (!zero_start) s += sS[loff + 32 * (int64_t)(k0 + q)] * u[j];
-      }
-    }
-#pragma unroll
-    for (int q = 0; q < CH; ++q) jc[q] = jn[q];
-  }
-  b = bb;
-  su = s;
+// C v in FP64 (energies and gradients)
+__device__ __forceinline__ void apply_C_row(const Ctx& c, const double* v, int64_t off, int64_t loff, int w,
+                                            double o[3]) {
+  apply_C_row_t<double>(c, plane(c.a, P_AEX), plane(c.a, P_K), v, off, loff, w, o);
 }
 
 // ---------------------------------------------------------------------------------------
@@ -714,7 +571,7 @@ __device__ __noinline__ bool learned_start_mixed(Ctx& c, const double* x, double
 // width, the same for the warp's 32 lanes, so the guards do not diverge.
 constexpr int kChunk32 = 8;  // FP32 gather chunk (16 measured slower: fewer resident warps)
 
-template <class VT, class ZT, class AT, int CH, bool NA = false>
+template <class VT, class ZT, class AT, int CH>
 __device__ __forceinline__ AT gather_row(const Ctx& c, const VT* sval, int64_t loff, int w, const ZT* z) {
   AT acc = 0;
   int jc[CH];
@@ -722,8 +579,8 @@ __device__ __forceinline__ AT gather_row(const Ctx& c, const VT* sval, int64_t l
 #pragma unroll
   for (int q = 0; q < CH; ++q) {
     const bool in = q < w;
-    jc[q] = in ? ldop<NA>(c.scol + loff + 32 * (int64_t)q) : 0;
-    vc[q] = in ? ldop<NA>(sval + loff + 32 * (int64_t)q) : VT(0);
+    jc[q] = in ? c.scol[loff + 32 * (int64_t)q] : 0;
+    vc[q] = in ? sval[loff + 32 * (int64_t)q] : VT(0);
   }
   for (int k0 = 0; k0 < w; k0 += CH) {
     int jn[CH];
@@ -732,8 +589,8 @@ __device__ __forceinline__ AT gather_row(const Ctx& c, const VT* sval, int64_t l
     for (int q = 0; q < CH; ++q) {
       const int k = k0 + CH + q;
       const bool in = k < w;
-      jn[q] = in ? ldop<NA>(c.scol + loff + 32 * (int64_t)k) : 0;
-      vn[q] = in ? ldop<NA>(sval + loff + 32 * (int64_t)k) : VT(0);
+      jn[q] = in ? c.scol[loff + 32 * (int64_t)k] : 0;
+      vn[q] = in ? sval[loff + 32 * (int64_t)k] : VT(0);
     }
 #pragma unroll
     for (int q = 0; q < CH; ++q)
@@ -779,8 +636,7 @@ __device__ __noinline__ bool pcg_loop2(Ctx& c, double alpha, double beta, double
     END_ROWS
     CHECK(grid_barrier(c.sy));
     FOR_ROWS(c)
-    const double acc = a.stage ? gather_row<double, double, double, 8>(c, c.sS, loff_, w_, z)
-                               : gather_row<double, double, double, 8, true>(c, c.sS, loff_, w_, z);
+    const double acc = gather_row<double, double, double, 8>(c, c.sS, loff_, w_, z);
     rec_store_w(rc, i, n, acc);
     pd += acc * z[i];
     END_ROWS
@@ -810,8 +666,14 @@ __device__ __noinline__ bool pcg_solve(Ctx& c, const double* x) {
   {
     double pg = 0, pr2 = 0, pb = 0, pz = 0;
     FOR_ROWS(c)
-    double b, su;
-    rhs_row(c.scol, c.sS, Dk, ps, x, a.u, n, zero_start, off_, loff_, w_, b, su);
+    double b = 0, su = 0;
+#pragma unroll 4
+    for (int k = 0; k < w_; ++k) {
+      const int64_t e = ENTRY(k);
+      const int j = c.scol[LENTRY(k)];
+      b += __ldg(Dk + e) * x[j] + __ldg(Dk + ps + e) * x[n + j] + __ldg(Dk + 2 * ps + e) * x[2 * n + j];
+      if (!zero_start) su += c.sS[LENTRY(k)] * a.u[j];
+    }
     if (zero_start) a.u[i] = 0.0;
     const double r = b - su;
     const double invd = __ldg(a.invdS + i);
@@ -957,8 +819,7 @@ __device__ __noinline__ bool pcg_inner2(Ctx& c, double alpha, double beta, doubl
     END_ROWS
     CHECK(grid_barrier(c.sy));
     FOR_ROWS(c)
-    const float acc = a.stage ? gather_row<float, float, float, kChunk32>(c, c.sS32, loff_, w_, z)
-                              : gather_row<float, float, float, kChunk32, true>(c, c.sS32, loff_, w_, z);
+    const float acc = gather_row<float, float, float, kChunk32>(c, c.sS32, loff_, w_, z);
     rc[i].w = acc;
     pd += (double)acc * (double)z[i];
     END_ROWS
@@ -986,8 +847,14 @@ __device__ __noinline__ bool pcg_solve_mixed(Ctx& c, const double* x) {
   {  // FP64 residual of the warm start; FP32 inner record
     double p0 = 0, p1 = 0, p2 = 0, p3 = 0, pz = 0;
     FOR_ROWS(c)
-    double b, su;
-    rhs_row(c.scol, c.sS, Dk, ps, x, a.u, n, zero_start, off_, loff_, w_, b, su);
+    double b = 0, su = 0;
+#pragma unroll 4
+    for (int k = 0; k < w_; ++k) {
+      const int64_t e = ENTRY(k);
+      const int j = c.scol[LENTRY(k)];
+      b += __ldg(Dk + e) * x[j] + __ldg(Dk + ps + e) * x[n + j] + __ldg(Dk + 2 * ps + e) * x[2 * n + j];
+      if (!zero_start) su += c.sS[LENTRY(k)] * a.u[j];
+    }
     if (zero_start) a.u[i] = 0.0;
     const double r = b - su;
     const double invd = __ldg(a.invdS + i);
@@ -1135,7 +1002,7 @@ __device__ __forceinline__ Rows rows_of(const Ctx& c) {
 constexpr int kChunkCoarse = 16;
 
 // gather_row over the staged pattern given by its column array
-template <class VT, class ZT, class AT, int CH, bool NA = false>
+template <class VT, class ZT, class AT, int CH>
 __device__ __forceinline__ AT gather_row_r(const int32_t* scol, const VT* sval, int64_t loff, int w, const ZT* z) {
   AT acc = 0;
   int jc[CH];
@@ -1143,8 +1010,8 @@ __device__ __forceinline__ AT gather_row_r(const int32_t* scol, const VT* sval, 
 #pragma unroll
   for (int q = 0; q < CH; ++q) {
     const bool in = q < w;
-    jc[q] = in ? ldop<NA>(scol + loff + 32 * (int64_t)q) : 0;
-    vc[q] = in ? ldop<NA>(sval + loff + 32 * (int64_t)q) : VT(0);
+    jc[q] = in ? scol[loff + 32 * (int64_t)q] : 0;
+    vc[q] = in ? sval[loff + 32 * (int64_t)q] : VT(0);
   }
   for (int k0 = 0; k0 < w; k0 += CH) {
     int jn[CH];
@@ -1153,8 +1020,8 @@ __device__ __forceinline__ AT gather_row_r(const int32_t* scol, const VT* sval, 
     for (int q = 0; q < CH; ++q) {
       const int k = k0 + CH + q;
       const bool in = k < w;
-      jn[q] = in ? ldop<NA>(scol + loff + 32 * (int64_t)k) : 0;
-      vn[q] = in ? ldop<NA>(sval + loff + 32 * (int64_t)k) : VT(0);
+      jn[q] = in ? scol[loff + 32 * (int64_t)k] : 0;
+      vn[q] = in ? sval[loff + 32 * (int64_t)k] : VT(0);
     }
 #pragma unroll
     for (int q = 0; q < CH; ++q)
@@ -1226,14 +1093,20 @@ __device__ __forceinline__ double coarse_xc(const Rows& r, int t) {
   return rb >= 0 ? r.cxc[rb - r.cb0] : 0.0;
 }
 
+// The box of this lane's row in slice t, -1 for Dirichlet and padding rows.
+__device__ __forceinline__ int coarse_row_box(const Ctx& c, int t) {
+  const unsigned bit = 1u << c.lane;
+  return (c.cmk[2 * t] & bit) ? c.csb[2 * t] : ((c.cmk[2 * t + 1] & bit) ? c.csb[2 * t + 1] : -1);
+}
+
 // grid_reduce plus the box exchange: before the barrier the CTA's box partials (a warp per
 // box over the slices' sums, a fixed-order warp sum) go to its slots; after it every slot is
 // loaded into shared memory together with the reduction's partials.
 template <int K>
 __device__ __noinline__ bool grid_reduce_coarse(Ctx& c, double (&v)[K]) {
   Sync& s = c.sy;
-  double(&sh)[32][kMaxRed] = red_sh;
-  double(&res)[kMaxRed] = red_res;
+  __shared__ double sh[32][kMaxRed];
+  __shared__ double res[kMaxRed];
   const int lane = c.lane, warp = c.warp, nw = c.nwarps;
   const unsigned long long tr0 = (s.timing && threadIdx.x == 0) ? globaltimer() : 0ull;
 #pragma unroll
@@ -1326,15 +1199,6 @@ __device__ __noinline__ void coarse_update(Ctx& c, bool restart, double alpha, d
     if (c.crows) {
       const float* row = c.crows + (size_t)q * nc;
       for (int j = c.lane; j < nc; j += 32) acc += (double)row[j] * c.cPr[j];
-    } else if ((nc & 3) == 0) {  // from L2, 16-byte loads all in flight at once
-      const float4* row = reinterpret_cast<const float4*>(a.Ainv32 + (size_t)(c.cb0 + q) * nc);
-      const int n4 = nc >> 2;
-#pragma unroll 8
-      for (int j = c.lane; j < n4; j += 32) {
-        const float4 r = __ldg(row + j);
-        const double* pr = c.cPr + 4 * j;
-        acc += (double)r.x * pr[0] + (double)r.y * pr[1] + (double)r.z * pr[2] + (double)r.w * pr[3];
-      }
     } else {
       const float* row = a.Ainv32 + (size_t)(c.cb0 + q) * nc;
       for (int j = c.lane; j < nc; j += 32) acc += (double)__ldg(row + j) * c.cPr[j];
@@ -1344,6 +1208,12 @@ __device__ __noinline__ void coarse_update(Ctx& c, bool restart, double alpha, d
   }
   __syncthreads();
   if (c.sy.timing && threadIdx.x == 0) c.t_cgat += globaltimer() - t0;
+}
+
+// xc of the box of this lane's row in slice t (0 for Dirichlet and padding rows).
+__device__ __forceinline__ double coarse_xc(const Ctx& c, int t) {
+  const int rb = coarse_row_box(c, t);
+  return rb >= 0 ? c.cxc[rb - c.cb0] : 0.0;
 }
 
 // Pr = P^T v for a residual v given per row by val(i) (after a warm start changed it).
@@ -1376,8 +1246,14 @@ __device__ __noinline__ bool pcg_solve_coarse(Ctx& c, const double* x) {
   {  // b = sum_k dk x_k, r0 = b - S u, and its box sums
     double pr2 = 0, pb = 0, pz = 0;
     FOR_ROWS_R(rw)
-    double b, su;
-    rhs_row(rw.scol, rw.sS, Dk, ps, x, a.u, n, zero_start, off_, loff_, w_, b, su);
+    double b = 0, su = 0;
+#pragma unroll 4
+    for (int k = 0; k < w_; ++k) {
+      const int64_t e = ENTRY(k);
+      const int j = rw.scol[LENTRY(k)];
+      b += __ldg(Dk + e) * x[j] + __ldg(Dk + ps + e) * x[n + j] + __ldg(Dk + 2 * ps + e) * x[2 * n + j];
+      if (!zero_start) su += rw.sS[LENTRY(k)] * a.u[j];
+    }
     if (zero_start) a.u[i] = 0.0;
     const double r = b - su;
     const double invd = __ldg(a.invdS + i);
@@ -1428,8 +1304,7 @@ __device__ __noinline__ bool pcg_solve_coarse(Ctx& c, const double* x) {
   {  // w0 = S z0, delta = w0.z0, box sums of w0
     double pd = 0;
     FOR_ROWS_R(rw)
-    const double acc = a.stage ? gather_row_r<double, double, double, kChunkCoarse>(rw.scol, rw.sS, loff_, w_, z)
-                               : gather_row_r<double, double, double, kChunkCoarse, true>(rw.scol, rw.sS, loff_, w_, z);
+    const double acc = gather_row_r<double, double, double, kChunkCoarse>(rw.scol, rw.sS, loff_, w_, z);
     rec_store_w(a.rec[0], i, n, acc);
     pd += acc * z[i];
     coarse_slice_sum(rw, s_ - rw.s0, acc);
@@ -1460,8 +1335,7 @@ __device__ __noinline__ bool pcg_solve_coarse(Ctx& c, const double* x) {
     END_ROWS
     CHECK(grid_barrier(c.sy));
     FOR_ROWS_R(rw)
-    const double acc = a.stage ? gather_row_r<double, double, double, kChunkCoarse>(rw.scol, rw.sS, loff_, w_, z)
-                               : gather_row_r<double, double, double, kChunkCoarse, true>(rw.scol, rw.sS, loff_, w_, z);
+    const double acc = gather_row_r<double, double, double, kChunkCoarse>(rw.scol, rw.sS, loff_, w_, z);
     rec_store_w(a.rec[0], i, n, acc);
     pd += acc * z[i];
     coarse_slice_sum(rw, s_ - rw.s0, acc);
@@ -1489,7 +1363,7 @@ __device__ __noinline__ bool pcg_solve_coarse(Ctx& c, const double* x) {
 template <bool TC>
 __device__ __noinline__ bool pcg_solve_mixed_coarse(Ctx& c, const double* x) {
   const SolveArgs& a = c.a;
-  const float* Dk = a.vals32 + (size_t)P_D * a.nent;  // FP32 divergence planes, FP64 sums
+  const double* Dk = plane(a, P_D);
   const int64_t ps = a.nent;
   const int n = a.Npad;
   const Rows rw = rows_of(c);
@@ -1500,8 +1374,14 @@ __device__ __noinline__ bool pcg_solve_mixed_coarse(Ctx& c, const double* x) {
   {  // FP64 residual of the warm start, FP32 inner record, box sums of the FP32 residual
     double p0 = 0, p1 = 0, pz = 0;
     FOR_ROWS_R(rw)
-    double b, su;
-    rhs_row(rw.scol, rw.sS, Dk, ps, x, a.u, n, zero_start, off_, loff_, w_, b, su);
+    double b = 0, su = 0;
+#pragma unroll 4
+    for (int k = 0; k < w_; ++k) {
+      const int64_t e = ENTRY(k);
+      const int j = rw.scol[LENTRY(k)];
+      b += __ldg(Dk + e) * x[j] + __ldg(Dk + ps + e) * x[n + j] + __ldg(Dk + 2 * ps + e) * x[2 * n + j];
+      if (!zero_start) su += rw.sS[LENTRY(k)] * a.u[j];
+    }
     if (zero_start) a.u[i] = 0.0;
     const double r = b - su;
     const double invd = __ldg(a.invdS + i);
@@ -1555,8 +1435,7 @@ __device__ __noinline__ bool pcg_solve_mixed_coarse(Ctx& c, const double* x) {
     {  // w0 = S32 z0, delta = w0.z0, box sums of w0
       double pd = 0;
       FOR_ROWS_R(rw)
-      const float acc = a.stage ? gather_row_r<float, float, float, kChunkCoarse>(rw.scol, rw.sS32, loff_, w_, z)
-                                : gather_row_r<float, float, float, kChunkCoarse, true>(rw.scol, rw.sS32, loff_, w_, z);
+      const float acc = gather_row_r<float, float, float, kChunkCoarse>(rw.scol, rw.sS32, loff_, w_, z);
       rc[i].w = acc;
       pd += (double)acc * (double)z[i];
       coarse_slice_sum(rw, s_ - rw.s0, (double)acc);
@@ -1571,46 +1450,23 @@ __device__ __noinline__ bool pcg_solve_mixed_coarse(Ctx& c, const double* x) {
       if (c.sy.timing && threadIdx.x == 0) c.t_phase_start = globaltimer();
       const float af = (float)alpha, bf = (float)beta;
       double pg = 0, pd = 0, pr2 = 0;
-      {  // update phase; the next slice's record, z, p and e are loaded before the current
-         // slice is updated, so a warp's load round trips overlap its arithmetic and stores
-        int s = rw.s0 + rw.warp;
-        PcgRec32 qn{};
-        float zn0 = 0.f, ppn = 0.f, en = 0.f;
-        if (s < rw.s1) {
-          const int i = s * kSlice + rw.lane;
-          qn = rc[i];
-          zn0 = z[i];
-          ppn = a.pp32[i];
-          en = a.e32[i];
-        }
-        for (; s < rw.s1; s += rw.nwarps) {
-          const int i = s * kSlice + rw.lane;
-          const PcgRec32 q = qn;
-          const float zc = zn0, ppc = ppn, ec = en;
-          const int sn2 = s + rw.nwarps;
-          if (sn2 < rw.s1) {
-            const int j = sn2 * kSlice + rw.lane;
-            qn = rc[j];
-            zn0 = z[j];
-            ppn = a.pp32[j];
-            en = a.e32[j];
-          }
-          const float sn = q.w + bf * q.s;
-          const float r = q.r - af * sn;
-          const float zn = r * q.invd + (float)coarse_xc(rw, s - rw.s0);
-          const float p = zc + bf * ppc;
-          a.pp32[i] = p;
-          a.e32[i] = ec + af * p;
-          rc[i] = PcgRec32{r, q.w, sn, q.invd};
-          z[i] = zn;
-          pg += (double)r * (double)zn;
-          pr2 += (double)r * (double)r;
-        }
-      }
+      FOR_ROWS_R(rw)
+      (void)w_;
+      const PcgRec32 q = rc[i];
+      const float sn = q.w + bf * q.s;
+      const float r = q.r - af * sn;
+      const float zn = r * q.invd + (float)coarse_xc(rw, s_ - rw.s0);
+      const float p = z[i] + bf * a.pp32[i];
+      a.pp32[i] = p;
+      a.e32[i] = a.e32[i] + af * p;
+      rc[i] = PcgRec32{r, q.w, sn, q.invd};
+      z[i] = zn;
+      pg += (double)r * (double)zn;
+      pr2 += (double)r * (double)r;
+      END_ROWS
       CHECK(grid_barrier(c.sy));
       FOR_ROWS_R(rw)
-      const float acc = a.stage ? gather_row_r<float, float, float, kChunkCoarse>(rw.scol, rw.sS32, loff_, w_, z)
-                                : gather_row_r<float, float, float, kChunkCoarse, true>(rw.scol, rw.sS32, loff_, w_, z);
+      const float acc = gather_row_r<float, float, float, kChunkCoarse>(rw.scol, rw.sS32, loff_, w_, z);
       rc[i].w = acc;
       pd += (double)acc * (double)z[i];
       coarse_slice_sum(rw, s_ - rw.s0, (double)acc);
@@ -1676,20 +1532,45 @@ __device__ bool eval(Ctx& c, const double* x, const double* xref, const double* 
   if (tm) c.t_pcg += globaltimer() - te0;
   const int n = a.Npad;
   const double* G = plane(a, P_G);
+  const int64_t ps = a.nent;
   const double cz0 = (-c.h * a.hdir[0]) / a.V;
   const double cz1 = (-c.h * a.hdir[1]) / a.V;
   const double cz2 = (-c.h * a.hdir[2]) / a.V;
   double pE = 0, pgd = 0, pdx = 0, px = 0, pgi = 0;
   FOR_ROWS(c)
-  double gc[3], gh[3];
-  if (a.mixed)  // FP32 operator values, FP64 vectors and sums
-    eval_row_t<float>(c, a.vals32 + (size_t)P_AEX * a.nent, a.vals32 + (size_t)P_K * a.nent,
-                      a.vals32 + (size_t)P_G * a.nent, x, a.u, a.hmag_on > 0, off_, loff_, w_, gc, gh);
-  else
-    eval_row_t<double>(c, plane(a, P_AEX), plane(a, P_K), G, x, a.u, a.hmag_on > 0, off_, loff_, w_, gc, gh);
+  double gc[3];
+  double gh0 = 0, gh1 = 0, gh2 = 0;
+  if (a.mixed) {  // FP32 operator values, FP64 vectors and sums
+    apply_C_row_t<float>(c, a.vals32 + (size_t)P_AEX * a.nent, a.vals32 + (size_t)P_K * a.nent, x, off_, loff_, w_,
+                         gc);
+    if (a.hmag_on > 0) {
+      const float* G32 = a.vals32 + (size_t)P_G * a.nent;
+#pragma unroll 4
+      for (int k = 0; k < w_; ++k) {
+        const int64_t e = ENTRY(k);
+        const double uj = a.u[c.scol[LENTRY(k)]];
+        gh0 += (double)__ldg(G32 + e) * uj;
+        gh1 += (double)__ldg(G32 + ps + e) * uj;
+        gh2 += (double)__ldg(G32 + 2 * ps + e) * uj;
+      }
+    }
+  } else {
+    apply_C_row(c, x, off_, loff_, w_, gc);
+    if (a.hmag_on > 0) {
+#pragma unroll 4
+      for (int k = 0; k < w_; ++k) {
+        const int64_t e = ENTRY(k);
+        const double uj = a.u[c.scol[LENTRY(k)]];
+        gh0 += __ldg(G + e) * uj;
+        gh1 += __ldg(G + ps + e) * uj;
+        gh2 += __ldg(G + 2 * ps + e) * uj;
+      }
+    }
+  }
   const double mi = __ldg(a.meas + i);
   const double xi[3] = {x[i], x[n + i], x[2 * n + i]};
   const double gz[3] = {cz0 * mi, cz1 * mi, cz2 * mi};
+  const double gh[3] = {gh0, gh1, gh2};
   double gfl[3], gp[3];
   for (int q = 0; q < 3; ++q) gfl[q] = (gz[q] + gc[q]) + gh[q];
   pE += (xi[0] * gz[0] + xi[1] * gz[1] + xi[2] * gz[2]) +
@@ -2187,10 +2068,10 @@ __device__ __forceinline__ void solve_body(const SolveArgs& args, int nblk, int 
     double* base = reinterpret_cast<double*>(smem + args.co_off);
     c.cPs = base;
     c.cPr = base + args.nc;
-    c.cslv = base + 2 * args.nc;
+    c.cxc = base + 2 * args.nc;
+    c.cslv = base + 3 * args.nc;
     c.csv = c.cslv + args.nc + kMaxGrid;
-    c.cxc = c.csv + 2 * args.meta_max;
-    c.csb = reinterpret_cast<int*>(c.cxc + args.co_nb);
+    c.csb = reinterpret_cast<int*>(c.csv + 2 * args.meta_max);
     c.cmk = reinterpret_cast<unsigned*>(c.csb + 2 * args.meta_max);
     int* bsl = reinterpret_cast<int*>(c.cmk + 2 * args.meta_max);
     for (int q = threadIdx.x; q <= args.nc; q += blockDim.x) bsl[q] = __ldg(args.bslot + q);
@@ -2308,16 +2189,13 @@ struct StagePlan {
   int extra_off;  // offset of the extra region, -1 = none
   int co_off;     // offset of the coarse region, -1 = none
   int co_rows;    // rows of Ac^-1 each CTA stages (the most boxes a CTA holds), 0 = none
-  int co_nb;      // the most boxes a CTA holds rows of (the size of its xc)
 };
-// Regions: [staged entries][slice metadata][coarse vectors: Ps, Pr (nc doubles each), the
-// staged box slots (nc + kMaxGrid doubles), per slice two partial sums, xc of the CTA's boxes,
-// per slice two box ids and two lane masks, every box's first slot (nc + 1 ints), the CTA's
-// rows of Ac^-1 in FP32 when they fit and `stage_rows`][tensor-core network].  Shared memory
-// is taken from the SM's L1 cache, so the rows are staged only for the two-CTA build: three
-// resident CTAs with their rows would leave L1 too small for the gathers.
+// Regions: [staged entries][slice metadata][coarse vectors: Ps, Pr, xc (nc doubles each),
+// the staged box slots (nc + kMaxGrid doubles), per slice two partial sums, two box ids and
+// two lane masks, every box's first slot (nc + 1 ints), the CTA's rows of Ac^-1 in FP32
+// when they fit][tensor-core network]
 StagePlan stage_plan(const DevMesh& m, int grid, size_t limit, size_t extra = 0, bool allow_stage = true,
-                     int nc = 0, bool stage_rows = true) {
+                     int nc = 0) {
   int64_t emax = 0, smax = 0;
   for (int b = 0; b < grid; ++b) {
     const int64_t s0 = (m.h.nslices * b) / grid, s1 = (m.h.nslices * (b + 1)) / grid;
@@ -2325,8 +2203,17 @@ StagePlan stage_plan(const DevMesh& m, int grid, size_t limit, size_t extra = 0,
     smax = std::max(smax, s1 - s0);
   }
   const size_t meta = (size_t)smax * (sizeof(int64_t) + sizeof(int32_t));
-  int bmax = 0;  // the most boxes one CTA holds rows of
-  if (nc > 0)
+  const size_t coarse = nc > 0 ? (size_t)(4 * nc + kMaxGrid + 2 * smax) * sizeof(double) +
+                                     (size_t)(4 * smax + nc + 1) * sizeof(int) + 16
+                               : 0;
+  const size_t need = (size_t)emax * (sizeof(double) + sizeof(int32_t) + (m.vals32 ? sizeof(float) : 0));
+  StagePlan p;
+  p.stage = (allow_stage && need + meta + 16 + coarse + (extra ? extra + 1024 : 0) <= limit) ? 1 : 0;
+  // the two-level preconditioner's rows of Ac^-1 per CTA, staged when they fit beside the rest
+  p.co_rows = 0;
+  size_t rows = 0;
+  if (nc > 0) {
+    int bmax = 0;
     for (int b = 0; b < grid; ++b) {
       const int64_t r0 = kSlice * ((m.h.nslices * b) / grid), r1 = kSlice * ((m.h.nslices * (b + 1)) / grid);
       int lo = INT_MAX, hi = -1;
@@ -2337,17 +2224,6 @@ StagePlan stage_plan(const DevMesh& m, int grid, size_t limit, size_t extra = 0,
         }
       if (hi >= 0) bmax = std::max(bmax, hi - lo + 1);
     }
-  const size_t coarse = nc > 0 ? (size_t)(3 * nc + kMaxGrid + 2 * smax + bmax) * sizeof(double) +
-                                     (size_t)(4 * smax + nc + 1) * sizeof(int) + 16
-                               : 0;
-  const size_t need = (size_t)emax * (sizeof(double) + sizeof(int32_t) + (m.vals32 ? sizeof(float) : 0));
-  StagePlan p;
-  p.stage = (allow_stage && need + meta + 16 + coarse + (extra ? extra + 1024 : 0) <= limit) ? 1 : 0;
-  // the two-level preconditioner's rows of Ac^-1 per CTA, staged when they fit beside the rest
-  p.co_rows = 0;
-  p.co_nb = bmax;
-  size_t rows = 0;
-  if (nc > 0 && stage_rows) {
     const size_t want = (size_t)bmax * nc * sizeof(float) + 16;
     const size_t used = (p.stage ? need : 0) + meta + 16 + coarse + (extra ? extra + 1024 : 0);
     if (bmax > 0 && used + want <= limit) {
@@ -2446,8 +2322,7 @@ void solver_configure(DevMesh& m) {
   // share SMs, would lose residency to the region and keep the network on mma.sync.
   const size_t extra =
       (m.warm == WARM_LEARNED && block == kTcThreads && grid <= prop.multiProcessorCount) ? (size_t)kSmTc : 0;
-  if (m.kernel_mb != 2 && m.kernel_mb != 3) m.kernel_mb = 2;
-  const StagePlan sp = stage_plan(m, grid, limit, extra, m.opt.stage_operators != 0, m.nc, m.kernel_mb == 2);
+  const StagePlan sp = stage_plan(m, grid, limit, extra, m.opt.stage_operators != 0, m.nc);
   m.stage = sp.stage;
   m.stage_max = sp.stage_max;
   m.meta_max = sp.meta_max;
@@ -2455,7 +2330,6 @@ void solver_configure(DevMesh& m) {
   m.tc_off = sp.extra_off;
   m.co_off = sp.co_off;
   m.co_rows = sp.co_rows;
-  m.co_nb = sp.co_nb;
   // The attribute is per kernel, shared by every mesh: raise it to the device limit once
   // (occupancy follows each launch's actual request).
   const int dsm = (int)(prop.sharedMemPerBlockOptin - 16 * 1024);
@@ -2463,6 +2337,7 @@ void solver_configure(DevMesh& m) {
       cudaFuncSetAttribute(k_solve<3, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, dsm) != cudaSuccess ||
       cudaFuncSetAttribute(k_solve<2, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, dsm) != cudaSuccess)
     throw std::runtime_error("cannot reserve shared memory for the solver kernel");
+  if (m.kernel_mb != 2 && m.kernel_mb != 3) m.kernel_mb = 2;
   int occ = 0;
   if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, solve_kernel(m), block, m.smem) != cudaSuccess || occ < 1)
     throw std::runtime_error("persistent solver kernel cannot be resident with " + std::to_string(block) +
@@ -2608,7 +2483,6 @@ SolveArgs solver_args(const DevMesh& m, int mode, double h, const mm_solver_para
   a.ctabox = m.ctabox;
   a.co_off = m.co_off;
   a.co_rows = m.co_rows;
-  a.co_nb = m.co_nb;
   a.bar_stall = m.bar_stall;
   a.warm = m.warm;
   a.warm_gate2 = m.warm_gate * m.warm_gate;
