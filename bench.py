@@ -287,6 +287,20 @@ def host_cores() -> int:
         return os.cpu_count() or 1
 
 
+def _reference_samples(workload, procs, warm, steps):
+    """``warm`` untimed then ``steps`` timed oracle samples in ``procs`` spawned processes
+    (each process builds the oracle's operators on its first sample, untimed).  Returns the
+    samples and the wall time of the timed ones."""
+    import multiprocessing as mp
+    from concurrent.futures import ProcessPoolExecutor
+
+    with ProcessPoolExecutor(max_workers=procs, mp_context=mp.get_context("spawn")) as ex:
+        list(ex.map(_oracle_job, [workload] * warm))
+        t0 = time.perf_counter()
+        res = list(ex.map(_oracle_job, [workload] * steps))
+        return res, time.perf_counter() - t0
+
+
 def run_reference(args, world, rank):
     """The reference's algorithm on the host cores: the oracle port (the reference's own
     esys-escript/JAX stack is not installable here), on the same workload and configuration
@@ -298,7 +312,7 @@ def run_reference(args, world, rank):
     memory bandwidth, so it is if anything low).  Under torchrun rank 0 alone runs."""
     if rank != 0:
         return 0
-    import multiprocessing as mp
+    from concurrent.futures.process import BrokenProcessPool
 
     cores = host_cores()
     avail = None
@@ -308,18 +322,27 @@ def run_reference(args, world, rank):
         avail = psutil.virtual_memory().available
     except Exception:
         pass
-    per_proc = {"large": 8 << 30, "multigrain": 1 << 30, "single": 1 << 28}[args.workload]
+    # peak resident memory of one sample process (the oracle's operator build): 24.7 GB
+    # measured on the large mesh, ~15x less on the multigrain one
+    per_proc = {"large": 26 << 30, "multigrain": 3 << 30, "single": 1 << 29}[args.workload]
     procs = max(1, min(8, cores, args.steps + args.warmup,
                        int(avail // per_proc) if avail else 8))
     if args.ref_procs > 0:
         procs = min(procs, args.ref_procs)
     for k in ("OMP_NUM_THREADS", "OPENBLAS_NUM_THREADS", "MKL_NUM_THREADS"):
         os.environ[k] = "1"
-    with mp.get_context("spawn").Pool(procs) as pool:
-        pool.map(_oracle_job, [args.workload] * max(args.warmup, procs), chunksize=1)
-        t0 = time.perf_counter()
-        res = pool.map(_oracle_job, [args.workload] * args.steps, chunksize=1)
-        wall = time.perf_counter() - t0
+    # A sample process that dies (the kernel's out-of-memory killer) breaks the executor with
+    # an error instead of leaving the map waiting: retry with half the processes, down to one.
+    while True:
+        try:
+            res, wall = _reference_samples(args.workload, procs, max(args.warmup, procs), args.steps)
+            break
+        except BrokenProcessPool as e:
+            if procs == 1:
+                print(json.dumps({"impl": "reference", "unavailable": f"the oracle's sample process died ({e!r}); "
+                                  f"it needs about {per_proc >> 30} GB of host memory"}), flush=True)
+                return 0
+            procs = max(1, procs // 2)
     secs = [r[0] for r in res]
     v = len(secs) / sum(secs)
     sample = (f"field step 1 of the sweep from the initial state (u = 0) per step, NumPy/SciPy oracle, "
