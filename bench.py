@@ -287,6 +287,31 @@ def host_cores() -> int:
         return os.cpu_count() or 1
 
 
+def host_memory_available():
+    """Bytes of host memory this process may still use: the host's available memory, capped
+    by the memory cgroup's limit less its usage (v2 or v1 files) where one is set; None if
+    unknown."""
+    avail = None
+    try:
+        import psutil
+
+        avail = psutil.virtual_memory().available
+    except Exception:
+        pass
+    for lim, use in (("/sys/fs/cgroup/memory.max", "/sys/fs/cgroup/memory.current"),
+                     ("/sys/fs/cgroup/memory/memory.limit_in_bytes", "/sys/fs/cgroup/memory/memory.usage_in_bytes")):
+        try:
+            text = pathlib.Path(lim).read_text().strip()
+            if text == "max" or int(text) >= 1 << 60:
+                break
+            left = max(0, int(text) - int(pathlib.Path(use).read_text().strip()))
+            avail = left if avail is None else min(avail, left)
+            break
+        except (OSError, ValueError):
+            continue
+    return avail
+
+
 def _reference_samples(workload, procs, warm, steps):
     """``warm`` untimed then ``steps`` timed oracle samples in ``procs`` spawned processes
     (each process builds the oracle's operators on its first sample, untimed).  Returns the
@@ -315,13 +340,7 @@ def run_reference(args, world, rank):
     from concurrent.futures.process import BrokenProcessPool
 
     cores = host_cores()
-    avail = None
-    try:
-        import psutil
-
-        avail = psutil.virtual_memory().available
-    except Exception:
-        pass
+    avail = host_memory_available()
     # peak resident memory of one sample process (the oracle's operator build): 24.7 GB
     # measured on the large mesh, ~15x less on the multigrain one
     per_proc = {"large": 26 << 30, "multigrain": 3 << 30, "single": 1 << 29}[args.workload]

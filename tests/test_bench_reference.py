@@ -60,3 +60,10 @@ def test_reference_arm_reports_unavailable_when_one_process_dies(monkeypatch, ca
     assert calls == [4, 2, 1]
     assert set(line) == {"impl", "unavailable"} and line["impl"] == "reference"
     assert "host memory" in line["unavailable"]
+
+
+def test_host_memory_budget_is_within_the_host():
+    import psutil
+
+    avail = bench.host_memory_available()
+    assert avail is not None and 0 <= avail <= psutil.virtual_memory().total
