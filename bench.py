@@ -746,7 +746,8 @@ def finish_b200(args, world, rank, local, name, variants, runs, head, j0, order,
     cpu = None
     if cpu_p is not None:
         cpu_p.join(timeout=1800)
-        res = cpu_q.get(timeout=5) if not cpu_q.empty() else {"error": "no result"}
+        res = (cpu_q.get(timeout=5) if not cpu_q.empty()
+               else {"error": f"no result (sample process exit code {cpu_p.exitcode}; -9: killed, e.g. out of memory)"})
         if "seconds" in res:
             same = {k: 1e3 / runs[k]["steps"][0]["device_ms"] for k in ("fp64", head)}
             cpu = {"value": 1.0 / res["seconds"], "unit": UNIT, "cores": 1, "host_cores": host_cores(), "kind": "port",
