@@ -341,9 +341,9 @@ def run_reference(args, world, rank):
 
     cores = host_cores()
     avail = host_memory_available()
-    # peak resident memory of one sample process (the oracle's operator build): 24.7 GB
+    # peak resident memory of one sample process (the oracle's operator build): 7.3 GB
     # measured on the large mesh, ~15x less on the multigrain one
-    per_proc = {"large": 26 << 30, "multigrain": 3 << 30, "single": 1 << 29}[args.workload]
+    per_proc = {"large": 9 << 30, "multigrain": 1 << 30, "single": 1 << 29}[args.workload]
     procs = max(1, min(8, cores, args.steps + args.warmup,
                        int(avail // per_proc) if avail else 8))
     if args.ref_procs > 0:

@@ -232,14 +232,16 @@ class Problem:
         SA = asm(lap * (2.0 * A / V)[:, None, None])
         mass = np.where(np.eye(4)[None] > 0, 2.0, 1.0) * (vol / 20.0)[:, None, None]
         mk = mass * (-2.0 * K / V)[:, None, None]  # [E,4,4]
-        # 3N x 3N interleaved: row 3i+p, col 3j+q
-        r3 = (3 * np.repeat(T, 4, axis=1))[:, :, None, None] + np.arange(3)[None, None, :, None]
-        c3 = (3 * np.tile(T, (1, 4)))[:, :, None, None] + np.arange(3)[None, None, None, :]
-        uu = uax[:, :, None] * uax[:, None, :]  # [E,3,3]
-        vals = mk.reshape(E, 16)[:, :, None, None] * uu[:, None, :, :]
-        r3b = np.broadcast_to(r3, vals.shape).ravel()
-        c3b = np.broadcast_to(c3, vals.shape).ravel()
-        Kani = sp.csr_matrix((vals.ravel(), (r3b, c3b)), shape=(3 * N, 3 * N))
+        # 3N x 3N interleaved: row 3i+p, col 3j+q.  One N x N block per (p, q), each entry
+        # the element sum of mk_ab u_p u_q in element order, placed by a Kronecker product
+        # (the blocks' stored entries do not overlap); assembled block by block so that the
+        # transient COO arrays stay N x N sized on large meshes.
+        Kani = None
+        for p in range(3):
+            for q in range(3):
+                unit = sp.csr_matrix(([1.0], ([p], [q])), shape=(3, 3))
+                blk = sp.kron(asm(mk * (uax[:, p] * uax[:, q])[:, None, None]), unit, format="csr")
+                Kani = blk if Kani is None else Kani + blk
         Cex = sp.kron(SA, sp.eye(3), format="csr")
         self.C = (Cex + Kani).tocsr()
         self.C.sum_duplicates()

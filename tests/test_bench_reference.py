@@ -1,9 +1,10 @@
 """The reference arm of bench.py when one of its sample processes dies.
 
-Each sample process builds the CPU oracle's operators, about 25 GB on the large mesh, so on a
-host with less memory the kernel's out-of-memory killer may end one.  The arm must then
-retry with half the processes, and once a single process dies too, print its
-``unavailable`` line and exit 0 rather than wait for a result that will never come.  The
+Each sample process builds the CPU oracle's operators, about 7 GB at its peak on the large
+mesh, so on a host with too little memory the kernel's out-of-memory killer may end one.
+The arm must then retry with half the processes, and once a single process dies too,
+print its ``unavailable`` line and exit 0 rather than wait for a result that will never
+come.  The
 process death is made on the host: the sampling helper raises the executor's own error."""
 
 import argparse
