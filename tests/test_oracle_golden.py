@@ -110,6 +110,33 @@ def test_pcg_matches_dense_solve():
     assert 0 < k < 40
 
 
+def test_twolevel_pcg_meets_the_same_stop_rule_in_fewer_iterations():
+    """The oracle's two-level PCG (the checker of the GPU's box-aggregate preconditioner)
+    solves the reference's Poisson system of a multigrain mesh to the reference's stop rule
+    r.r <= tol^2 b.b, agrees with the Jacobi solve to that accuracy, and needs fewer
+    iterations; one box holding every interior node is also a valid aggregate."""
+    from mammos_mumag import synthetic
+
+    X, T, tag, krn, m0 = synthetic.multigrain(n=12, L=30.0, grains=4, cone_deg=15.0, gb=2.0, seed=3)
+    P = O.Problem(X, T, tag, krn)
+    b = P.divergence(m0)
+    x0 = np.zeros(P.N)
+    xj, kj = O.pcg(P.S, P.diagS, b, x0, 1e-10)
+    nb = 4  # 4^3 geometric boxes over the interior nodes, Dirichlet nodes in none
+    lo, hi = P.X.min(0), P.X.max(0)
+    ijk = np.minimum(((P.X - lo) / (hi - lo) * nb).astype(int), nb - 1)
+    box = ijk[:, 0] + nb * (ijk[:, 1] + nb * ijk[:, 2])
+    box[P.bnd] = -1
+    inner = box >= 0
+    box[inner] = np.unique(box[inner], return_inverse=True)[1].ravel()  # no empty boxes
+    for agg in (box, np.where(P.bnd, -1, 0)):
+        xc, kc = O.pcg_twolevel(P.S, P.diagS, b, x0, 1e-10, agg)
+        r = b - P.S @ xc
+        assert r @ r <= 1e-20 * (b @ b)
+        assert np.abs(xc - xj).max() <= 1e-7 * np.abs(xj).max()
+        assert 0 < kc < kj
+
+
 def test_single_grain_sweep_fixture_is_the_oracles():
     """tests/golden/sweep_single.npz (the single-grain sweep through switching that the GPU
     sweeps are compared with) is what the oracle computes: regenerated here (a few seconds)."""
